@@ -1,0 +1,72 @@
+// rpy_kernels.cuh -- launch interface of the pairwise RPY block products.
+//
+// A block product V_t = M(t <- s) F_s is computed in two launches:
+//   1. rpy_tile: grid (target tiles x source splits); each CTA stages its
+//      source split (positions, forces, torques as float4) into shared memory
+//      with one bulk async copy per array, then every thread sums the pair
+//      blocks of its TI targets over the split in FP32 with blockwise
+//      compensated (TwoSum) accumulation, and writes one partial per target.
+//   2. rpy_reduce: sums the partials of each target over the splits in FP64
+//      in a fixed order (deterministic), adds the wall self block, and writes
+//      or accumulates the result in the caller's layout.
+// The split count is chosen so that the grid fills every SM; the partials
+// buffer (`scratch`) holds nsplit * (VD/3) * nt float4.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+
+namespace cufil {
+
+struct RpyBlockDesc {
+    int wall;             // 1: Swan-Brady wall blocks, 0: unbounded
+    int vd, fd;           // 3 or 6
+    int self_set;         // targets and sources are the same particles
+    const float4 *xt;     // target centres [nt] (w ignored)
+    int nt;
+    float at;             // target radius (unbounded only)
+    const float4 *xs;     // source centres [ns]
+    const float4 *fs;     // source forces [ns]
+    const float4 *ts;     // source torques [ns] (fd == 6)
+    int ns;
+    float as;             // source radius (unbounded only)
+    float mu;             // viscosity (unbounded only)
+};
+
+struct RpyPlan {
+    int ti;        // targets per thread
+    int tiles;     // target tiles (gridDim.x)
+    int nsplit;    // source splits (gridDim.y)
+    int split;     // sources per split
+    size_t smem;   // dynamic shared memory bytes of the tile kernel
+    size_t scratch_float4;  // float4 entries of the partials buffer
+};
+
+// Number of float4 entries needed in the partials buffer for any product with
+// at most nt_max targets (sizing helper for allocators).
+size_t rpy_scratch_float4(int nt_max, int ns_max, int vd, int num_sms);
+
+RpyPlan rpy_plan(int nt, int ns, int vd, int fd, int num_sms);
+
+// Launches the tile kernel; partials land in `scratch`.
+int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, int *dev_err,
+                     cudaStream_t st);
+
+// Output modes of the reduction.
+enum RpyOut : int { kOutWrite = 0, kOutAdd = 1 };
+
+// Reduces partials into out_f[i*stride + c] (float) for c < vd; components
+// vd..stride-1 are zeroed in write mode (the reference writes all six
+// entries of a segment velocity, cuda_functions.cu:460-469).
+int rpy_launch_reduce_f32(const RpyBlockDesc &d, const RpyPlan &plan, const float4 *scratch, float *out_f,
+                          int stride, int mode, cudaStream_t st);
+
+// Packing helpers between the reference's AoS host layouts and float4 arrays.
+int pack_xyz_to_float4(const float *aos3, float4 *out, int n, cudaStream_t st);
+int pack_ft6_to_float4(const float *aos6, float4 *force, float4 *torque, int n, cudaStream_t st);
+
+// Full product V_t (=|+=) M F_s with the right staging; convenience wrapper.
+int rpy_block_product(const RpyBlockDesc &d, float4 *scratch, size_t scratch_cap, int *dev_err, float *out_f,
+                      int stride, int mode, int num_sms, cudaStream_t st);
+
+}  // namespace cufil

@@ -1,0 +1,208 @@
+/*
+ * cufil.h -- C ABI of the B200 mobility engine for the cilia/filament Stokes
+ * simulator racksa/CUFCM_FIL.
+ *
+ * The reference exposes its hot path as the abstract C++ class
+ * `mobility_solver` (src/cilia/mobility/mobility_solver.hpp:19-128) whose
+ * back-ends (rpy_mobility_solver, fcm_mobility_solver) implement pure virtual
+ * staging/evaluation methods (mobility_solver.hpp:26-46) and whose generic
+ * layer assembles and solves the implicit saddle-point system
+ * (mobility_solver.hpp:81-111).  This header replaces that class with plain C
+ * entry points: opaque handles, plain pointers and sizes, int status codes.
+ * Every entry point cites the reference method it stands in for.
+ *
+ * Layouts follow the reference's host buffers exactly
+ * (mobility_solver.hpp:53-63, rpy_mobility_solver.cu:61-67):
+ *   x_segs [3*n_seg]  segment centres, AoS (x,y,z)
+ *   f_segs [6*n_seg]  segment force + torque, AoS (fx,fy,fz,tx,ty,tz)
+ *   v_segs [6*n_seg]  segment velocity + angular velocity, AoS
+ *   x_blobs, f_blobs, v_blobs [3*n_blob]  blob centres / forces / velocities
+ * Segment order is swimmer -> filament -> segment
+ * (id = n*NFIL*NSEG + m*NSEG + k, mobility_solver.cpp:432).
+ *
+ * Error convention: every function returns CF_OK (0) or a CF_E* code and
+ * never exits or aborts; cf_last_error() gives a thread-local message.
+ * A handle is not thread-safe; distinct handles are independent.
+ */
+#ifndef CUFIL_H
+#define CUFIL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CF_API __attribute__((visibility("default")))
+#else
+#define CF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define CF_OK 0
+#define CF_EINVAL 1          /* bad argument or size */
+#define CF_ENOMEM 2          /* device or pinned allocation failed */
+#define CF_ECUDA 3           /* CUDA runtime / driver error */
+#define CF_NOT_CONVERGED 4   /* GMRES stopped at its iteration cap */
+#define CF_NONFINITE 5       /* NaN/Inf met in inputs or iterates */
+#define CF_TIMEOUT 6         /* a bounded device wait gave up */
+#define CF_ENOTSUP 7         /* configuration not supported */
+
+/* Thread-local message for the last failing call on this thread. */
+CF_API const char *cf_last_error(void);
+/* ABI version: major*10000 + minor*100 + patch. */
+CF_API int cf_version(void);
+
+/* ============================================================ mobility ==
+ * Back-end of mobility_solver: staging + block products of the RPY grand
+ * mobility matrix (rpy_mobility_solver.{hpp,cu}; kernels cuda_functions.cu).
+ */
+typedef struct cf_mobility cf_mobility;
+
+typedef struct cf_mobility_config {
+    int n_seg;          /* NSWIM*NFIL*NSEG segments (may be 0) */
+    int n_blob;         /* NSWIM*NBLOB rigid-body blobs (may be 0) */
+    int wall;           /* 1: no-slip wall z=0, Swan-Brady (INFINITE_PLANE_WALL);
+                           0: unbounded RPY (cuda_functions.cu:205-356) */
+    int seg_dof;        /* 3: segments carry forces only (PRESCRIBED_CILIA);
+                           6: forces + torques, velocities + angular velocities */
+    double seg_radius;  /* RSEG (config.hpp); the wall formula assumes 1 */
+    double blob_radius; /* RBLOB */
+    double mu;          /* MU; the wall formula assumes 1 */
+    int device;         /* CUDA device ordinal */
+} cf_mobility_config;
+
+/* allocate_host_memory + allocate_device_memory (rpy_mobility_solver.cu:54-117) */
+CF_API int cf_mobility_create(const cf_mobility_config *cfg, cf_mobility **out);
+/* free_host_memory + free_device_memory (rpy_mobility_solver.cu:14-52) */
+CF_API int cf_mobility_destroy(cf_mobility *h);
+
+/* copy_{segment,blob}_{positions,forces}_to_device (rpy_mobility_solver.cu:119-175) */
+CF_API int cf_copy_segment_positions_to_device(cf_mobility *h, const float *x_segs);
+CF_API int cf_copy_segment_forces_to_device(cf_mobility *h, const float *f_segs);
+CF_API int cf_copy_blob_positions_to_device(cf_mobility *h, const float *x_blobs);
+CF_API int cf_copy_blob_forces_to_device(cf_mobility *h, const float *f_blobs);
+/* copy_{segment,blob}_velocities_to_host (rpy_mobility_solver.cu:177-205);
+ * these wait for the engine's stream. */
+CF_API int cf_copy_segment_velocities_to_host(cf_mobility *h, float *v_segs);
+CF_API int cf_copy_blob_velocities_to_host(cf_mobility *h, float *v_blobs);
+/* wait_for_device (rpy_mobility_solver.cu:247-256) */
+CF_API int cf_wait_for_device(cf_mobility *h);
+
+/* evaluate_*_mobility (rpy_mobility_solver.cu:258-338; kernels
+ * cuda_functions.cu:362-757).  Write/accumulate semantics mirror the kernels:
+ *   segment_segment  V_seg  = M_ss F_seg                       (Mss_mult)
+ *   segment_blob     V_seg += M_sb F_blob                      (Msb_mult)
+ *   blob_blob        V_blob = M_bb F_blob                      (Mbb_mult)
+ *   blob_segment     V_blob += M_bs F_seg  if seg_dof == 3,
+ *                    V_blob  = M_bs F_seg  if seg_dof == 6     (Mbs_mult)
+ *   full             V_seg = M_ss F_seg + M_sb F_blob,
+ *                    V_blob = M_bb F_blob + M_bs F_seg
+ * All are asynchronous on the engine's stream. */
+CF_API int cf_evaluate_segment_segment_mobility(cf_mobility *h);
+CF_API int cf_evaluate_segment_blob_mobility(cf_mobility *h);
+CF_API int cf_evaluate_blob_blob_mobility(cf_mobility *h);
+CF_API int cf_evaluate_blob_segment_mobility(cf_mobility *h);
+CF_API int cf_evaluate_full_mobility(cf_mobility *h);
+
+/* One synchronous host call: positions + forces in, velocities out
+ * (read_positions_and_forces + evaluate_full_mobility + copy_*_to_host).
+ * Any of the blob pointers may be NULL when n_blob == 0. */
+CF_API int cf_apply_mobility(cf_mobility *h, const float *x_segs, const float *x_blobs,
+                      const float *f_segs, const float *f_blobs,
+                      float *v_segs, float *v_blobs);
+
+/* Same product on device-resident buffers in the same AoS layouts (no host
+ * copies), enqueued on `stream` (a cudaStream_t; NULL is the legacy default
+ * stream, as everywhere in CUDA).  Asynchronous. */
+CF_API int cf_apply_mobility_device(cf_mobility *h, const float *d_x_segs, const float *d_x_blobs,
+                             const float *d_f_segs, const float *d_f_blobs,
+                             float *d_v_segs, float *d_v_blobs, void *stream);
+
+/* ========================================================== simulation ==
+ * Generic layer of mobility_solver for prescribed-shape cilia above a no-slip
+ * wall (CILIA_TYPE 3, BODY_OR_SURFACE_TYPE 0, MOBILITY_TYPE 1,
+ * SOLVER_TYPE 1 with right preconditioning): beat kinematics
+ * (filament::initial_guess, filament.cpp:1336-1500), RHS assembly
+ * (mobility_solver.cpp:284-634), block-diagonal preconditioner
+ * (apply_preconditioner_new, :1102-1594), saddle-point product
+ * (system_matrix_mult_new, :1887-2185) and GMRES (solve_linear_system,
+ * :2187-2669), all device-resident.
+ *
+ * Saddle vector layout (wall, PRESCRIBED_BODY_VELOCITIES, mobility_solver.cpp:361,373):
+ *   [ 3*N_s segment constraint forces lambda | N_fil phase rates | N_fil angle rates ]
+ * where the rate blocks are present when dynamic_phase / dynamic_angle are set.
+ */
+typedef struct cf_sim cf_sim;
+
+#define CF_BEAT_FULFORD_BLAKE 1          /* SHAPE_SEQUENCE 1 */
+#define CF_BEAT_FULFORD_BLAKE_ORIGINAL 4 /* SHAPE_SEQUENCE 4 */
+
+#define CF_PRECOND_NONE 0
+#define CF_PRECOND_BLOCK_DIAG 1          /* apply_preconditioner_new */
+#define CF_PRECOND_LEARNED 2             /* per-filament MLP (flexible GMRES) */
+
+typedef struct cf_sim_config {
+    int n_fil;              /* NFIL (one swimmer: the wall) */
+    int n_seg;              /* NSEG segments per filament */
+    double seg_sep;         /* SEG_SEP; DL = SEG_SEP*RSEG, RSEG = 1 */
+    int beat;               /* CF_BEAT_* */
+    int dynamic_phase;      /* DYNAMIC_PHASE_EVOLUTION */
+    int dynamic_angle;      /* DYNAMIC_SHAPE_ROTATION */
+    double dt;              /* DT = PERIOD/STEPS_PER_PERIOD */
+    double spring_factor;   /* TORSIONAL_SPRING_MAGNITUDE_FACTOR */
+    double gmres_tol;       /* LINEAR_SYSTEM_TOL (relative residual) */
+    int gmres_max_iter;     /* MAX_LINEAR_SYSTEM_ITER (capped at system size) */
+    int precond;            /* CF_PRECOND_* */
+    /* Base positions [3*n_fil] and per-filament natural frequency [n_fil]. */
+    const double *base_pos;
+    const double *omega0;
+    /* Initial phase and shape-rotation angle [n_fil] each (psi.dat). */
+    const double *phase0;
+    const double *angle0;
+    /* Reference generalised forces over one period (input/forcing/*.dat). */
+    const double *gen_phase_force_refs; int n_gen_phase_refs;
+    const double *gen_angle_force_refs; int n_gen_angle_refs;
+    /* Reference arclength parameters [rows*cols] (rows = phases over one period,
+     * cols = segments); NULL selects the bisection of
+     * filament::find_fitted_shape_s (WRITE_GENERALISED_FORCES mode). */
+    const double *s_values_ref; int s_ref_rows; int s_ref_cols;
+    int device;
+} cf_sim_config;
+
+CF_API int cf_sim_create(const cf_sim_config *cfg, cf_sim **out);
+CF_API int cf_sim_destroy(cf_sim *s);
+
+/* One implicit step nt: filament::initial_guess (phase/angle update when
+ * nt > 0, kinematics) + mobility_solver::compute_velocities (RHS, GMRES with
+ * warm start).  iters/relres may be NULL.  Returns CF_NOT_CONVERGED when GMRES
+ * met its cap (the iterate is still stored, as the reference does). */
+CF_API int cf_sim_step(cf_sim *s, int nt, int *iters, double *relres);
+/* Same without waiting for the result: iteration count and residual are
+ * recorded on the device and read by cf_sim_last_solve. */
+CF_API int cf_sim_step_async(cf_sim *s, int nt);
+CF_API int cf_sim_last_solve(cf_sim *s, int *iters, double *relres);
+/* Copy of the filament state [n_fil] each (any pointer may be NULL). */
+CF_API int cf_sim_get_state(cf_sim *s, double *phase, double *angle, double *phase_dot, double *angle_dot);
+/* Segment positions [3*N_s] and constraint forces [6*N_s] in the reference's
+ * host layouts (x_segs_host / f_segs_host). */
+CF_API int cf_sim_get_segments(cf_sim *s, float *x_segs, float *f_segs);
+/* Velocity directions K_phase, K_angle [3*N_s] each (vel_dir_phase/angle). */
+CF_API int cf_sim_get_directions(cf_sim *s, double *k_phase, double *k_angle);
+/* Size of the saddle-point system. */
+CF_API int cf_sim_system_size(cf_sim *s);
+/* Kinematics only (filament::initial_guess). */
+CF_API int cf_sim_initial_guess(cf_sim *s, int nt);
+/* assemble_rhs (mobility_solver.cpp:284-634) for the current state. */
+CF_API int cf_sim_assemble_rhs(cf_sim *s, int nt, double *rhs);
+/* apply_preconditioner_new: out = P^{-1} in (host vectors, system size). */
+CF_API int cf_sim_apply_preconditioner(cf_sim *s, const double *in, double *out);
+/* system_matrix_mult_new: out = A in (host vectors, system size). */
+CF_API int cf_sim_system_matvec(cf_sim *s, const double *in, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUFIL_H */
