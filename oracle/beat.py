@@ -113,14 +113,17 @@ class Beat:
             length += ((s / dl - fl) / (ce - fl)) * 0.5 * dl * (f[fl] + f[ce])
         return length
 
-    def s_bisection(self, psi):
-        """find_fitted_shape_s in WRITE_GENERALISED_FORCES mode (filament.cpp:1128-1180)."""
+    def s_bisection(self, psi, tol_factor=0.1):
+        """find_fitted_shape_s in WRITE_GENERALISED_FORCES mode (filament.cpp:1128-1180).
+
+        The bisection stops when the length fraction is within tol_factor/NSEG of its target;
+        the reference code uses 0.1 (filament.cpp:1143)."""
         n = self.nseg
         table = self._trap_table(psi)
         s = np.zeros(n)
         s[-1] = 1.0
         total = self.curve_length(1.0, psi, table)
-        tol = 0.1 / n
+        tol = tol_factor / n
         for k in range(1, n - 1):
             target = k / (n - 1)
             lo, hi = s[k - 1], 1.0
