@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Benchmark: implicit time steps per second of the plain wall-cilia simulation.
+
+Workload ("plain implicit simulation", one array per GPU): 256 prescribed
+Fulford-Blake cilia x 20 segments (5120 segments) on a 16 x 16 wall lattice of
+spacing 20a, segment spacing 2.6a, phases U(0, 2 pi) from a seed, angles
+N(0, 0.05), dt = T/300, dynamic phase and shape-rotation rates with the
+reference's own generalised-force tables, FP32 pair mobility, FP64 GMRES to a
+relative residual of 1e-6 with the block-diagonal preconditioner.  A step is
+one implicit time step (kinematics, RHS, GMRES, state update), one graph
+launch.  Every rank runs its own array (replicas: the path does not shard a
+single array), so `value` is the sum over ranks (weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference algorithm on the host cores (the
+oracle's restatement of the reference's CPU-side GMRES + an OpenMP RPY sum;
+the reference has no CPU mobility of its own) on a bounded sample of the same
+workload: each step is one full implicit step of the same 5120-segment array.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NX = 16            # 16 x 16 = 256 cilia
+NSEG = 20
+SEG_SEP = 2.6
+SPACING = 20.0
+GMRES_TOL = 1e-6
+F_PAIR = 154       # algorithmic flops of one 3x3 wall RPY pair (cuda_functions.cu:63-150)
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal SIMT FP32 peak at max SM clock
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_inputs(s_table_from="engine"):
+    from cufcm_fil_b200 import workloads
+    data = np.load(ROOT / "cufcm_fil_b200" / "data" / "fulford_blake_nseg20_sep2.6.npz")
+    F = NX * NX
+    bases = workloads.lattice_bases(F, NX, SPACING, 0.5 * SEG_SEP)
+    rng = np.random.default_rng(2024)
+    phase0 = rng.uniform(0.0, 2.0 * math.pi, F)
+    angle0 = rng.normal(0.0, 0.05, F)
+    # The arclength table over one period is what the reference's WRITE_GENERALISED_FORCES pre-run writes;
+    # the engine regenerates it on the device by the same bisection, the reference arm on the host.
+    if s_table_from == "engine":
+        from cufcm_fil_b200.sim import arclength_table
+        s_table = arclength_table(nseg=NSEG, seg_sep=SEG_SEP, steps=300)
+    else:
+        from oracle import implicit
+        _, _, s_table = implicit.write_generalised_forces_run(1, nseg=NSEG, seg_sep=SEG_SEP, tol=1e-3)
+    return dict(bases=bases, nseg=NSEG, seg_sep=SEG_SEP, dt=1.0 / 300, phase0=phase0, angle0=angle0,
+                spring_factor=0.01, phase_refs=data["phase"], angle_refs=data["angle"], s_table=s_table)
+
+
+def config_dict(extra=None):
+    c = {"workload": "plain implicit wall-cilia simulation: 256 cilia x 20 segments, 16x16 lattice spacing 20a, "
+                     "Fulford-Blake beat, dt=T/300, GMRES tol 1e-6, block-diagonal preconditioner",
+         "n_cilia": NX * NX, "segments_per_cilium": NSEG, "segments": NX * NX * NSEG, "lattice_spacing": SPACING,
+         "segment_spacing": SEG_SEP, "gmres_tol": GMRES_TOL, "l2": "flushed between timed steps (256 MiB write)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- distributed
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    from cufcm_fil_b200 import RpyMobilitySolver
+    from cufcm_fil_b200.sim import WallCiliaSimulation
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    inp = workload_inputs()
+    sim = WallCiliaSimulation(**inp, gmres_tol=GMRES_TOL, device=local)
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    nt = 0
+    for _ in range(args.warmup):
+        sim.step_async(nt)
+        nt += 1
+    sim.last_solve()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    first_nt = nt
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()           # L2 flush, outside the step's events
+                ev[k][0].record(stream)
+            sim.step_async(nt)
+            nt += 1
+            with torch.cuda.stream(stream):
+                ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    res = sim.last_solve()
+    iters = sim.iteration_log(4096)[[i % 4096 for i in range(first_nt, nt)]]
+    launches = int(sum(sim.launches_per_step(int(i)) for i in iters))
+    max_ms = max_over_ranks(world, total_ms)
+    steps_all = sum_over_ranks(world, float(args.steps))
+    value = steps_all / (max_ms / 1e3)
+
+    # ---- end to end through the host API: state up from pinned memory, step, results down
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64)).pin_memory()
+    st = sim.state()
+    h_phase, h_angle, h_pd, h_ad = (pin(st[k]) for k in ("phase", "angle", "phase_dot", "angle_dot"))
+    F = NX * NX
+    N = F * NSEG
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_events = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    e_events[0].record(stream)
+    for k in range(args.steps):
+        sim.set_state(h_phase, h_angle, h_pd, h_ad)   # H2D 4*F doubles
+        sim.step(nt)                                    # D2H: solver status
+        nt += 1
+        out = sim.state()                               # D2H 4*F doubles
+        x_segs, f_segs = sim.segments()                 # D2H 3N doubles (positions) + 3N doubles (forces)
+        h_phase.copy_(torch.from_numpy(out["phase"]))
+        h_angle.copy_(torch.from_numpy(out["angle"]))
+        h_pd.copy_(torch.from_numpy(out["phase_dot"]))
+        h_ad.copy_(torch.from_numpy(out["angle_dot"]))
+    e_events[1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(world, e_events[0].elapsed_time(e_events[1]))
+    e2e_value = steps_all / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant kernel: the pair mobility product (tile kernel + reduce) on this geometry
+    x_segs, _ = sim.segments()
+    mob = RpyMobilitySolver(N, 0, wall=True, seg_dof=3, device=local)
+    xd = torch.as_tensor(x_segs, device=dev)
+    fd = torch.randn(6 * N, device=dev)
+    vd = torch.empty(6 * N, device=dev)
+    ms = torch.cuda.Stream(device=dev)
+    for _ in range(5):
+        mob.apply_device(xd, fd, vd, stream=ms)
+    ms.synchronize()
+    reps = 50
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mt = 0.0
+    for r in range(reps):
+        with torch.cuda.stream(ms):
+            flush.zero_()
+            a.record(ms)
+        mob.apply_device(xd, fd, vd, stream=ms)
+        with torch.cuda.stream(ms):
+            b.record(ms)
+        ms.synchronize()
+        mt += a.elapsed_time(b)
+    apply_us = mt / reps * 1e3
+    pairs = float(N) * N
+    achieved = pairs * F_PAIR / (apply_us * 1e-6) / 1e12
+    mob.finalise()
+
+    if rank == 0:
+        cs = clocks.summary()
+        line = {
+            "metric": "timesteps/s (plain GMRES, tol 1e-6)", "value": value, "unit": "timesteps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs / f64 GMRES",
+            "data": "synthetic (seeded phases; reference forcing tables)",
+            "config": config_dict({"parallelism": f"replicas x{world}"}),
+            "gmres_iters_per_step": float(np.mean(iters)), "last_relres": res.relative_residual,
+            "rpy_pairs_per_s": pairs / (apply_us * 1e-6), "rpy_apply_us": apply_us,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+                         "frac": achieved / FP32_PEAK_TFLOPS, "traffic": None,
+                         "note": f"pair mobility product, {F_PAIR} flop/pair x {N}^2 pairs per launch; peak is the "
+                                 "nominal FP32 SIMT rate (148 SMs x 128 lanes x 2 x 1.965 GHz)"},
+            "e2e": {"value": e2e_value, "unit": "timesteps/s", "h2d_bytes_per_step": 4 * F * 8,
+                    "d2h_bytes_per_step": 4 * F * 8 + 3 * N * 8 + 3 * N * 8 + 16},
+            "gpu_launches": launches, "clocks": cs,
+            "cpu_baseline": cpu_baseline(inp) if (world == 1 and not args.no_cpu_baseline) else None,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(inp, steps=1):
+    """The oracle (FP64 restatement of the reference's step) on all host cores: one implicit step."""
+    import oracle
+    from oracle import implicit
+    sim = implicit.WallCilia(bases=inp["bases"], nseg=inp["nseg"], seg_sep=inp["seg_sep"], shape_sequence=1,
+                             dt=inp["dt"], phase0=inp["phase0"], angle0=inp["angle0"],
+                             spring_factor=inp["spring_factor"], phase_refs=inp["phase_refs"],
+                             angle_refs=inp["angle_refs"], s_table=inp["s_table"], gmres_tol=GMRES_TOL)
+    t0 = time.perf_counter()
+    its = []
+    for nt in range(steps):
+        it, _ = sim.step(nt)
+        its.append(it)
+    dt = time.perf_counter() - t0
+    return {"value": steps / dt, "unit": "timesteps/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{steps} implicit step(s) of the same 5120-segment array from the same initial state "
+                      f"({int(np.mean(its))} GMRES iterations)"}
+
+
+# ------------------------------------------------------------------ reference
+def run_reference(args):
+    world, rank, _ = dist_init()
+    if rank != 0:
+        return
+    import oracle
+    from oracle import implicit
+    inp = workload_inputs(s_table_from="host")
+    sim = implicit.WallCilia(bases=inp["bases"], nseg=inp["nseg"], seg_sep=inp["seg_sep"], shape_sequence=1,
+                             dt=inp["dt"], phase0=inp["phase0"], angle0=inp["angle0"],
+                             spring_factor=inp["spring_factor"], phase_refs=inp["phase_refs"],
+                             angle_refs=inp["angle_refs"], s_table=inp["s_table"], gmres_tol=GMRES_TOL)
+    nt = 0
+    for _ in range(args.warmup):
+        sim.step(nt)
+        nt += 1
+    t0 = time.perf_counter()
+    its = []
+    for _ in range(args.steps):
+        it, _ = sim.step(nt)
+        its.append(it)
+        nt += 1
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    cores = oracle.num_threads()
+    line = {
+        "impl": "reference", "metric": "timesteps/s (plain GMRES, tol 1e-6)", "value": value, "unit": "timesteps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded phases; reference forcing tables)", "config": config_dict(),
+        "gmres_iters_per_step": float(np.mean(its)),
+        "cpu_baseline": {"value": value, "unit": "timesteps/s", "cores": cores, "kind": "port",
+                         "sample": "each step is one full implicit step of the 5120-segment array: the reference's "
+                                   "host GMRES/preconditioner/beat restated in FP64 with an OpenMP RPY sum"},
+        "e2e": {"value": value, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

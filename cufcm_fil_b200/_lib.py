@@ -56,7 +56,7 @@ class SimConfig(ctypes.Structure):
                 ("gen_phase_force_refs", ctypes.c_void_p), ("n_gen_phase_refs", ctypes.c_int),
                 ("gen_angle_force_refs", ctypes.c_void_p), ("n_gen_angle_refs", ctypes.c_int),
                 ("s_values_ref", ctypes.c_void_p), ("s_ref_rows", ctypes.c_int), ("s_ref_cols", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("s_tol_factor", ctypes.c_double), ("device", ctypes.c_int)]
 
 
 _vp = ctypes.c_void_p
@@ -91,7 +91,12 @@ SIGNATURES = {
     "cf_sim_get_state": [_vp, _vp, _vp, _vp, _vp],
     "cf_sim_get_segments": [_vp, _vp, _vp],
     "cf_sim_get_directions": [_vp, _vp, _vp],
+    "cf_sim_get_arclengths": [_vp, _vp],
     "cf_sim_system_size": [_vp],
+    "cf_sim_stream": [_vp, ctypes.POINTER(_vp)],
+    "cf_sim_set_state": [_vp, _vp, _vp, _vp, _vp],
+    "cf_sim_iteration_log": [_vp, _vp, _i],
+    "cf_sim_launches_per_step": [_vp, _i],
     "cf_sim_initial_guess": [_vp, _i],
     "cf_sim_assemble_rhs": [_vp, _i, _vp],
     "cf_sim_apply_preconditioner": [_vp, _vp, _vp],

@@ -226,11 +226,11 @@ __global__ void pack_ft6_kernel(const float *__restrict__ a, float4 *__restrict_
     }
 }
 
+// Raises the dynamic shared-memory cap of one instantiation once per device.
+// Called before any launch (and therefore before any stream capture).
 template <bool WALL, int VD, int FD, int TI, bool SELF>
-int launch_tiles_t(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, int *dev_err,
-                   cudaStream_t st) {
+int configure_tiles_t() {
     auto kern = rpy_tile_kernel<WALL, VD, FD, TI, SELF>;
-    // Raise the dynamic shared-memory cap once per device for this instantiation.
     static bool configured[64] = {};
     int dev = 0;
     CF_CUDA(cudaGetDevice(&dev));
@@ -238,6 +238,14 @@ int launch_tiles_t(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, 
         CF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 + 3 * kMaxSplit * 16));
         if (dev >= 0 && dev < 64) configured[dev] = true;
     }
+    return CF_OK;
+}
+
+template <bool WALL, int VD, int FD, int TI, bool SELF>
+int launch_tiles_t(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, int *dev_err,
+                   cudaStream_t st) {
+    auto kern = rpy_tile_kernel<WALL, VD, FD, TI, SELF>;
+    CF_TRY((configure_tiles_t<WALL, VD, FD, TI, SELF>()));
     TileParams p;
     p.xt = d.xt;
     p.xs = d.xs;
@@ -324,6 +332,15 @@ int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch
                             : dispatch_dof<true, false>(d, plan, scratch, dev_err, st);
     // Unbounded blocks need no mask: r = 0 is handled by the containment branch.
     return dispatch_dof<false, false>(d, plan, scratch, dev_err, st);
+}
+
+int rpy_prepare(const RpyBlockDesc &d, const RpyPlan &plan) {
+    const bool self = d.self_set != 0;
+    if (d.wall && self) {
+        if (d.vd == 3 && d.fd == 3) return plan.ti == 2 ? configure_tiles_t<true, 3, 3, 2, true>() : configure_tiles_t<true, 3, 3, 1, true>();
+        if (d.vd == 6 && d.fd == 6) return plan.ti == 2 ? configure_tiles_t<true, 6, 6, 2, true>() : configure_tiles_t<true, 6, 6, 1, true>();
+    }
+    return CF_OK;  // other instantiations configure themselves on first launch
 }
 
 int rpy_launch_reduce_f32(const RpyBlockDesc &d, const RpyPlan &plan, const float4 *scratch, float *out_f,

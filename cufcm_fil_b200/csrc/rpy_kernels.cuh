@@ -48,6 +48,10 @@ size_t rpy_scratch_float4(int nt_max, int ns_max, int vd, int num_sms);
 
 RpyPlan rpy_plan(int nt, int ns, int vd, int fd, int num_sms);
 
+// Configures the tile-kernel instantiation used by (d, plan) so that later
+// launches may be captured into a CUDA graph.
+int rpy_prepare(const RpyBlockDesc &d, const RpyPlan &plan);
+
 // Launches the tile kernel; partials land in `scratch`.
 int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, int *dev_err,
                      cudaStream_t st);

@@ -1,0 +1,219 @@
+"""Host mirror of the reference's mobility-solver generic layer for prescribed cilia on a wall.
+
+``WallCiliaSimulation`` stands in for the pair (swimmer/filament objects,
+``mobility_solver``) that ``cilia_sim_main.cu`` drives for CILIA_TYPE 3 on an
+INFINITE_PLANE_WALL: one :meth:`step` is filament::initial_guess followed by
+mobility_solver::compute_velocities (cilia_sim_main.cu:405-416), executed on
+the device by libcufil.so.  The component methods keep the reference's names
+(``initial_guess``, ``assemble_rhs``, ``apply_preconditioner_new``,
+``system_matrix_mult_new``) so that a caller can test or drive each stage.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+@dataclass
+class GmresResult:
+    iterations: int
+    relative_residual: float
+    status: int
+
+
+class WallCiliaSimulation:
+    def __init__(self, *, bases, nseg=20, seg_sep=2.6, beat=_lib.CF_BEAT_FULFORD_BLAKE, dt=1.0 / 300,
+                 dynamic_phase=True, dynamic_angle=True, spring_factor=0.01, gmres_tol=1e-6, gmres_max_iter=350,
+                 precond=_lib.CF_PRECOND_BLOCK_DIAG, omega0=None, phase0=None, angle0=None, phase_refs=None,
+                 angle_refs=None, s_table=None, s_tol_factor=0.0, device=0):
+        self.bases = np.ascontiguousarray(bases, np.float64).reshape(-1, 3)
+        self.n_fil = self.bases.shape[0]
+        self.nseg = int(nseg)
+        f = self.n_fil
+        self._keep = []
+
+        def arr(x, n=None):
+            if x is None:
+                return None
+            a = np.ascontiguousarray(x, np.float64).ravel()
+            if n is not None:
+                assert a.size == n, (a.size, n)
+            self._keep.append(a)
+            return a
+
+        om, ph, an = arr(omega0, f), arr(phase0, f), arr(angle0, f)
+        pr, ar = arr(phase_refs), arr(angle_refs)
+        st = None if s_table is None else np.ascontiguousarray(s_table, np.float64)
+        if st is not None:
+            self._keep.append(st)
+        cfg = _lib.SimConfig(
+            n_fil=f, n_seg=self.nseg, seg_sep=float(seg_sep), beat=int(beat), dynamic_phase=int(bool(dynamic_phase)),
+            dynamic_angle=int(bool(dynamic_angle)), dt=float(dt), spring_factor=float(spring_factor),
+            gmres_tol=float(gmres_tol), gmres_max_iter=int(gmres_max_iter), precond=int(precond),
+            base_pos=_p(self.bases), omega0=_p(om), phase0=_p(ph), angle0=_p(an),
+            gen_phase_force_refs=_p(pr), n_gen_phase_refs=0 if pr is None else pr.size,
+            gen_angle_force_refs=_p(ar), n_gen_angle_refs=0 if ar is None else ar.size,
+            s_values_ref=_p(st), s_ref_rows=0 if st is None else st.shape[0],
+            s_ref_cols=0 if st is None else st.shape[1], s_tol_factor=float(s_tol_factor), device=int(device))
+        h = ctypes.c_void_p()
+        _lib.call("cf_sim_create", ctypes.byref(cfg), ctypes.byref(h))
+        self._h = h
+        self.size = _lib.load().cf_sim_system_size(h)
+        self.n_seg_total = self.n_fil * self.nseg
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.call("cf_sim_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- whole step -------------------------------------------------------
+    def step(self, nt: int) -> GmresResult:
+        """filament::initial_guess + mobility_solver::compute_velocities for step nt (synchronous)."""
+        it = ctypes.c_int()
+        rel = ctypes.c_double()
+        rc = _lib.call("cf_sim_step", self._h, int(nt), ctypes.byref(it), ctypes.byref(rel),
+                       ok=(_lib.CF_OK, _lib.CF_NOT_CONVERGED))
+        return GmresResult(it.value, rel.value, rc)
+
+    def step_async(self, nt: int):
+        """Enqueues step nt (one graph launch); read the solve with :meth:`last_solve`."""
+        _lib.call("cf_sim_step_async", self._h, int(nt))
+
+    def last_solve(self) -> GmresResult:
+        it = ctypes.c_int()
+        rel = ctypes.c_double()
+        rc = _lib.call("cf_sim_last_solve", self._h, ctypes.byref(it), ctypes.byref(rel),
+                       ok=(_lib.CF_OK, _lib.CF_NOT_CONVERGED))
+        return GmresResult(it.value, rel.value, rc)
+
+    # -- stages -----------------------------------------------------------
+    def initial_guess(self, nt: int):
+        _lib.call("cf_sim_initial_guess", self._h, int(nt))
+
+    def assemble_rhs(self, nt: int = 0) -> np.ndarray:
+        out = np.zeros(self.size)
+        _lib.call("cf_sim_assemble_rhs", self._h, int(nt), _p(out))
+        return out
+
+    def apply_preconditioner_new(self, v) -> np.ndarray:
+        v = np.ascontiguousarray(v, np.float64)
+        out = np.zeros(self.size)
+        _lib.call("cf_sim_apply_preconditioner", self._h, _p(v), _p(out))
+        return out
+
+    def system_matrix_mult_new(self, v) -> np.ndarray:
+        v = np.ascontiguousarray(v, np.float64)
+        out = np.zeros(self.size)
+        _lib.call("cf_sim_system_matvec", self._h, _p(v), _p(out))
+        return out
+
+    # -- state ------------------------------------------------------------
+    def stream_handle(self) -> int:
+        """cudaStream_t of the engine's stream (for events / external streams)."""
+        h = ctypes.c_void_p()
+        _lib.call("cf_sim_stream", self._h, ctypes.byref(h))
+        return h.value or 0
+
+    def set_state(self, phase=None, angle=None, phase_dot=None, angle_dot=None):
+        """Asynchronous upload of filament state from (preferably pinned) float64 host arrays."""
+        def q(a):
+            return None if a is None else ctypes.c_void_p(a.ctypes.data if hasattr(a, "ctypes") else a.data_ptr())
+        _lib.call("cf_sim_set_state", self._h, q(phase), q(angle), q(phase_dot), q(angle_dot))
+
+    def iteration_log(self, n: int) -> np.ndarray:
+        out = np.zeros(n, np.int32)
+        _lib.call("cf_sim_iteration_log", self._h, ctypes.c_void_p(out.ctypes.data), int(n))
+        return out
+
+    def launches_per_step(self, iters: int) -> int:
+        return _lib.load().cf_sim_launches_per_step(self._h, int(iters))
+
+    def state(self):
+        f = self.n_fil
+        ph, an, pd, ad = (np.zeros(f) for _ in range(4))
+        _lib.call("cf_sim_get_state", self._h, _p(ph), _p(an), _p(pd), _p(ad))
+        return dict(phase=ph, angle=an, phase_dot=pd, angle_dot=ad)
+
+    def segments(self):
+        """(x_segs [3N], f_segs [6N]) in the reference's host layouts."""
+        x = np.zeros(3 * self.n_seg_total, np.float32)
+        fs = np.zeros(6 * self.n_seg_total, np.float32)
+        _lib.call("cf_sim_get_segments", self._h, _p(x), _p(fs))
+        return x, fs
+
+    def directions(self):
+        kp = np.zeros(3 * self.n_seg_total)
+        ka = np.zeros(3 * self.n_seg_total)
+        _lib.call("cf_sim_get_directions", self._h, _p(kp), _p(ka))
+        return kp, ka
+
+    def arclengths(self) -> np.ndarray:
+        """Arclength parameters s of the current kinematics, [n_fil, nseg]."""
+        out = np.zeros(self.n_seg_total)
+        _lib.call("cf_sim_get_arclengths", self._h, _p(out))
+        return out.reshape(self.n_fil, self.nseg)
+
+    def tips(self) -> np.ndarray:
+        x, _ = self.segments()
+        return x.reshape(self.n_fil, self.nseg, 3)[:, -1, :].astype(np.float64)
+
+    def generalised_forces(self):
+        """K_phase^T lambda and K_angle^T lambda per filament (cilia_sim_main.cu:420-440)."""
+        kp, ka = self.directions()
+        _, fs = self.segments()
+        lam = fs.reshape(-1, 6)[:, :3].astype(np.float64)
+        kp = kp.reshape(-1, 3)
+        ka = ka.reshape(-1, 3)
+        qp = (kp * lam).sum(1).reshape(self.n_fil, self.nseg).sum(1)
+        qa = (ka * lam).sum(1).reshape(self.n_fil, self.nseg).sum(1)
+        return qp, qa
+
+
+def write_generalised_forces_run(beat=_lib.CF_BEAT_FULFORD_BLAKE, nseg=20, seg_sep=2.6, steps=300, tol=1e-8):
+    """The reference's WRITE_GENERALISED_FORCES run on the device: one filament with a prescribed
+    phase speed of 2 pi per period, arclength by bisection (cilia_sim_main.cu:101-140, 318-338, 420-440).
+    Returns (phase forces [steps], angle forces [steps])."""
+    qp = np.zeros(steps)
+    qa = np.zeros(steps)
+    with WallCiliaSimulation(bases=[[0.0, 0.0, 0.5 * seg_sep]], nseg=nseg, seg_sep=seg_sep, beat=beat,
+                             dt=1.0 / steps, dynamic_phase=False, dynamic_angle=False, gmres_tol=tol) as sim:
+        for nt in range(steps):
+            sim.step(nt)
+            a, b = sim.generalised_forces()
+            qp[nt], qa[nt] = a[0], b[0]
+    return qp, qa
+
+
+def arclength_table(beat=_lib.CF_BEAT_FULFORD_BLAKE, nseg=20, seg_sep=2.6, steps=300, tol_factor=0.0):
+    """Arclength parameters over one period [steps, nseg], as the reference's WRITE_GENERALISED_FORCES
+    run writes its s_values file (phase advancing by 2 pi/steps per step, bisection on the device)."""
+    out = np.zeros((steps, nseg))
+    with WallCiliaSimulation(bases=[[0.0, 0.0, 0.5 * seg_sep]], nseg=nseg, seg_sep=seg_sep, beat=beat,
+                             dt=1.0 / steps, dynamic_phase=False, dynamic_angle=False, gmres_tol=1e-3,
+                             s_tol_factor=tol_factor) as sim:
+        for nt in range(steps):
+            sim.initial_guess(nt)
+            out[nt] = sim.arclengths()[0]
+    return out

@@ -169,6 +169,9 @@ typedef struct cf_sim_config {
      * cols = segments); NULL selects the bisection of
      * filament::find_fitted_shape_s (WRITE_GENERALISED_FORCES mode). */
     const double *s_values_ref; int s_ref_rows; int s_ref_cols;
+    /* Bisection tolerance on the length fraction, times NSEG (0 selects the
+     * reference's 0.1, filament.cpp:1143). */
+    double s_tol_factor;
     int device;
 } cf_sim_config;
 
@@ -191,6 +194,18 @@ CF_API int cf_sim_get_state(cf_sim *s, double *phase, double *angle, double *pha
 CF_API int cf_sim_get_segments(cf_sim *s, float *x_segs, float *f_segs);
 /* Velocity directions K_phase, K_angle [3*N_s] each (vel_dir_phase/angle). */
 CF_API int cf_sim_get_directions(cf_sim *s, double *k_phase, double *k_angle);
+/* Arclength parameters of the current kinematics [n_fil*n_seg] (s_to_use). */
+CF_API int cf_sim_get_arclengths(cf_sim *s, double *s_values);
+/* The engine's stream of this handle (a cudaStream_t). */
+CF_API int cf_sim_stream(cf_sim *s, void **stream);
+/* Overwrites the filament state [n_fil] each from host memory (any pointer may
+ * be NULL); the rates are also the GMRES warm start.  Asynchronous. */
+CF_API int cf_sim_set_state(cf_sim *s, const double *phase, const double *angle, const double *phase_dot,
+                            const double *angle_dot);
+/* GMRES iterations of step nt are kept at index nt % 4096; copies the first n. */
+CF_API int cf_sim_iteration_log(cf_sim *s, int *iters, int n);
+/* Kernels launched by one step that ran `iters` GMRES iterations. */
+CF_API int cf_sim_launches_per_step(cf_sim *s, int iters);
 /* Size of the saddle-point system. */
 CF_API int cf_sim_system_size(cf_sim *s);
 /* Kinematics only (filament::initial_guess). */

@@ -1,0 +1,149 @@
+"""GPU parity of the device-resident implicit step through the C ABI.
+
+Stages are compared with the FP64 oracle (oracle/implicit.py, the restatement
+of mobility_solver.cpp and filament.cpp); whole runs are compared with the
+reference's own generalised-force tables and with oracle trajectories.
+Tolerances: FP64 stages 1e-10 relative; anything that contains the FP32 pair
+mobility 1e-5 relative (the mobility contract); trajectories as stated below.
+"""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import implicit
+from cufcm_fil_b200 import _lib, workloads
+from cufcm_fil_b200.sim import WallCiliaSimulation, write_generalised_forces_run
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(Path(__file__).resolve().parent / "golden" / "reference_forcing_nseg20_sep2.6.npz")
+
+
+@pytest.fixture(scope="module")
+def s_table():
+    # Arclength table of the Fulford-Blake beat over one period from the oracle's bisection
+    # (the reference's WRITE_GENERALISED_FORCES run writes the same table).
+    _, _, sv = implicit.write_generalised_forces_run(1, tol=1e-3)
+    return sv
+
+
+def make_pair(nx, spacing, s_table, seed=0, **kw):
+    F = nx * nx
+    bases = workloads.lattice_bases(F, nx, spacing, 1.3)
+    rng = np.random.default_rng(seed)
+    phase0 = rng.uniform(0, 2 * np.pi, F)
+    angle0 = rng.normal(0, 0.05, F)
+    args = dict(nseg=20, seg_sep=2.6, dt=1 / 300, phase0=phase0, angle0=angle0, spring_factor=0.01,
+                phase_refs=GOLD["fb_phase"], angle_refs=GOLD["fb_angle"], s_table=s_table)
+    args.update(kw)
+    tol = args.pop("gmres_tol", 1e-6)
+    gpu = WallCiliaSimulation(bases=bases, gmres_tol=tol, **args)
+    cpu = implicit.WallCilia(bases=bases, shape_sequence=1, gmres_tol=tol,
+                             **{k: v for k, v in args.items() if k not in ("beat",)})
+    return gpu, cpu
+
+
+def test_kinematics_rhs_match_oracle(s_table):
+    gpu, cpu = make_pair(3, 40.0, s_table)
+    with gpu:
+        gpu.initial_guess(0)
+        cpu.initial_guess(0)
+        x, _ = gpu.segments()
+        kp, ka = gpu.directions()
+        np.testing.assert_allclose(x.reshape(-1, 3), cpu.x, rtol=0, atol=2e-5)   # float32 output
+        np.testing.assert_allclose(kp, cpu.kp.ravel(), rtol=1e-10, atol=1e-9)
+        np.testing.assert_allclose(ka, cpu.ka.ravel(), rtol=1e-10, atol=1e-9)
+        np.testing.assert_allclose(gpu.arclengths(), cpu.s_values, rtol=0, atol=1e-12)
+        rhs = gpu.assemble_rhs(0)
+        np.testing.assert_allclose(rhs, cpu.assemble_rhs(), rtol=1e-11, atol=1e-6)
+
+
+def test_bisection_arclengths_match_oracle():
+    with WallCiliaSimulation(bases=[[0, 0, 1.3]], nseg=20, seg_sep=2.6, dynamic_phase=False,
+                             dynamic_angle=False) as gpu:
+        beat = oracle.beat.Beat(1, 20)
+        for nt in range(0, 300, 37):
+            gpu.initial_guess(nt)
+            psi = 2 * math.pi * nt / 300
+            np.testing.assert_allclose(gpu.arclengths()[0], beat.s_bisection(psi), atol=1e-9)
+
+
+@pytest.mark.parametrize("dyn", [(True, True), (True, False), (False, True), (False, False)])
+def test_preconditioner_and_saddle_product_match_oracle(s_table, dyn):
+    gpu, cpu = make_pair(3, 40.0, s_table, dynamic_phase=dyn[0], dynamic_angle=dyn[1])
+    with gpu:
+        gpu.initial_guess(0)
+        cpu.initial_guess(0)
+        assert gpu.size == cpu.size
+        rng = np.random.default_rng(11)
+        for _ in range(2):
+            v = rng.standard_normal(gpu.size)
+            np.testing.assert_allclose(gpu.apply_preconditioner_new(v), cpu.precond(v), rtol=1e-10, atol=1e-10)
+            got = gpu.system_matrix_mult_new(v)
+            ref = cpu.matvec(v)
+            assert oracle.rel_l2(got, ref) <= 1e-5
+
+
+def test_write_generalised_forces_run_matches_reference_table():
+    # One filament, prescribed phase speed, 300 steps: the reference's own generalised-force table
+    # (written in FP32 with GMRES tolerance 1e-4) to 1e-4 relative L2.
+    qp, qa = write_generalised_forces_run(_lib.CF_BEAT_FULFORD_BLAKE, nseg=20, seg_sep=2.6, steps=300, tol=1e-8)
+    assert np.linalg.norm(qp - GOLD["fb_phase"]) / np.linalg.norm(GOLD["fb_phase"]) < 1e-4
+    assert np.linalg.norm(qa - GOLD["fb_angle"]) / np.linalg.norm(GOLD["fb_angle"]) < 1e-4
+
+
+def test_step_solution_satisfies_system_and_matches_oracle(s_table):
+    gpu, cpu = make_pair(4, 20.0, s_table, seed=3)
+    with gpu:
+        res = gpu.step(0)
+        it_cpu, rel_cpu = cpu.step(0)
+        assert res.status == _lib.CF_OK and res.relative_residual <= 1e-6
+        st = gpu.state()
+        # the converged phase/angle rates agree with the oracle's FP64 GMRES to the solver tolerance
+        np.testing.assert_allclose(st["phase_dot"], cpu.phase_dot, rtol=5e-5, atol=1e-5)
+        np.testing.assert_allclose(st["angle_dot"], cpu.angle_dot, rtol=5e-5, atol=1e-5)
+        # true FP64 residual of the GPU solution against the oracle operator
+        _, fs = gpu.segments()
+        sol = np.concatenate([fs.reshape(-1, 6)[:, :3].astype(np.float64).ravel(), st["phase_dot"], st["angle_dot"]])
+        r = cpu.assemble_rhs() - cpu.matvec(sol)
+        assert np.linalg.norm(r) / np.linalg.norm(cpu.assemble_rhs()) < 2e-5
+        assert abs(res.iterations - it_cpu) <= max(3, 0.2 * it_cpu)
+
+
+@pytest.mark.parametrize("spacing,steps,tip_tol", [(60.0, 300, 1e-3), (20.0, 60, 1e-2)])
+def test_tip_trajectories_match_oracle(s_table, spacing, steps, tip_tol):
+    # 16 cilia x 20 segments; tips after `steps` implicit steps at GMRES tolerance 1e-6.
+    gpu, cpu = make_pair(4, spacing, s_table, seed=5)
+    L = 2.6 * 19
+    with gpu:
+        worst = 0.0
+        for nt in range(steps):
+            gpu.step(nt)
+            cpu.step(nt)
+            if nt % 30 == 29 or nt == steps - 1:
+                worst = max(worst, np.abs(gpu.tips() - cpu.tips()).max() / L)
+        assert worst < tip_tol, worst
+
+
+def test_async_steps_equal_sync_steps(s_table):
+    g1, _ = make_pair(4, 20.0, s_table, seed=9)
+    g2, _ = make_pair(4, 20.0, s_table, seed=9)
+    with g1, g2:
+        for nt in range(5):
+            g1.step(nt)
+            g2.step_async(nt)
+        g2.last_solve()
+        np.testing.assert_array_equal(g1.tips(), g2.tips())
+        np.testing.assert_array_equal(g1.state()["phase"], g2.state()["phase"])
+
+
+def test_zero_rhs_gives_zero_solution():
+    # prescribed phase speed 0 and no dynamic unknowns: RHS = 0 -> lambda = 0 (mobility_solver.cpp:2222-2290)
+    with WallCiliaSimulation(bases=[[0, 0, 1.3], [30, 0, 1.3]], dynamic_phase=False, dynamic_angle=False,
+                             omega0=[0.0, 0.0]) as gpu:
+        res = gpu.step(0)
+        _, fs = gpu.segments()
+        assert res.iterations == 0 and np.all(fs == 0.0)
