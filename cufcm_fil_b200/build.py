@@ -23,6 +23,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fvisibility=hidden"]
 LINK_LIBS = ["-lcufft", "-lcuda"]
+# The FP32 pair kernels: flush denormals and use the hardware reciprocal / square-root
+# approximations (positions and forces are O(1e-3..1e3); the sums are checked against FP64).
+PER_FILE_FLAGS = {"rpy_kernels.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]}
 
 
 def nvcc() -> str:
@@ -50,7 +53,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         stale = force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header)
         if not stale:
             continue
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *PER_FILE_FLAGS.get(src.name, []), "-I", str(INCLUDE), "-c", str(src),
+               "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

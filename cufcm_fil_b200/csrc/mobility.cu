@@ -196,8 +196,9 @@ extern "C" int cf_mobility_create(const cf_mobility_config *cfg, cf_mobility **o
             break;
         // Partials buffer: the largest of the four block products' plans.
         const int sd = cfg->seg_dof, n_s = cfg->n_seg, n_b = cfg->n_blob;
-        const RpyPlan plans[4] = {rpy_plan(n_s, n_s, sd, sd, h->num_sms), rpy_plan(n_s, n_b, sd, 3, h->num_sms),
-                                  rpy_plan(n_b, n_b, 3, 3, h->num_sms), rpy_plan(n_b, n_s, 3, sd, h->num_sms)};
+        const RpyPlan plans[6] = {rpy_plan(n_s, n_s, sd, sd, h->num_sms), rpy_plan(n_s, n_b, sd, 3, h->num_sms),
+                                  rpy_plan(n_b, n_b, 3, 3, h->num_sms), rpy_plan(n_b, n_s, 3, sd, h->num_sms),
+                                  rpy_plan_sym(n_s, h->num_sms), rpy_plan_sym(n_b, h->num_sms)};
         h->scratch_cap = 1;
         for (const RpyPlan &pl : plans) h->scratch_cap = std::max(h->scratch_cap, pl.scratch_float4);
         if ((rc = dalloc(&h->scratch, h->scratch_cap))) break;

@@ -22,6 +22,8 @@ constexpr int kThreads = 128;
 constexpr int kMaxSplit = 2048;   // sources staged per CTA (<= 96 KB with torques)
 constexpr int kMinSplit = 64;     // keep each split long enough to amortise staging
 constexpr int kBlockSum = 64;     // sources per FP32 block sum before TwoSum
+constexpr int kCtasPerSm = 8;     // launch bound: 8 x 128 threads x 64 registers = one SM's file
+constexpr int kStageCost = 24;    // per-CTA staging/epilogue cost in units of one source
 
 struct TileParams {
     const float4 *xt;
@@ -88,7 +90,7 @@ __device__ __forceinline__ void tile_sum(const float4 *__restrict__ xs_s, const 
 // grid: (tiles, nsplit); block: 128.  SELF: targets and sources are the same
 // particle set (wall mode skips j == i here; the reduction adds the self block).
 template <bool WALL, int VD, int FD, int TI, bool SELF>
-__global__ void __launch_bounds__(kThreads) rpy_tile_kernel(TileParams p) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_tile_kernel(TileParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
     float4 *xs_s = reinterpret_cast<float4 *>(smem_raw + 16);
@@ -158,7 +160,100 @@ __global__ void __launch_bounds__(kThreads) rpy_tile_kernel(TileParams p) {
             o.y = hi[k][3 * w + 1] + lo[k][3 * w + 1];
             o.z = hi[k][3 * w + 2] + lo[k][3 * w + 2];
             o.w = 0.0f;
-            p.partial[(static_cast<size_t>(blockIdx.y) * W + w) * p.ntp + i] = o;
+            p.partial[(static_cast<size_t>(i) * gridDim.y + blockIdx.y) * W + w] = o;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric wall kernel for the segment-segment block (targets == sources, 3x3).
+// The grand mobility is symmetric, so each unordered pair is evaluated once and
+// applied in both directions (wall_pair_sym_f32).  Work unit: one warp and one
+// pair of 32-particle tiles (I <= J) of the upper triangle.  The warp's lanes
+// own the 32 targets of tile I; the 32 sources of tile J, with the accumulators
+// of their own velocities, rotate around the warp by one lane per step, so after
+// 32 steps every lane has met every source and every source accumulator is back
+// in its home lane.  Diagonal tiles are evaluated one-sided (j != i).  Each
+// target receives exactly one partial per tile, written to
+// partial[i * nb + tile] -- no atomics, deterministic.
+struct SymParams {
+    const float4 *x;
+    const float4 *f;
+    float4 *partial;
+    int n, nb;
+    long long items;
+};
+
+__device__ __forceinline__ void sym_item(long long t, int nb, int &I, int &J) {
+    // t enumerates the upper triangle row by row: row I holds nb - I tiles.
+    const double b = 2.0 * nb + 1.0;
+    int r = static_cast<int>(floor(0.5 * (b - sqrt(fmax(0.0, b * b - 8.0 * static_cast<double>(t))))));
+    r = max(0, min(r, nb - 1));
+    auto start = [nb](long long row) { return row * nb - row * (row - 1) / 2; };
+    while (r + 1 < nb && start(r + 1) <= t) ++r;
+    while (r > 0 && start(r) > t) --r;
+    I = r;
+    J = r + static_cast<int>(t - start(r));
+}
+
+__device__ __forceinline__ void sym_load(const SymParams &p, int idx, int lane, float4 &x, float4 &f) {
+    if (idx < p.n) {
+        x = p.x[idx];
+        f = p.f[idx];
+    } else {
+        // inert padding: far from everything (and from each other), zero force
+        x = make_float4(1.0e5f * static_cast<float>(lane + 1), 0.0f, 1.0e4f, 0.0f);
+        f = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_kernel(SymParams p) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int src_lane = (lane + 1) & 31;
+    const long long nwarps = static_cast<long long>(gridDim.x) * (kThreads / 32);
+    for (long long t = static_cast<long long>(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5); t < p.items;
+         t += nwarps) {
+        int I, J;
+        sym_item(t, p.nb, I, J);
+        const int i = I * 32 + lane;
+        const int j = J * 32 + lane;
+        float4 xi, fi, xs, fs;
+        sym_load(p, i, lane, xi, fi);
+        sym_load(p, j, lane, xs, fs);
+        const float fiv[3] = {fi.x, fi.y, fi.z};
+        float vi[3] = {0.0f, 0.0f, 0.0f};
+        if (I == J) {
+#pragma unroll 1
+            for (int step = 1; step < 32; ++step) {
+                xs.x = __shfl_sync(full, xs.x, src_lane);
+                xs.y = __shfl_sync(full, xs.y, src_lane);
+                xs.z = __shfl_sync(full, xs.z, src_lane);
+                fs.x = __shfl_sync(full, fs.x, src_lane);
+                fs.y = __shfl_sync(full, fs.y, src_lane);
+                fs.z = __shfl_sync(full, fs.z, src_lane);
+                const float fsv[3] = {fs.x, fs.y, fs.z};
+                wall_pair_f32<3, 3>(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, vi);
+            }
+            if (i < p.n) p.partial[static_cast<size_t>(i) * p.nb + I] = make_float4(vi[0], vi[1], vi[2], 0.0f);
+        } else {
+            float vs[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll 2
+            for (int step = 0; step < 32; ++step) {
+                const float fsv[3] = {fs.x, fs.y, fs.z};
+                wall_pair_sym_f32(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, fiv, vi, vs);
+                xs.x = __shfl_sync(full, xs.x, src_lane);
+                xs.y = __shfl_sync(full, xs.y, src_lane);
+                xs.z = __shfl_sync(full, xs.z, src_lane);
+                fs.x = __shfl_sync(full, fs.x, src_lane);
+                fs.y = __shfl_sync(full, fs.y, src_lane);
+                fs.z = __shfl_sync(full, fs.z, src_lane);
+                vs[0] = __shfl_sync(full, vs[0], src_lane);
+                vs[1] = __shfl_sync(full, vs[1], src_lane);
+                vs[2] = __shfl_sync(full, vs[2], src_lane);
+            }
+            if (i < p.n) p.partial[static_cast<size_t>(i) * p.nb + J] = make_float4(vi[0], vi[1], vi[2], 0.0f);
+            if (j < p.n) p.partial[static_cast<size_t>(j) * p.nb + I] = make_float4(vs[0], vs[1], vs[2], 0.0f);
         }
     }
 }
@@ -170,23 +265,33 @@ struct ReduceParams {
     int nsplit, nt, ntp, stride, mode;
 };
 
+// One warp per target: the lanes stride over the target's partials, FP64
+// shuffle reduction (fixed order, deterministic), lane 0 adds the wall self
+// block and writes or accumulates the result.
 template <bool WALL_SELF, int VD, int FD>
 __global__ void rpy_reduce_kernel(ReduceParams p) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.nt) return;
     constexpr int W = VD / 3;
     double v[VD];
 #pragma unroll
     for (int c = 0; c < VD; ++c) v[c] = 0.0;
-    for (int s = 0; s < p.nsplit; ++s) {
+    const float4 *pt = p.partial + static_cast<size_t>(i) * p.nsplit * W;
+    for (int s = lane; s < p.nsplit; s += 32) {
 #pragma unroll
         for (int w = 0; w < W; ++w) {
-            const float4 q = p.partial[(static_cast<size_t>(s) * W + w) * p.ntp + i];
+            const float4 q = pt[s * W + w];
             v[3 * w + 0] += q.x;
             v[3 * w + 1] += q.y;
             v[3 * w + 2] += q.z;
         }
     }
+#pragma unroll
+    for (int c = 0; c < VD; ++c)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+    if (lane != 0) return;
     if constexpr (WALL_SELF) {
         const float4 f4 = p.ft[i];
         float f[6] = {f4.x, f4.y, f4.z, 0.f, 0.f, 0.f};
@@ -283,8 +388,8 @@ int dispatch_dof(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, in
 
 template <bool WS, int VD, int FD>
 int launch_reduce_t(const ReduceParams &p, cudaStream_t st) {
-    const int threads = 128;
-    const int blocks = (p.nt + threads - 1) / threads;
+    const int threads = 256;  // 8 targets per block
+    const int blocks = (p.nt + 7) / 8;
     rpy_reduce_kernel<WS, VD, FD><<<blocks, threads, 0, st>>>(p);
     CF_CHECK_LAUNCH("rpy_reduce_kernel");
     return CF_OK;
@@ -292,24 +397,61 @@ int launch_reduce_t(const ReduceParams &p, cudaStream_t st) {
 
 }  // namespace
 
+RpyPlan rpy_plan_sym(int n, int num_sms) {
+    RpyPlan pl{};
+    pl.sym = 1;
+    pl.ti = 1;
+    const int nb = std::max(1, (n + 31) / 32);
+    pl.nb = nb;
+    pl.items = static_cast<long long>(nb) * (nb + 1) / 2;
+    const long long max_warps = static_cast<long long>(std::max(1, num_sms)) * kCtasPerSm * (kThreads / 32);
+    const long long per_warp = (pl.items + max_warps - 1) / max_warps;  // balanced: every warp does per_warp items
+    const long long warps = (pl.items + per_warp - 1) / per_warp;
+    pl.grid = static_cast<int>((warps + (kThreads / 32) - 1) / (kThreads / 32));
+    pl.tiles = pl.grid;
+    pl.nsplit = nb;  // partials per target
+    pl.split = 32;
+    pl.smem = 0;
+    pl.scratch_float4 = static_cast<size_t>(nb) * std::max(n, 1);
+    return pl;
+}
+
 RpyPlan rpy_plan(int nt, int ns, int vd, int fd, int num_sms) {
-    RpyPlan pl;
+    // Every CTA does the same work (128*TI targets x `split` sources), so the
+    // kernel time is (waves) x (time of one CTA).  Choose the split count that
+    // minimises waves * (split + staging overhead), with the resident CTA count
+    // per SM bounded by the launch bounds (8) and by shared memory.
+    RpyPlan pl{};
     pl.ti = (vd == 3) ? 2 : 1;
     const int per_cta = kThreads * pl.ti;
     pl.tiles = std::max(1, (nt + per_cta - 1) / per_cta);
-    // Aim for ~8 resident CTAs per SM in one wave.
-    const int want_ctas = std::max(1, num_sms) * 8;
-    int nsplit = std::max(1, (want_ctas + pl.tiles - 1) / pl.tiles);
-    nsplit = std::min(nsplit, std::max(1, ns / kMinSplit));
-    nsplit = std::max(nsplit, (ns + kMaxSplit - 1) / kMaxSplit);
-    nsplit = std::max(nsplit, 1);
-    int split = (ns + nsplit - 1) / nsplit;
-    split = std::max(split, 1);
-    nsplit = std::max(1, (ns + split - 1) / split);
-    pl.nsplit = nsplit;
-    pl.split = split;
-    pl.smem = 16 + static_cast<size_t>(split) * sizeof(float4) * (fd > 3 ? 3 : 2);
-    pl.scratch_float4 = static_cast<size_t>(nsplit) * (vd / 3) * std::max(nt, 1);
+    const int sms = std::max(1, num_sms);
+    const size_t src_bytes = sizeof(float4) * (fd > 3 ? 3 : 2);
+    const int nmin = std::max(1, (ns + kMaxSplit - 1) / kMaxSplit);
+    const int nmax = std::max(nmin, std::min(ns / kMinSplit, 8 * sms));
+    int best_nsplit = nmin;
+    double best_cost = 1e300;
+    for (int cand = nmin; cand <= nmax; ++cand) {
+        const int split = std::max(1, (ns + cand - 1) / cand);
+        const int nsplit = std::max(1, (ns + split - 1) / split);
+        const size_t smem = 16 + static_cast<size_t>(split) * src_bytes;
+        const int cap = std::min<int>(kCtasPerSm, static_cast<int>((227u * 1024u) / (smem + 1024u)));
+        if (cap < 1) continue;
+        const long long slots = static_cast<long long>(sms) * cap;
+        const long long ctas = static_cast<long long>(pl.tiles) * nsplit;
+        const long long waves = (ctas + slots - 1) / slots;
+        // fewer than 4 resident CTAs (16 warps) per SM issues poorly: penalise
+        const double occ = cap >= 4 ? 1.0 : 4.0 / cap;
+        const double cost = static_cast<double>(waves) * (split + kStageCost) * occ;
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best_nsplit = nsplit;
+        }
+    }
+    pl.split = std::max(1, (ns + best_nsplit - 1) / best_nsplit);
+    pl.nsplit = std::max(1, (ns + pl.split - 1) / pl.split);
+    pl.smem = 16 + static_cast<size_t>(pl.split) * src_bytes;
+    pl.scratch_float4 = static_cast<size_t>(pl.nsplit) * (vd / 3) * std::max(nt, 1);
     return pl;
 }
 
@@ -327,6 +469,18 @@ size_t rpy_scratch_float4(int nt_max, int ns_max, int vd, int num_sms) {
 int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, int *dev_err,
                      cudaStream_t st) {
     if (d.nt <= 0) return CF_OK;
+    if (plan.sym) {
+        SymParams p;
+        p.x = d.xs;
+        p.f = d.fs;
+        p.partial = scratch;
+        p.n = d.nt;
+        p.nb = plan.nb;
+        p.items = plan.items;
+        rpy_wall_sym_kernel<<<plan.grid, kThreads, 0, st>>>(p);
+        CF_CHECK_LAUNCH("rpy_wall_sym_kernel");
+        return CF_OK;
+    }
     const bool self = d.self_set != 0;
     if (d.wall) return self ? dispatch_dof<true, true>(d, plan, scratch, dev_err, st)
                             : dispatch_dof<true, false>(d, plan, scratch, dev_err, st);
@@ -335,6 +489,7 @@ int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch
 }
 
 int rpy_prepare(const RpyBlockDesc &d, const RpyPlan &plan) {
+    if (plan.sym) return CF_OK;  // no dynamic shared memory
     const bool self = d.self_set != 0;
     if (d.wall && self) {
         if (d.vd == 3 && d.fd == 3) return plan.ti == 2 ? configure_tiles_t<true, 3, 3, 2, true>() : configure_tiles_t<true, 3, 3, 1, true>();
@@ -379,10 +534,16 @@ int pack_ft6_to_float4(const float *aos6, float4 *force, float4 *torque, int n, 
     return CF_OK;
 }
 
+RpyPlan rpy_plan_for(const RpyBlockDesc &d, int num_sms) {
+    if (d.wall && d.self_set && d.vd == 3 && d.fd == 3 && d.nt == d.ns && d.xt == d.xs)
+        return rpy_plan_sym(d.nt, num_sms);
+    return rpy_plan(d.nt, d.ns, d.vd, d.fd, num_sms);
+}
+
 int rpy_block_product(const RpyBlockDesc &d, float4 *scratch, size_t scratch_cap, int *dev_err, float *out_f,
                       int stride, int mode, int num_sms, cudaStream_t st) {
     if (d.nt <= 0) return CF_OK;
-    RpyPlan plan = rpy_plan(d.nt, d.ns, d.vd, d.fd, num_sms);
+    RpyPlan plan = rpy_plan_for(d, num_sms);
     if (plan.scratch_float4 > scratch_cap)
         return set_error(CF_EINVAL, "rpy: scratch too small (%zu < %zu float4)", scratch_cap, plan.scratch_float4);
     if (d.ns > 0) CF_TRY(rpy_launch_tiles(d, plan, scratch, dev_err, st));

@@ -10,7 +10,9 @@
 //      in a fixed order (deterministic), adds the wall self block, and writes
 //      or accumulates the result in the caller's layout.
 // The split count is chosen so that the grid fills every SM; the partials
-// buffer (`scratch`) holds nsplit * (VD/3) * nt float4.
+// buffer (`scratch`) holds nt * nsplit * (VD/3) float4, target-major:
+// partial[(i * nsplit + s) * (VD/3) + w], so the splits of one target are
+// contiguous for the reduction.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,6 +36,10 @@ struct RpyBlockDesc {
 };
 
 struct RpyPlan {
+    int sym;       // 1: symmetric warp-tile kernel (wall, segments on segments, 3x3)
+    int nb;        // symmetric: 32-particle tiles
+    long long items;  // symmetric: tile pairs of the upper triangle
+    int grid;      // symmetric: CTAs
     int ti;        // targets per thread
     int tiles;     // target tiles (gridDim.x)
     int nsplit;    // source splits (gridDim.y)
@@ -47,6 +53,10 @@ struct RpyPlan {
 size_t rpy_scratch_float4(int nt_max, int ns_max, int vd, int num_sms);
 
 RpyPlan rpy_plan(int nt, int ns, int vd, int fd, int num_sms);
+// Plan of the symmetric kernel for n particles acting on themselves.
+RpyPlan rpy_plan_sym(int n, int num_sms);
+// The plan rpy_block_product uses for d (symmetric when d allows it).
+RpyPlan rpy_plan_for(const RpyBlockDesc &d, int num_sms);
 
 // Configures the tile-kernel instantiation used by (d, plan) so that later
 // launches may be captured into a CUDA graph.

@@ -247,3 +247,73 @@ __device__ __forceinline__ void free_pair_f32(float dx, float dy, float dz, floa
 }
 
 }  // namespace cufil
+
+namespace cufil {
+
+// Both directions of one wall pair from a single block evaluation.
+//   d = x_i - x_j, hz = z_i + z_j; fj, fi: source forces of j and i.
+//   vi += M(i <- j) fj,  vj += M(j <- i) fi = M(i <- j)^T fi.
+// The grand mobility is symmetric, so the image block is written as
+//   M = c6 [k0 I + a d' d'^T + b d' z^T + c z d'^T + k4 z z^T],  d' = (dx, dy, hz),
+// with the coefficients of the reference's wall branch (cuda_functions.cu:118-150)
+// regrouped: a = alpha w^2, b = beta w, c = gamma w^2 hz (w = 1/|d'|).
+__device__ __forceinline__ void wall_pair_sym_f32(float dx, float dy, float dz, float zi, float zj, const float *fj,
+                                                  const float *fi, float *vi, float *vj) {
+    const float c6 = RpyConst::inv6pi;
+    const float c8 = RpyConst::inv8pi;
+    const float q2 = dx * dx + dy * dy;
+    // free space: M = A I + B d d^T (even in d)
+    const float s = rsqrtf(fmaf(dz, dz, q2));
+    const float s2 = s * s;
+    const float g = c8 * s;
+    const float A = g * fmaf(2.0f / 3.0f, s2, 1.0f);
+    const float B = g * fmaf(-2.0f, s2, 1.0f) * s2;
+    // image system
+    const float hz = zi + zj;
+    const float hz2 = hz * hz;
+    const float w = rsqrtf(q2 + hz2);
+    const float w2 = w * w, w3 = w2 * w, w5 = w3 * w2;
+    const float h = __fdividef(zj, hz);
+    const float hm = 1.0f - h;
+    const float ez2 = w2 * hz2;
+    const float hh = h * hm;
+    const float t5 = fmaf(-5.0f, ez2, 1.0f);
+    const float w075 = 0.75f * w;
+    const float hw15 = 1.5f * h * w;
+    const float k0 = -(w075 * fmaf(2.0f * hh, ez2, 1.0f) + 0.5f * (w3 * fmaf(-3.0f, ez2, 1.0f) - w5 * t5));
+    const float al = -(w075 * fmaf(-6.0f * hh, ez2, 1.0f) - 1.5f * w3 * t5 + 2.5f * w5 * fmaf(-7.0f, ez2, 1.0f));
+    const float be = (hz * w) * (hw15 * fmaf(-6.0f * hm, ez2, 1.0f) - 3.0f * w3 * t5 + 5.0f * w5 * fmaf(-7.0f, ez2, 2.0f));
+    const float ga = hw15 - 5.0f * w5;
+    const float de = -((3.0f * h * h * w + 3.0f * w3) * ez2 + fmaf(-15.0f, ez2, 2.0f) * w5);
+    const float K0 = c6 * k0;
+    const float a = c6 * al * w2;
+    const float b = c6 * be * w;
+    const float c = c6 * ga * w2 * hz;
+    const float e = c6 * de;
+    // i <- j
+    {
+        const float dF = dx * fj[0] + dy * fj[1] + dz * fj[2];
+        const float dpF = dx * fj[0] + dy * fj[1] + hz * fj[2];
+        const float t0 = B * dF;
+        const float t1 = a * dpF + b * fj[2];
+        const float t2 = c * dpF + e * fj[2];
+        const float AK = A + K0;
+        vi[0] += AK * fj[0] + t0 * dx + t1 * dx;
+        vi[1] += AK * fj[1] + t0 * dy + t1 * dy;
+        vi[2] += AK * fj[2] + t0 * dz + t1 * hz + t2;
+    }
+    // j <- i (transpose)
+    {
+        const float dF = dx * fi[0] + dy * fi[1] + dz * fi[2];
+        const float dpF = dx * fi[0] + dy * fi[1] + hz * fi[2];
+        const float t0 = B * dF;
+        const float t1 = a * dpF + c * fi[2];
+        const float t2 = b * dpF + e * fi[2];
+        const float AK = A + K0;
+        vj[0] += AK * fi[0] + t0 * dx + t1 * dx;
+        vj[1] += AK * fi[1] + t0 * dy + t1 * dy;
+        vj[2] += AK * fi[2] + t0 * dz + t1 * hz + t2;
+    }
+}
+
+}  // namespace cufil

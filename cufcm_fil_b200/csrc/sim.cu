@@ -37,7 +37,7 @@ struct cf_sim {
     float4 *partial = nullptr;
     int *err = nullptr;
     int fil_threads = 64;
-    size_t kin_smem = 0, pre_smem = 0;
+    size_t kin_smem = 0, pre_smem = 0, givens_smem = 0;
     int dots_grid = 0, update_grid = 0;
     bool use_graph = true;
     cudaGraph_t graph = nullptr;
@@ -108,7 +108,9 @@ int launch_kinematics(cf_sim *s, cudaStream_t st) {
 
 int launch_matvec_tail(cf_sim *s, const double *v, double *out, cudaStream_t st) {
     CF_TRY(rpy_launch_tiles(s->desc, s->plan, s->partial, s->err, st));
-    saddle_epilogue_kernel<<<s->d.F, s->fil_threads, 0, st>>>(s->d, v, out);
+    const int warps_per_block = 8;
+    saddle_epilogue_kernel<<<(s->d.N + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(
+        s->d, v, out);
     CF_CHECK_LAUNCH("saddle_epilogue_kernel");
     return CF_OK;
 }
@@ -133,13 +135,13 @@ int launch_body(cf_sim *s, cudaGraphConditionalHandle h, cudaStream_t st) {
     CF_CHECK_LAUNCH("update_kernel");
     dots_kernel<<<s->dots_grid, 256, 0, st>>>(s->d, s->d.h2);
     CF_CHECK_LAUNCH("dots_kernel");
-    update_kernel<<<s->update_grid, 256, 0, st>>>(s->d, s->d.h2, 1, h);
+    update_kernel<<<s->update_grid, 256, s->givens_smem, st>>>(s->d, s->d.h2, 1, h);
     CF_CHECK_LAUNCH("update_kernel");
     return CF_OK;
 }
 
 int launch_finish(cf_sim *s, cudaStream_t st) {
-    backsub_kernel<<<1, 32, 0, st>>>(s->d);
+    backsub_kernel<<<1, 256, sizeof(double) * (s->d.max_iter + 1), st>>>(s->d);
     CF_CHECK_LAUNCH("backsub_kernel");
     combine_kernel<<<s->update_grid, 256, 0, st>>>(s->d);
     CF_CHECK_LAUNCH("combine_kernel");
@@ -378,7 +380,7 @@ extern "C" int cf_sim_create(const cf_sim_config *cfg, cf_sim **out) {
         desc.ns = N;
         desc.as = 1.0f;
         desc.mu = 1.0f;
-        s->plan = rpy_plan(N, N, 3, 3, s->num_sms);
+        s->plan = rpy_plan_for(desc, s->num_sms);
         if ((rc = sim_alloc(s, &s->partial, s->plan.scratch_float4))) break;
         d.partial = s->partial;
         d.nsplit = s->plan.nsplit;
@@ -386,10 +388,11 @@ extern "C" int cf_sim_create(const cf_sim_config *cfg, cf_sim **out) {
         s->fil_threads = std::min(256, std::max(64, (3 * ns + 31) / 32 * 32));
         s->kin_smem = sizeof(double) * (2 * (10 * ns + 1) + ns);
         s->pre_smem = sizeof(double) * 3 * ns;
+        s->givens_smem = sizeof(double) * 3 * (d.max_iter + 2);
         d.dots_chunk = 4096;
         d.dots_nchunk = (d.n + d.dots_chunk - 1) / d.dots_chunk;
         s->dots_grid = 2 * s->num_sms;
-        s->update_grid = std::min(4 * s->num_sms, (d.n + 255) / 256);
+        s->update_grid = std::min(8 * s->num_sms, (d.n + 31) / 32);
         if ((rc = sim_alloc(s, &d.dots_partial, (mi + 1) * d.dots_nchunk)) ||
             (rc = sim_alloc(s, &d.norm_partial, std::max(F, std::max(s->update_grid, s->dots_grid)))))
             break;
@@ -398,6 +401,12 @@ extern "C" int cf_sim_create(const cf_sim_config *cfg, cf_sim **out) {
             (rc = cuda_status(cudaMemset(d.H, 0, sizeof(double) * (mi + 2) * (mi + 1)), "cudaMemset", __FILE__,
                               __LINE__)))
             break;
+        if (s->givens_smem > 48 * 1024) {
+            if ((rc = cuda_status(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       static_cast<int>(s->givens_smem)),
+                                  "cudaFuncSetAttribute", __FILE__, __LINE__)))
+                break;
+        }
         if (s->kin_smem > 48 * 1024) {
             if ((rc = cuda_status(cudaFuncSetAttribute(kinematics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        static_cast<int>(s->kin_smem)),
@@ -597,6 +606,8 @@ extern "C" int cf_sim_system_matvec(cf_sim *s, const double *in, double *out) {
     CF_CUDA(cudaMemcpyAsync(s->d.z, in, b, cudaMemcpyHostToDevice, s->stream));
     pack_forces_kernel<<<(s->d.N + 255) / 256, 256, 0, s->stream>>>(s->d, s->d.z);
     CF_CHECK_LAUNCH("pack_forces_kernel");
+    filament_rows_kernel<<<s->d.F, s->fil_threads, 0, s->stream>>>(s->d, s->d.z, s->d.w);
+    CF_CHECK_LAUNCH("filament_rows_kernel");
     CF_TRY(launch_matvec_tail(s, s->d.z, s->d.w, s->stream));
     CF_CUDA(cudaMemcpyAsync(out, s->d.w, b, cudaMemcpyDeviceToHost, s->stream));
     GmresCtl c;

