@@ -83,6 +83,7 @@ SIGNATURES = {
     "cf_evaluate_full_mobility": [_vp],
     "cf_apply_mobility": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "cf_apply_mobility_device": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "cf_rpy_wall_segments_noalloc": [_vp, _vp, _vp, _i, _vp],
     "cf_sim_create": [ctypes.POINTER(SimConfig), ctypes.POINTER(_vp)],
     "cf_sim_destroy": [_vp],
     "cf_sim_step": [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_d)],

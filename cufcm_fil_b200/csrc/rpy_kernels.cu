@@ -417,6 +417,10 @@ RpyPlan rpy_plan_sym(int n, int num_sms) {
 }
 
 RpyPlan rpy_plan(int nt, int ns, int vd, int fd, int num_sms) {
+    return rpy_plan_capped(nt, ns, vd, fd, num_sms, 1 << 30);
+}
+
+RpyPlan rpy_plan_capped(int nt, int ns, int vd, int fd, int num_sms, int max_nsplit) {
     // Every CTA does the same work (128*TI targets x `split` sources), so the
     // kernel time is (waves) x (time of one CTA).  Choose the split count that
     // minimises waves * (split + staging overhead), with the resident CTA count
@@ -428,7 +432,7 @@ RpyPlan rpy_plan(int nt, int ns, int vd, int fd, int num_sms) {
     const int sms = std::max(1, num_sms);
     const size_t src_bytes = sizeof(float4) * (fd > 3 ? 3 : 2);
     const int nmin = std::max(1, (ns + kMaxSplit - 1) / kMaxSplit);
-    const int nmax = std::max(nmin, std::min(ns / kMinSplit, 8 * sms));
+    const int nmax = std::max(nmin, std::min(std::min(ns / kMinSplit, 8 * sms), max_nsplit));
     int best_nsplit = nmin;
     double best_cost = 1e300;
     for (int cand = nmin; cand <= nmax; ++cand) {

@@ -53,6 +53,9 @@ struct RpyPlan {
 size_t rpy_scratch_float4(int nt_max, int ns_max, int vd, int num_sms);
 
 RpyPlan rpy_plan(int nt, int ns, int vd, int fd, int num_sms);
+// Same with at most max_nsplit source splits (bounded partials buffer); the
+// split count never drops below ceil(ns / 2048).
+RpyPlan rpy_plan_capped(int nt, int ns, int vd, int fd, int num_sms, int max_nsplit);
 // Plan of the symmetric kernel for n particles acting on themselves.
 RpyPlan rpy_plan_sym(int n, int num_sms);
 // The plan rpy_block_product uses for d (symmetric when d allows it).

@@ -121,6 +121,21 @@ CF_API int cf_apply_mobility_device(cf_mobility *h, const float *d_x_segs, const
                              const float *d_f_segs, const float *d_f_blobs,
                              float *d_v_segs, float *d_v_blobs, void *stream);
 
+/* Wall segment-segment product V_seg = M_ss F_seg (3-dof segments, the
+ * product of cf_evaluate_segment_segment_mobility with wall = 1, seg_dof = 3)
+ * on device buffers in the AoS layouts above, for callers that cannot allocate
+ * device memory (inside stream capture, or under a host that owns all device
+ * memory through its own allocator).  No counterpart in the reference.  It
+ * allocates nothing: its scratch is a fixed array inside this library (about
+ * 2.3 MB per GPU that loads it, held until the process exits), so n_seg is
+ * limited to 8192 (larger values give CF_EINVAL).  The first call on a device
+ * resolves that array's device address; make it before any stream capture.
+ * Asynchronous on `stream` (NULL: the legacy default stream).  All calls share
+ * the one array, so calls that overlap on the GPU race: serialise them (one
+ * stream, or events). */
+CF_API int cf_rpy_wall_segments_noalloc(const float *d_x_segs, const float *d_f_segs, float *d_v_segs, int n_seg,
+                                        void *stream);
+
 /* ========================================================== simulation ==
  * Generic layer of mobility_solver for prescribed-shape cilia above a no-slip
  * wall (CILIA_TYPE 3, BODY_OR_SURFACE_TYPE 0, MOBILITY_TYPE 1,
