@@ -150,24 +150,34 @@ def barrier(world):
         torch.cuda.synchronize()
 
 
-def max_over_ranks(world, value):
+def _reduce(world, value, op):
     if world == 1:
-        return value
+        return float(value)
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(world, value):
+    """Timing of a multi-rank run: the slowest rank's device time."""
+    import torch.distributed as dist
+    return _reduce(world, value, dist.ReduceOp.MAX if world > 1 else None)
 
 
 def sum_over_ranks(world, value):
-    if world == 1:
-        return value
-    import torch
+    """Whole-job work: every rank runs its own replica."""
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(world, value, dist.ReduceOp.SUM if world > 1 else None)
+
+
+def replica_throughput(world, steps_per_rank, rank_ms):
+    """value = (steps of all ranks) / (slowest rank's time), the weak-scaling aggregate."""
+    total_steps = sum_over_ranks(world, steps_per_rank)
+    slowest_ms = max_over_ranks(world, rank_ms)
+    return total_steps / (slowest_ms / 1e3), slowest_ms
 
 
 # ----------------------------------------------------------------------- ours
@@ -211,9 +221,8 @@ def run_ours(args):
     res = sim.last_solve()
     iters = sim.iteration_log(4096)[[i % 4096 for i in range(first_nt, nt)]]
     launches = int(sum(sim.launches_per_step(int(i)) for i in iters))
-    max_ms = max_over_ranks(world, total_ms)
+    value, max_ms = replica_throughput(world, float(args.steps), total_ms)
     steps_all = sum_over_ranks(world, float(args.steps))
-    value = steps_all / (max_ms / 1e3)
 
     # ---- end to end through the host API: state up from pinned memory, step, results down
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64)).pin_memory()
