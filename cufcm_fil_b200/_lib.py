@@ -59,6 +59,12 @@ class SimConfig(ctypes.Structure):
                 ("s_tol_factor", ctypes.c_double), ("device", ctypes.c_int)]
 
 
+class FcmConfig(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("rh", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+                ("eta", ctypes.c_double), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("boxsize", ctypes.c_double), ("device", ctypes.c_int)]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _d = ctypes.c_double
@@ -84,6 +90,12 @@ SIGNATURES = {
     "cf_apply_mobility": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "cf_apply_mobility_device": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "cf_rpy_wall_segments_noalloc": [_vp, _vp, _vp, _i, _vp],
+    "cf_fcm_create": [ctypes.POINTER(FcmConfig), ctypes.POINTER(_vp)],
+    "cf_fcm_destroy": [_vp],
+    "cf_fcm_apply": [_vp, _vp, _vp, _vp],
+    "cf_fcm_apply_device": [_vp, _vp, _vp, _vp, _vp],
+    "cf_fcm_apply_segments_blobs": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp],
+    "cf_fcm_info": [_vp, _vp],
     "cf_sim_create": [ctypes.POINTER(SimConfig), ctypes.POINTER(_vp)],
     "cf_sim_destroy": [_vp],
     "cf_sim_step": [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_d)],

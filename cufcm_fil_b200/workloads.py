@@ -57,3 +57,16 @@ def fibonacci_sphere(n: int, radius: float, centre=(0.0, 0.0, 0.0)) -> np.ndarra
 def random_forces(n: int, dof: int, seed: int) -> np.ndarray:
     """Forces (and torques) i.i.d. N(0,1), [n, dof]."""
     return np.random.default_rng(seed).standard_normal((n, dof))
+
+
+def sphere_with_cilia(n_cilia: int = 1000, nseg: int = 20, n_body: int = 10000, radius: float = 100.0,
+                      seg_sep: float = 2.2, centre=(512.0, 512.0, 512.0)):
+    """Spherical body of `radius` with `n_body` blobs on a Fibonacci sphere and `n_cilia`
+    straight radial cilia of `nseg` segments (first segment seg_sep outside the surface).
+    Returns (segment centres [n_cilia*nseg, 3], blob centres [n_body, 3])."""
+    c = np.asarray(centre, float)
+    blobs = fibonacci_sphere(n_body, radius, c)
+    dirs = fibonacci_sphere(n_cilia, 1.0)
+    k = np.arange(1, nseg + 1)[None, :, None]
+    segs = c + dirs[:, None, :] * (radius + seg_sep * k)
+    return segs.reshape(-1, 3), blobs

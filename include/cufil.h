@@ -136,6 +136,38 @@ CF_API int cf_apply_mobility_device(cf_mobility *h, const float *d_x_segs, const
 CF_API int cf_rpy_wall_segments_noalloc(const float *d_x_segs, const float *d_f_segs, float *d_v_segs, int n_seg,
                                         void *stream);
 
+/* ================================================================ fcm ==
+ * Fast force-coupling method in a triply periodic box: the reference's cuFCM
+ * FCM_solver (src/cufcm/CUFCM_SOLVER.cu:20-727) for translating particles
+ * (ROTATION 0): spread -> FFT Stokes solve -> gather + near-field and self
+ * corrections.  Positions, forces and velocities are [3N] AoS float arrays. */
+typedef struct cf_fcm cf_fcm;
+
+typedef struct cf_fcm_config {
+    int n;                    /* particles N */
+    double rh;                /* hydrodynamic radius; FCM width sigma = rh/sqrt(pi) */
+    double alpha, beta, eta;  /* grid Gaussian Sigma = alpha*dx, support ngd = round(alpha*beta) (<= 32),
+                                 correction radius Rc = eta*alpha*dx (simulation_info keys) */
+    int nx, ny, nz;           /* FFT grid (nx even) */
+    double boxsize;           /* Lx; Ly = boxsize*ny/nx, Lz = boxsize*nz/nx */
+    int device;
+} cf_fcm_config;
+
+/* FCM_solver::FCM_solver: derived parameters, buffers, cuFFT plans (CUFCM_SOLVER.cu:20-248) */
+CF_API int cf_fcm_create(const cf_fcm_config *cfg, cf_fcm **out);
+CF_API int cf_fcm_destroy(cf_fcm *h);
+/* FCM_solver::hydrodynamic_solver on host arrays (synchronous) */
+CF_API int cf_fcm_apply(cf_fcm *h, const float *Y, const float *F, float *V);
+/* Same on device arrays, ordered after the work already on `stream` (NULL: legacy default stream). */
+CF_API int cf_fcm_apply_device(cf_fcm *h, const float *d_Y, const float *d_F, float *d_V, void *stream);
+/* fcm_mobility_solver::evaluate_full_mobility (fcm_mobility_solver.cu:463-502): the first n_seg particles are
+ * segments (x_segs [3n_seg], f_segs [6n_seg] of which the forces are used, v_segs [6n_seg] with zero angular
+ * slots), the rest blobs (x_blobs, f_blobs, v_blobs [3(N-n_seg)]). */
+CF_API int cf_fcm_apply_segments_blobs(cf_fcm *h, int n_seg, const float *x_segs, const float *x_blobs,
+                                       const float *f_segs, const float *f_blobs, float *v_segs, float *v_blobs);
+/* Derived parameters: [ngd, dx, sigma, Sigma, Rc, Mx, My, Mz, self mobility] */
+CF_API int cf_fcm_info(cf_fcm *h, double *info);
+
 /* ========================================================== simulation ==
  * Generic layer of mobility_solver for prescribed-shape cilia above a no-slip
  * wall (CILIA_TYPE 3, BODY_OR_SURFACE_TYPE 0, MOBILITY_TYPE 1,

@@ -12,6 +12,9 @@ include guard turns the original into a no-op.  Outputs (headers, objects,
 the built libraries travel with the tree so GPU tests can run them where the
 reference sources are absent.
 
+It also builds the reference's cuFCM solver (src/cufcm/*.cu, float, translation
+only as configured) with ref_fcm_wrapper.cu into oracle/_ref/libref_fcm.so.
+
 Variants (switches of config.hpp):
   wall3  CILIA_TYPE 3 (prescribed), BODY_OR_SURFACE_TYPE 0 (wall)  -- as mounted
   wall6  CILIA_TYPE 0 (6-dof segments), BODY_OR_SURFACE_TYPE 0
@@ -58,6 +61,35 @@ def available() -> bool:
     return (REF_ROOT / "src" / "cilia" / "cuda_functions.cu").exists()
 
 
+FCM_SOURCES = ["CUFCM_SOLVER.cu", "CUFCM_FCM.cu", "CUFCM_CORRECTION.cu", "CUFCM_DATA.cu", "CUFCM_CELLLIST.cu",
+               "CUFCM_RANDOMPACKER.cu"]
+FCM_WRAPPER = HERE / "ref_fcm_wrapper.cu"
+
+
+def fcm_lib_path() -> Path:
+    return OUT / "libref_fcm.so"
+
+
+def build_fcm(verbose: bool = False, force: bool = False) -> Path | None:
+    """The reference's cuFCM (src/cufcm, float build, ROTATION 0 as configured) with ref_fcm_wrapper.cu."""
+    src_dir = REF_ROOT / "src" / "cufcm"
+    if not (src_dir / "CUFCM_SOLVER.cu").exists():
+        return None
+    OUT.mkdir(exist_ok=True)
+    lib = fcm_lib_path()
+    srcs = [FCM_WRAPPER] + [src_dir / f for f in FCM_SOURCES]
+    newest = max(p.stat().st_mtime for p in srcs)
+    if force or not lib.exists() or lib.stat().st_mtime < newest:
+        nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+        cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-w", "-Xcompiler", "-fPIC",
+               "-shared", "-I", str(src_dir), *map(str, srcs), "-lcufft", "-lcurand", "-o", str(lib) + ".tmp"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(str(lib) + ".tmp", lib)
+    return lib
+
+
 def build(verbose: bool = False, force: bool = False) -> list[Path]:
     """Builds every variant; a no-op returning [] when the reference tree is absent."""
     if not available():
@@ -83,6 +115,9 @@ def build(verbose: bool = False, force: bool = False) -> list[Path]:
             subprocess.run(cmd, check=True)
             os.replace(str(lib) + ".tmp", lib)
         built.append(lib)
+    fcm = build_fcm(verbose, force)
+    if fcm is not None:
+        built.append(fcm)
     return built
 
 
