@@ -96,6 +96,8 @@ SIGNATURES = {
     "cf_fcm_apply_device": [_vp, _vp, _vp, _vp, _vp],
     "cf_fcm_apply_segments_blobs": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp],
     "cf_fcm_info": [_vp, _vp],
+    "cf_fcm_set_timing": [_vp, _i],
+    "cf_fcm_stage_times": [_vp, _vp],
     "cf_sim_create": [ctypes.POINTER(SimConfig), ctypes.POINTER(_vp)],
     "cf_sim_destroy": [_vp],
     "cf_sim_step": [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_d)],

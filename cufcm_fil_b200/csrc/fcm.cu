@@ -47,6 +47,9 @@ struct cf_fcm {
     size_t sort_tmp_bytes = 0;
     cufftHandle plan_fwd = 0, plan_inv = 0;
     bool have_fwd = false, have_inv = false;
+    // optional per-stage timing: events between stages of the last apply
+    bool timing = false;
+    cudaEvent_t ev[7] = {};
 };
 
 namespace cufil {
@@ -348,7 +351,13 @@ int fcm_run(cf_fcm *h, const float *dY, const float *dF, float *dV, cudaStream_t
     const fcmk::Params p = params_of(h);
     const int N = h->N;
     const int tb = 128, nb = (N + tb - 1) / tb, wb = (N + 3) / 4;
+    auto mark = [&](int i) -> int {
+        if (h->timing) CF_CUDA(cudaEventRecord(h->ev[i], st));
+        return CF_OK;
+    };
+    CF_TRY(mark(0));
     CF_CUDA(cudaMemsetAsync(h->grid, 0, sizeof(float) * 3 * h->grid_size, st));
+    CF_TRY(mark(1));
     fcmk::prep_kernel<<<nb, tb, 0, st>>>(p, dY, h->x4, h->keys, h->vals);
     CF_CHECK_LAUNCH("fcm prep_kernel");
     size_t tmp = h->sort_tmp_bytes;
@@ -360,18 +369,23 @@ int fcm_run(cf_fcm *h, const float *dY, const float *dF, float *dV, cudaStream_t
     CF_CUDA(cudaMemsetAsync(h->cell_end, 0, sizeof(int) * h->ncell, st));
     fcmk::cell_bounds_kernel<<<nb, tb, 0, st>>>(p, h->keys_sorted, h->cell_start, h->cell_end);
     CF_CHECK_LAUNCH("fcm cell_bounds_kernel");
+    CF_TRY(mark(2));
     fcmk::spread_kernel<<<wb, 128, 0, st>>>(p, h->xs, h->fs, h->grid);
     CF_CHECK_LAUNCH("fcm spread_kernel");
+    CF_TRY(mark(3));
     CF_TRY(cufft_status(cufftExecR2C(h->plan_fwd, h->grid, h->spec), "cufftExecR2C"));
     const size_t sb = (h->fft_size + 255) / 256;
     fcmk::stokes_kernel<<<static_cast<unsigned>(sb), 256, 0, st>>>(p, h->spec);
     CF_CHECK_LAUNCH("fcm stokes_kernel");
     CF_TRY(cufft_status(cufftExecC2R(h->plan_inv, h->spec, h->grid), "cufftExecC2R"));
+    CF_TRY(mark(4));
     fcmk::gather_kernel<<<wb, 128, 0, st>>>(p, h->xs, h->grid, h->vgs);
     CF_CHECK_LAUNCH("fcm gather_kernel");
+    CF_TRY(mark(5));
     fcmk::correction_kernel<<<nb, tb, 0, st>>>(p, h->xs, h->fs, h->keys_sorted, h->cell_start, h->cell_end, h->vgs,
                                                h->perm, dV);
     CF_CHECK_LAUNCH("fcm correction_kernel");
+    CF_TRY(mark(6));
     return CF_OK;
 }
 
@@ -471,6 +485,8 @@ extern "C" int cf_fcm_destroy(cf_fcm *h) {
     if (!h) return CF_OK;
     cudaSetDevice(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : h->ev)
+        if (e) cudaEventDestroy(e);
     if (h->have_fwd) cufftDestroy(h->plan_fwd);
     if (h->have_inv) cufftDestroy(h->plan_inv);
     for (void *p : {(void *)h->grid, (void *)h->spec, (void *)h->x4, (void *)h->xs, (void *)h->fs, (void *)h->ys,
@@ -558,5 +574,25 @@ extern "C" int cf_fcm_info(cf_fcm *h, double *info) {
     info[6] = h->My;
     info[7] = h->Mz;
     info[8] = h->self_mob;
+    return CF_OK;
+}
+
+extern "C" int cf_fcm_set_timing(cf_fcm *h, int enable) {
+    clear_error();
+    CF_REQUIRE(h, "cf_fcm_set_timing: null handle");
+    CF_CUDA(cudaSetDevice(h->cfg.device));
+    if (enable && !h->ev[0])
+        for (cudaEvent_t &e : h->ev) CF_CUDA(cudaEventCreate(&e));
+    h->timing = enable != 0;
+    return CF_OK;
+}
+
+extern "C" int cf_fcm_stage_times(cf_fcm *h, float *ms) {
+    clear_error();
+    CF_REQUIRE(h && ms, "cf_fcm_stage_times: null argument");
+    CF_REQUIRE(h->timing, "cf_fcm_stage_times: timing is off (cf_fcm_set_timing)");
+    CF_CUDA(cudaSetDevice(h->cfg.device));
+    CF_CUDA(cudaEventSynchronize(h->ev[6]));
+    for (int i = 0; i < 6; ++i) CF_CUDA(cudaEventElapsedTime(&ms[i], h->ev[i], h->ev[i + 1]));
     return CF_OK;
 }

@@ -258,6 +258,77 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_kernel(SymP
     }
 }
 
+// ---------------------------------------------------------------------------
+// Batched form of the symmetric wall kernel: many independent particle sets
+// (arrays) in one launch.  Work items of all arrays are concatenated; a warp
+// finds its array by binary search over the arrays' first items.  Arrays whose
+// `active` flag is 0 are skipped (converged GMRES systems).
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_batch_kernel(SymBatchParams p) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int src_lane = (lane + 1) & 31;
+    const long long nwarps = static_cast<long long>(gridDim.x) * (kThreads / 32);
+    for (long long t = static_cast<long long>(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5); t < p.items;
+         t += nwarps) {
+        int lo = 0, hi = p.B - 1;  // last array whose first item <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (p.item0[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const int b = lo;
+        if (p.active && !p.active[b]) continue;
+        const int nb = p.nb[b];
+        SymParams q;
+        q.x = p.x + p.seg0[b];
+        q.f = p.f + p.seg0[b];
+        q.partial = p.partial + p.poff[b];
+        q.n = p.n[b];
+        q.nb = nb;
+        int I, J;
+        sym_item(t - p.item0[b], nb, I, J);
+        const int i = I * 32 + lane;
+        const int j = J * 32 + lane;
+        float4 xi, fi, xs, fs;
+        sym_load(q, i, lane, xi, fi);
+        sym_load(q, j, lane, xs, fs);
+        const float fiv[3] = {fi.x, fi.y, fi.z};
+        float vi[3] = {0.0f, 0.0f, 0.0f};
+        if (I == J) {
+#pragma unroll 1
+            for (int step = 1; step < 32; ++step) {
+                xs.x = __shfl_sync(full, xs.x, src_lane);
+                xs.y = __shfl_sync(full, xs.y, src_lane);
+                xs.z = __shfl_sync(full, xs.z, src_lane);
+                fs.x = __shfl_sync(full, fs.x, src_lane);
+                fs.y = __shfl_sync(full, fs.y, src_lane);
+                fs.z = __shfl_sync(full, fs.z, src_lane);
+                const float fsv[3] = {fs.x, fs.y, fs.z};
+                wall_pair_f32<3, 3>(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, vi);
+            }
+            if (i < q.n) q.partial[static_cast<size_t>(i) * nb + I] = make_float4(vi[0], vi[1], vi[2], 0.0f);
+        } else {
+            float vs[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll 2
+            for (int step = 0; step < 32; ++step) {
+                const float fsv[3] = {fs.x, fs.y, fs.z};
+                wall_pair_sym_f32(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, fiv, vi, vs);
+                xs.x = __shfl_sync(full, xs.x, src_lane);
+                xs.y = __shfl_sync(full, xs.y, src_lane);
+                xs.z = __shfl_sync(full, xs.z, src_lane);
+                fs.x = __shfl_sync(full, fs.x, src_lane);
+                fs.y = __shfl_sync(full, fs.y, src_lane);
+                fs.z = __shfl_sync(full, fs.z, src_lane);
+                vs[0] = __shfl_sync(full, vs[0], src_lane);
+                vs[1] = __shfl_sync(full, vs[1], src_lane);
+                vs[2] = __shfl_sync(full, vs[2], src_lane);
+            }
+            if (i < q.n) q.partial[static_cast<size_t>(i) * nb + J] = make_float4(vi[0], vi[1], vi[2], 0.0f);
+            if (j < q.n) q.partial[static_cast<size_t>(j) * nb + I] = make_float4(vs[0], vs[1], vs[2], 0.0f);
+        }
+    }
+}
+
 struct ReduceParams {
     const float4 *partial;
     const float4 *xt, *ft, *tt;  // self block inputs (wall, self set)
@@ -553,5 +624,18 @@ int rpy_block_product(const RpyBlockDesc &d, float4 *scratch, size_t scratch_cap
     if (d.ns > 0) CF_TRY(rpy_launch_tiles(d, plan, scratch, dev_err, st));
     return rpy_launch_reduce_f32(d, plan, scratch, out_f, stride, mode, st);
 }
+
+}  // namespace cufil
+
+namespace cufil {
+
+int rpy_launch_sym_batch(const SymBatchParams &p, int grid, cudaStream_t st) {
+    if (p.items <= 0) return CF_OK;
+    rpy_wall_sym_batch_kernel<<<grid, kThreads, 0, st>>>(p);
+    CF_CHECK_LAUNCH("rpy_wall_sym_batch_kernel");
+    return CF_OK;
+}
+
+int rpy_sym_batch_max_grid(int num_sms) { return std::max(1, num_sms) * kCtasPerSm; }
 
 }  // namespace cufil

@@ -69,6 +69,24 @@ int rpy_prepare(const RpyBlockDesc &d, const RpyPlan &plan);
 int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, int *dev_err,
                      cudaStream_t st);
 
+// Batched symmetric wall products (segments on segments, 3x3) of B independent
+// particle sets stored back to back.  Per array b: particles [seg0[b], seg0[b]+n[b])
+// of x/f, nb[b] = ceil(n[b]/32) tiles, partials at partial + poff[b] laid out
+// [i * nb[b] + tile], and work items [item0[b], item0[b+1]) (item0[B] == items).
+struct SymBatchParams {
+    const float4 *x;
+    const float4 *f;
+    float4 *partial;
+    const int *seg0, *n, *nb;
+    const long long *poff, *item0;
+    const int *active;  // may be null: every array active
+    int B;
+    long long items;
+};
+int rpy_launch_sym_batch(const SymBatchParams &p, int grid, cudaStream_t st);
+// Largest useful grid of the batched kernel (one resident wave).
+int rpy_sym_batch_max_grid(int num_sms);
+
 // Output modes of the reduction.
 enum RpyOut : int { kOutWrite = 0, kOutAdd = 1 };
 

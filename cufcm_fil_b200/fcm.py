@@ -53,6 +53,17 @@ class FcmSolver:
         keys = ["ngd", "dx", "sigma", "Sigma", "Rc", "Mx", "My", "Mz", "self_mobility"]
         return dict(zip(keys, out.tolist()))
 
+    STAGES = ("clear", "hash_sort", "spread", "fft_solve", "gather", "correction")
+
+    def set_timing(self, enable: bool = True):
+        _lib.call("cf_fcm_set_timing", self._h, int(bool(enable)))
+
+    def stage_times(self) -> dict:
+        """Milliseconds of each stage of the last apply (timing must be on)."""
+        out = np.zeros(6, np.float32)
+        _lib.call("cf_fcm_stage_times", self._h, _p(out))
+        return dict(zip(self.STAGES, out.tolist()))
+
     def hydrodynamic_solver(self, Y, F) -> np.ndarray:
         """V = M_FCM F for positions Y [N,3] and forces F [N,3] (host arrays)."""
         Y = np.ascontiguousarray(Y, np.float32).ravel()

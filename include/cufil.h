@@ -165,6 +165,11 @@ CF_API int cf_fcm_apply_device(cf_fcm *h, const float *d_Y, const float *d_F, fl
  * slots), the rest blobs (x_blobs, f_blobs, v_blobs [3(N-n_seg)]). */
 CF_API int cf_fcm_apply_segments_blobs(cf_fcm *h, int n_seg, const float *x_segs, const float *x_blobs,
                                        const float *f_segs, const float *f_blobs, float *v_segs, float *v_blobs);
+/* Stage timing with CUDA events (off by default): after an apply, ms[6] =
+ * [grid clear, hash + sort + cell list, spread, FFT + solve + inverse FFT,
+ *  gather, corrections + scatter]. */
+CF_API int cf_fcm_set_timing(cf_fcm *h, int enable);
+CF_API int cf_fcm_stage_times(cf_fcm *h, float *ms);
 /* Derived parameters: [ngd, dx, sigma, Sigma, Rc, Mx, My, Mz, self mobility] */
 CF_API int cf_fcm_info(cf_fcm *h, double *info);
 
