@@ -116,6 +116,25 @@ SIGNATURES = {
     "cf_sim_assemble_rhs": [_vp, _i, _vp],
     "cf_sim_apply_preconditioner": [_vp, _vp, _vp],
     "cf_sim_system_matvec": [_vp, _vp, _vp],
+    "cf_sim_autotune": [_vp, _i, _vp],
+    "cf_sim_set_tuning": [_vp, _vp],
+    "cf_sim_get_tuning": [_vp, _vp],
+    "cf_batch_create": [_vp, _i, ctypes.POINTER(_vp)],
+    "cf_batch_destroy": [_vp],
+    "cf_batch_shape": [_vp, _vp, _vp, _vp, _vp],
+    "cf_batch_step": [_vp, _i, _vp, _vp],
+    "cf_batch_step_async": [_vp, _i],
+    "cf_batch_last_solve": [_vp, _vp, _vp, _vp],
+    "cf_batch_get_state": [_vp, _vp, _vp, _vp, _vp],
+    "cf_batch_set_state": [_vp, _vp, _vp, _vp, _vp],
+    "cf_batch_get_segments": [_vp, _vp],
+    "cf_batch_get_solution": [_vp, _i, _vp],
+    "cf_batch_iteration_log": [_vp, _i, _vp, _i],
+    "cf_batch_stream": [_vp, ctypes.POINTER(_vp)],
+    "cf_batch_launches_per_step": [_vp, _i],
+    "cf_batch_autotune": [_vp, _i, _vp],
+    "cf_batch_set_tuning": [_vp, _vp],
+    "cf_batch_get_tuning": [_vp, _vp],
 }
 _RESTYPES = {"cf_last_error": ctypes.c_char_p}
 

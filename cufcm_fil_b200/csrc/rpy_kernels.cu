@@ -262,7 +262,10 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_kernel(SymP
 // Batched form of the symmetric wall kernel: many independent particle sets
 // (arrays) in one launch.  Work items of all arrays are concatenated; a warp
 // finds its array by binary search over the arrays' first items.  Arrays whose
-// `active` flag is 0 are skipped (converged GMRES systems).
+// `active` flag is 0 are skipped (converged GMRES systems).  Partials are
+// stored slot-major per array, partial[poff + slot * n + i] (slot = the other
+// tile of the pair), so that both these writes and the per-segment reduction
+// that reads them are coalesced.
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_batch_kernel(SymBatchParams p) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -306,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_batch_kerne
                 const float fsv[3] = {fs.x, fs.y, fs.z};
                 wall_pair_f32<3, 3>(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, vi);
             }
-            if (i < q.n) q.partial[static_cast<size_t>(i) * nb + I] = make_float4(vi[0], vi[1], vi[2], 0.0f);
+            if (i < q.n) q.partial[static_cast<size_t>(I) * q.n + i] = make_float4(vi[0], vi[1], vi[2], 0.0f);
         } else {
             float vs[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll 2
@@ -323,8 +326,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_batch_kerne
                 vs[1] = __shfl_sync(full, vs[1], src_lane);
                 vs[2] = __shfl_sync(full, vs[2], src_lane);
             }
-            if (i < q.n) q.partial[static_cast<size_t>(i) * nb + J] = make_float4(vi[0], vi[1], vi[2], 0.0f);
-            if (j < q.n) q.partial[static_cast<size_t>(j) * nb + I] = make_float4(vs[0], vs[1], vs[2], 0.0f);
+            if (i < q.n) q.partial[static_cast<size_t>(J) * q.n + i] = make_float4(vi[0], vi[1], vi[2], 0.0f);
+            if (j < q.n) q.partial[static_cast<size_t>(I) * q.n + j] = make_float4(vs[0], vs[1], vs[2], 0.0f);
         }
     }
 }

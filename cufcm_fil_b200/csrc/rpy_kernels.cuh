@@ -72,7 +72,7 @@ int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch
 // Batched symmetric wall products (segments on segments, 3x3) of B independent
 // particle sets stored back to back.  Per array b: particles [seg0[b], seg0[b]+n[b])
 // of x/f, nb[b] = ceil(n[b]/32) tiles, partials at partial + poff[b] laid out
-// [i * nb[b] + tile], and work items [item0[b], item0[b+1]) (item0[B] == items).
+// slot-major, [tile * n[b] + i], and work items [item0[b], item0[b+1]) (item0[B] == items).
 struct SymBatchParams {
     const float4 *x;
     const float4 *f;

@@ -1,4 +1,5 @@
-// sim.cu -- cf_sim: the device-resident implicit step for prescribed cilia on a wall.
+// sim.cu -- cf_sim / cf_batch: the device-resident implicit step for
+// prescribed cilia on a wall, for one array or a batch of independent arrays.
 //
 // Host side of the generic mobility_solver layer
 // (src/cilia/mobility/mobility_solver.{hpp,cpp}) for CILIA_TYPE 3 on an
@@ -9,11 +10,19 @@
 // and no host synchronisation.  The reference instead runs GMRES on the host
 // with one H2D copy, one kernel and one D2H copy per iteration
 // (mobility_solver.cpp:1910-1913, 2102).
+//
+// A batch runs many independent arrays (periodic-orbit / bisection sweeps)
+// through the same graph: every stage is one kernel over all arrays, the pair
+// product is one grid-stride launch over the (array, target tile, source tile)
+// work list of every array, and arrays whose GMRES stopped are masked out of
+// the remaining iterations.  A single array (cf_sim) is a batch of one.
 #include "common.cuh"
 #include "rpy_kernels.cuh"
 #include "sim_kernels.cuh"
 
 #include <algorithm>
+#include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -23,45 +32,63 @@
 using namespace cufil;
 
 namespace {
-constexpr int kIterLogCap = 4096;  // steps remembered by cf_sim_iteration_log
-}
+constexpr int kIterLogCap = 4096;  // steps remembered by the iteration log (per array)
+constexpr int kMinDotsChunk = 1024;
 
-struct cf_sim {
-    cf_sim_config cfg{};
+// Launch shapes chosen by the autotuner (or the defaults).
+struct Tuning {
+    int pair_ctas_per_sm = 8;   // pair kernel residency target
+    int dots_chunk = 4096;      // rows per dot-product item
+    int dots_blocks_per_sm = 2;
+    int update_blocks_per_sm = 8;
+    int update_rows = 32;       // rows per update / combine tile (32, 64, 128 or 256)
+};
+}  // namespace
+
+struct Engine {
+    int device = 0;
     int num_sms = CF_B200_SMS;
+    int B = 0;
+    cf_sim_config common{};
+    std::vector<ArrayInfo> arr;  // host copy of the placement table
     cudaStream_t stream = nullptr;
     cudaStream_t cap_stream = nullptr;  // captures the loop body
     SimDev d{};
-    RpyBlockDesc desc{};
-    RpyPlan plan{};
-    float4 *partial = nullptr;
+    SymBatchParams pair{};
+    int pair_grid = 1, dots_grid = 1, update_grid = 1, epi_grid = 1;
+    Tuning tune;
+    ArrayInfo *d_arr = nullptr;
+    int *d_chunk_arr = nullptr;
     int *err = nullptr;
     int fil_threads = 64;
     size_t kin_smem = 0, pre_smem = 0, givens_smem = 0;
-    int dots_grid = 0, update_grid = 0;
     bool use_graph = true;
+    bool stepped = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle handle = 0;
     std::vector<void *> allocations;
 };
 
+struct cf_sim : Engine {};
+struct cf_batch : Engine {};
+
 namespace {
 
 template <typename T>
-int sim_alloc(cf_sim *s, T **p, size_t n) {
+int eng_alloc(Engine *e, T **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
     void *q = nullptr;
     CF_CUDA(cudaMalloc(&q, n * sizeof(T)));
-    s->allocations.push_back(q);
+    e->allocations.push_back(q);
     *p = static_cast<T *>(q);
     return CF_OK;
 }
 
 template <typename T>
-int sim_upload(cf_sim *s, T **p, const T *host, size_t n) {
-    CF_TRY(sim_alloc(s, p, n));
+int eng_upload(Engine *e, T **p, const T *host, size_t n) {
+    CF_TRY(eng_alloc(e, p, n));
     if (host && n) CF_CUDA(cudaMemcpy(*p, host, n * sizeof(T), cudaMemcpyHostToDevice));
     return CF_OK;
 }
@@ -100,60 +127,128 @@ BeatCoeffs beat_table(int beat) {
     return b;
 }
 
-int launch_kinematics(cf_sim *s, cudaStream_t st) {
-    kinematics_kernel<<<s->d.F, s->fil_threads, s->kin_smem, st>>>(s->d);
+// Pair-kernel grid: every warp gets the same number of (array, tile, tile) items.
+int pair_grid_for(long long items, int num_sms, int ctas_per_sm) {
+    const long long max_warps = static_cast<long long>(std::max(1, num_sms)) * std::max(1, ctas_per_sm) * 4;
+    const long long per_warp = std::max(1LL, (items + max_warps - 1) / max_warps);
+    const long long warps = (items + per_warp - 1) / per_warp;
+    return static_cast<int>(std::max(1LL, (warps + 3) / 4));
+}
+
+// Re-derives the chunk tables and launch grids from the tuning and uploads
+// the placement table; drops the captured graph (it holds the old values).
+int apply_tuning(Engine *e, const Tuning &t) {
+    SimDev &d = e->d;
+    e->tune = t;
+    d.dots_chunk = t.dots_chunk;
+    int c = 0;
+    std::vector<int> chunk_arr;
+    for (int b = 0; b < e->B; ++b) {
+        ArrayInfo &a = e->arr[b];
+        a.chunk0 = c;
+        a.nchunk = (a.n + t.dots_chunk - 1) / t.dots_chunk;
+        for (int q = 0; q < a.nchunk; ++q) chunk_arr.push_back(b);
+        c += a.nchunk;
+    }
+    d.C_tot = c;
+    CF_CUDA(cudaMemcpy(e->d_arr, e->arr.data(), sizeof(ArrayInfo) * e->B, cudaMemcpyHostToDevice));
+    CF_CUDA(cudaMemcpy(e->d_chunk_arr, chunk_arr.data(), sizeof(int) * c, cudaMemcpyHostToDevice));
+    e->pair_grid = pair_grid_for(e->pair.items, e->num_sms, t.pair_ctas_per_sm);
+    e->dots_grid = std::max(1, e->num_sms * t.dots_blocks_per_sm);
+    const long long ntiles = d.nrows / t.update_rows;
+    e->update_grid = static_cast<int>(std::max(1LL, std::min(ntiles, 1LL * e->num_sms * t.update_blocks_per_sm)));
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->exec = nullptr;
+    e->graph = nullptr;
+    return CF_OK;
+}
+
+int launch_kinematics(Engine *e, cudaStream_t st) {
+    kinematics_kernel<<<e->d.F, e->fil_threads, e->kin_smem, st>>>(e->d);
     CF_CHECK_LAUNCH("kinematics_kernel");
     return CF_OK;
 }
 
-int launch_matvec_tail(cf_sim *s, const double *v, double *out, cudaStream_t st) {
-    CF_TRY(rpy_launch_tiles(s->desc, s->plan, s->partial, s->err, st));
-    const int warps_per_block = 8;
-    saddle_epilogue_kernel<<<(s->d.N + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(
-        s->d, v, out);
+int launch_step_begin(Engine *e, int nt, cudaStream_t st) {
+    step_begin_kernel<<<1, 256, 0, st>>>(e->d, nt);
+    CF_CHECK_LAUNCH("step_begin_kernel");
+    return CF_OK;
+}
+
+int launch_matvec_tail(Engine *e, const double *v, double *out, cudaStream_t st) {
+    CF_TRY(rpy_launch_sym_batch(e->pair, e->pair_grid, st));
+    saddle_epilogue_kernel<<<e->epi_grid, 256, 0, st>>>(e->d, v, out);
     CF_CHECK_LAUNCH("saddle_epilogue_kernel");
     return CF_OK;
 }
 
-int launch_prologue(cf_sim *s, cudaGraphConditionalHandle h, cudaStream_t st) {
-    CF_TRY(launch_kinematics(s, st));
-    rhs_kernel<<<s->d.F, s->fil_threads, 0, st>>>(s->d);
+template <int ROWS>
+int launch_update_t(Engine *e, const double *h, int final_pass, cudaGraphConditionalHandle hc, int grid,
+                    cudaStream_t st) {
+    update_kernel<ROWS><<<grid, 256, final_pass ? e->givens_smem : 0, st>>>(e->d, h, final_pass, hc);
+    CF_CHECK_LAUNCH("update_kernel");
+    return CF_OK;
+}
+
+int launch_update(Engine *e, const double *h, int final_pass, cudaGraphConditionalHandle hc, cudaStream_t st,
+                  int rows, int grid) {
+    switch (rows) {
+        case 32: return launch_update_t<32>(e, h, final_pass, hc, grid, st);
+        case 64: return launch_update_t<64>(e, h, final_pass, hc, grid, st);
+        case 128: return launch_update_t<128>(e, h, final_pass, hc, grid, st);
+        case 256: return launch_update_t<256>(e, h, final_pass, hc, grid, st);
+        default: return set_error(CF_EINVAL, "update tile of %d rows not built", rows);
+    }
+}
+
+int launch_combine(Engine *e, cudaStream_t st) {
+    const int grid = e->update_grid;
+    switch (e->tune.update_rows) {
+        case 32: combine_kernel<32><<<grid, 256, 0, st>>>(e->d); break;
+        case 64: combine_kernel<64><<<grid, 256, 0, st>>>(e->d); break;
+        case 128: combine_kernel<128><<<grid, 256, 0, st>>>(e->d); break;
+        case 256: combine_kernel<256><<<grid, 256, 0, st>>>(e->d); break;
+        default: return set_error(CF_EINVAL, "combine tile of %d rows not built", e->tune.update_rows);
+    }
+    CF_CHECK_LAUNCH("combine_kernel");
+    return CF_OK;
+}
+
+int launch_prologue(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
+    CF_TRY(launch_kinematics(e, st));
+    rhs_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d);
     CF_CHECK_LAUNCH("rhs_kernel");
-    CF_TRY(launch_matvec_tail(s, s->d.sol, s->d.w, st));
-    residual_decide_kernel<<<s->d.F, s->fil_threads, 0, st>>>(s->d, h);
+    CF_TRY(launch_matvec_tail(e, e->d.sol, e->d.w, st));
+    residual_decide_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, h);
     CF_CHECK_LAUNCH("residual_decide_kernel");
     return CF_OK;
 }
 
-int launch_body(cf_sim *s, cudaGraphConditionalHandle h, cudaStream_t st) {
-    arnoldi_precond_kernel<<<s->d.F, s->fil_threads, s->pre_smem, st>>>(s->d, h);
+int launch_body(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
+    arnoldi_precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, h);
     CF_CHECK_LAUNCH("arnoldi_precond_kernel");
-    CF_TRY(launch_matvec_tail(s, s->d.z, s->d.w, st));
-    dots_kernel<<<s->dots_grid, 256, 0, st>>>(s->d, s->d.h1);
+    CF_TRY(launch_matvec_tail(e, e->d.z, e->d.w, st));
+    dots_kernel<<<e->dots_grid, 256, 0, st>>>(e->d, e->d.h1);
     CF_CHECK_LAUNCH("dots_kernel");
-    update_kernel<<<s->update_grid, 256, 0, st>>>(s->d, s->d.h1, 0, h);
-    CF_CHECK_LAUNCH("update_kernel");
-    dots_kernel<<<s->dots_grid, 256, 0, st>>>(s->d, s->d.h2);
+    CF_TRY(launch_update(e, e->d.h1, 0, h, st, e->tune.update_rows, e->update_grid));
+    dots_kernel<<<e->dots_grid, 256, 0, st>>>(e->d, e->d.h2);
     CF_CHECK_LAUNCH("dots_kernel");
-    update_kernel<<<s->update_grid, 256, s->givens_smem, st>>>(s->d, s->d.h2, 1, h);
-    CF_CHECK_LAUNCH("update_kernel");
-    return CF_OK;
+    return launch_update(e, e->d.h2, 1, h, st, e->tune.update_rows, e->update_grid);
 }
 
-int launch_finish(cf_sim *s, cudaStream_t st) {
-    backsub_kernel<<<1, 256, sizeof(double) * (s->d.max_iter + 1), st>>>(s->d);
+int launch_finish(Engine *e, cudaStream_t st) {
+    backsub_kernel<<<e->B, 256, sizeof(double) * (e->d.mi_max + 1), st>>>(e->d);
     CF_CHECK_LAUNCH("backsub_kernel");
-    combine_kernel<<<s->update_grid, 256, 0, st>>>(s->d);
-    CF_CHECK_LAUNCH("combine_kernel");
-    finish_kernel<<<s->d.F, s->fil_threads, s->pre_smem, st>>>(s->d);
+    CF_TRY(launch_combine(e, st));
+    finish_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d);
     CF_CHECK_LAUNCH("finish_kernel");
     return CF_OK;
 }
 
 // Captures prologue -> WHILE(body) -> finish into one executable graph.
-int build_graph(cf_sim *s) {
-    CF_TRY(rpy_prepare(s->desc, s->plan));
-    cudaStream_t st = s->stream;
+int build_graph(Engine *e) {
+    cudaStream_t st = e->stream;
     CF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = CF_OK;
     cudaGraph_t g = nullptr;
@@ -164,16 +259,16 @@ int build_graph(cf_sim *s) {
         if ((rc = cuda_status(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps),
                               "cudaStreamGetCaptureInfo", __FILE__, __LINE__)))
             break;
-        if ((rc = cuda_status(cudaGraphConditionalHandleCreate(&s->handle, g, 0, cudaGraphCondAssignDefault),
+        if ((rc = cuda_status(cudaGraphConditionalHandleCreate(&e->handle, g, 0, cudaGraphCondAssignDefault),
                               "cudaGraphConditionalHandleCreate", __FILE__, __LINE__)))
             break;
-        if ((rc = launch_prologue(s, s->handle, st))) break;
+        if ((rc = launch_prologue(e, e->handle, st))) break;
         if ((rc = cuda_status(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps),
                               "cudaStreamGetCaptureInfo", __FILE__, __LINE__)))
             break;
         cudaGraphNodeParams cp{};
         cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = s->handle;
+        cp.conditional.handle = e->handle;
         cp.conditional.type = cudaGraphCondTypeWhile;
         cp.conditional.size = 1;
         cudaGraphNode_t wnode;
@@ -184,257 +279,593 @@ int build_graph(cf_sim *s) {
         if ((rc = cuda_status(cudaStreamUpdateCaptureDependencies(st, &wnode, 1, cudaStreamSetCaptureDependencies),
                               "cudaStreamUpdateCaptureDependencies", __FILE__, __LINE__)))
             break;
-        if ((rc = cuda_status(cudaStreamBeginCaptureToGraph(s->cap_stream, body, nullptr, nullptr, 0,
+        if ((rc = cuda_status(cudaStreamBeginCaptureToGraph(e->cap_stream, body, nullptr, nullptr, 0,
                                                             cudaStreamCaptureModeThreadLocal),
                               "cudaStreamBeginCaptureToGraph", __FILE__, __LINE__)))
             break;
-        rc = launch_body(s, s->handle, s->cap_stream);
+        rc = launch_body(e, e->handle, e->cap_stream);
         cudaGraph_t body_out = nullptr;
-        cudaError_t e2 = cudaStreamEndCapture(s->cap_stream, &body_out);
+        cudaError_t e2 = cudaStreamEndCapture(e->cap_stream, &body_out);
         if (rc) break;
         if ((rc = cuda_status(e2, "cudaStreamEndCapture(body)", __FILE__, __LINE__))) break;
-        if ((rc = launch_finish(s, st))) break;
+        if ((rc = launch_finish(e, st))) break;
     } while (0);
     cudaGraph_t full = nullptr;
-    cudaError_t e = cudaStreamEndCapture(st, &full);
+    cudaError_t ce = cudaStreamEndCapture(st, &full);
     if (rc) {
         if (full) cudaGraphDestroy(full);
         return rc;
     }
-    CF_TRY(cuda_status(e, "cudaStreamEndCapture", __FILE__, __LINE__));
-    s->graph = full;
-    CF_CUDA(cudaGraphInstantiate(&s->exec, s->graph, 0));
+    CF_TRY(cuda_status(ce, "cudaStreamEndCapture", __FILE__, __LINE__));
+    e->graph = full;
+    CF_CUDA(cudaGraphInstantiate(&e->exec, e->graph, 0));
     return CF_OK;
 }
 
-int read_ctl(cf_sim *s, GmresCtl *out) {
-    CF_CUDA(cudaMemcpyAsync(out, s->d.ctl, sizeof(GmresCtl), cudaMemcpyDeviceToHost, s->stream));
-    CF_CUDA(cudaStreamSynchronize(s->stream));
+int check_err_flag(Engine *e) {
     int flags = 0;
-    CF_CUDA(cudaMemcpy(&flags, s->err, sizeof(int), cudaMemcpyDeviceToHost));
+    CF_CUDA(cudaMemcpy(&flags, e->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (flags) {
-        CF_CUDA(cudaMemset(s->err, 0, sizeof(int)));
+        CF_CUDA(cudaMemset(e->err, 0, sizeof(int)));
         return set_error(CF_TIMEOUT, "sim: a bounded device wait gave up (flags 0x%x)", flags);
     }
     return CF_OK;
 }
 
-int status_of(const GmresCtl &c) {
+int read_loop(Engine *e, LoopCtl *out) {
+    CF_CUDA(cudaMemcpyAsync(out, e->d.lc, sizeof(LoopCtl), cudaMemcpyDeviceToHost, e->stream));
+    CF_CUDA(cudaStreamSynchronize(e->stream));
+    return check_err_flag(e);
+}
+
+int read_ctls(Engine *e, std::vector<GmresCtl> &out) {
+    out.resize(e->B);
+    CF_CUDA(cudaMemcpyAsync(out.data(), e->d.ctl, sizeof(GmresCtl) * e->B, cudaMemcpyDeviceToHost, e->stream));
+    CF_CUDA(cudaStreamSynchronize(e->stream));
+    return check_err_flag(e);
+}
+
+int iters_of(const GmresCtl &c) {
+    return (c.status == kGmresConverged || c.status == kGmresMaxIter) ? c.iters : 0;
+}
+
+int status_of(const GmresCtl &c, int b, int B) {
+    char where[48] = "";
+    if (B > 1) std::snprintf(where, sizeof(where), " (array %d)", b);
     switch (c.status) {
         case kGmresMaxIter:
-            return set_error(CF_NOT_CONVERGED, "GMRES stopped at its cap: %d iterations, relative residual %.3e",
-                             c.iters, c.relres);
+            return set_error(CF_NOT_CONVERGED, "GMRES stopped at its cap%s: %d iterations, relative residual %.3e",
+                             where, c.iters, c.relres);
         case kGmresNonFinite:
-            return set_error(CF_NONFINITE, "GMRES met a non-finite value (relative residual %.3e)", c.relres);
+            return set_error(CF_NONFINITE, "GMRES met a non-finite value%s (relative residual %.3e)", where,
+                             c.relres);
         default:
             return CF_OK;
     }
 }
 
-int run_step(cf_sim *s, int nt) {
-    set_nt_kernel<<<1, 1, 0, s->stream>>>(s->d.ctl, nt);
-    CF_CHECK_LAUNCH("set_nt_kernel");
-    if (s->use_graph) {
-        if (!s->exec) {
-            int rc = build_graph(s);
+// Worst status over the arrays: a non-finite array outranks a capped one.
+int batch_status(const std::vector<GmresCtl> &c) {
+    int rc = CF_OK;
+    for (size_t b = 0; b < c.size(); ++b) {
+        if (c[b].status == kGmresNonFinite) return status_of(c[b], static_cast<int>(b), static_cast<int>(c.size()));
+        if (c[b].status == kGmresMaxIter && rc == CF_OK)
+            rc = status_of(c[b], static_cast<int>(b), static_cast<int>(c.size()));
+    }
+    return rc;
+}
+
+int run_step(Engine *e, int nt) {
+    CF_TRY(launch_step_begin(e, nt, e->stream));
+    e->stepped = true;
+    if (e->use_graph) {
+        if (!e->exec) {
+            int rc = build_graph(e);
             if (rc != CF_OK) {
                 // Conditional graph nodes unavailable: fall back to the host-driven loop.
                 cudaGetLastError();
-                s->use_graph = false;
+                e->use_graph = false;
             }
         }
-        if (s->use_graph) {
-            CF_CUDA(cudaGraphLaunch(s->exec, s->stream));
+        if (e->use_graph) {
+            CF_CUDA(cudaGraphLaunch(e->exec, e->stream));
             return CF_OK;
         }
     }
-    CF_TRY(launch_prologue(s, 0, s->stream));
-    GmresCtl c;
-    CF_TRY(read_ctl(s, &c));
+    CF_TRY(launch_prologue(e, 0, e->stream));
+    LoopCtl lc;
+    CF_TRY(read_loop(e, &lc));
     int guard = 0;
-    while (c.cond && guard++ <= s->d.max_iter) {
-        CF_TRY(launch_body(s, 0, s->stream));
-        CF_TRY(read_ctl(s, &c));
+    while (lc.cond && guard++ <= e->d.mi_max) {
+        CF_TRY(launch_body(e, 0, e->stream));
+        CF_TRY(read_loop(e, &lc));
     }
-    return launch_finish(s, s->stream);
+    return launch_finish(e, e->stream);
+}
+
+bool same_table(const double *a, const double *b, int n) {
+    if (a == b) return true;
+    if (!a || !b) return false;
+    return std::memcmp(a, b, sizeof(double) * n) == 0;
+}
+
+int validate(const cf_sim_config *cfg, const char *who) {
+    CF_REQUIRE(cfg->n_fil > 0 && cfg->n_seg >= 2 && cfg->n_seg <= 256,
+               "%s: need n_fil > 0 and 2 <= n_seg <= 256 (got %d, %d)", who, cfg->n_fil, cfg->n_seg);
+    CF_REQUIRE(static_cast<long long>(cfg->n_fil) * cfg->n_seg < (1LL << 26), "%s: too many segments", who);
+    CF_REQUIRE(cfg->beat == CF_BEAT_FULFORD_BLAKE || cfg->beat == CF_BEAT_FULFORD_BLAKE_ORIGINAL,
+               "%s: unknown beat %d", who, cfg->beat);
+    CF_REQUIRE(cfg->precond == CF_PRECOND_NONE || cfg->precond == CF_PRECOND_BLOCK_DIAG,
+               "%s: preconditioner %d not available in this entry point", who, cfg->precond);
+    CF_REQUIRE(cfg->dt > 0 && cfg->seg_sep > 0, "%s: dt and seg_sep must be positive", who);
+    CF_REQUIRE(cfg->gmres_tol > 0 && cfg->gmres_max_iter > 0, "%s: bad GMRES tolerance / cap", who);
+    CF_REQUIRE(cfg->base_pos, "%s: base_pos is required", who);
+    CF_REQUIRE(!cfg->dynamic_phase || (cfg->gen_phase_force_refs && cfg->n_gen_phase_refs >= 2),
+               "%s: dynamic phase needs the reference generalised phase forces", who);
+    CF_REQUIRE(!cfg->dynamic_angle || (cfg->gen_angle_force_refs && cfg->n_gen_angle_refs >= 2),
+               "%s: dynamic angle needs the reference generalised angle forces", who);
+    CF_REQUIRE(!cfg->s_values_ref || (cfg->s_ref_rows >= 1 && cfg->s_ref_cols >= 2),
+               "%s: bad arclength table shape", who);
+    return CF_OK;
+}
+
+// Fields every array of a batch shares with the first.
+int validate_shared(const cf_sim_config &a, const cf_sim_config &c, int b) {
+    const bool same = a.n_seg == c.n_seg && a.seg_sep == c.seg_sep && a.beat == c.beat &&
+                      a.dynamic_phase == c.dynamic_phase && a.dynamic_angle == c.dynamic_angle && a.dt == c.dt &&
+                      a.spring_factor == c.spring_factor && a.gmres_tol == c.gmres_tol &&
+                      a.gmres_max_iter == c.gmres_max_iter && a.precond == c.precond &&
+                      a.s_tol_factor == c.s_tol_factor && a.device == c.device &&
+                      a.n_gen_phase_refs == c.n_gen_phase_refs && a.n_gen_angle_refs == c.n_gen_angle_refs &&
+                      a.s_ref_rows == c.s_ref_rows && a.s_ref_cols == c.s_ref_cols &&
+                      (a.s_values_ref == nullptr) == (c.s_values_ref == nullptr);
+    CF_REQUIRE(same, "cf_batch_create: array %d differs from array 0 in a shared setting "
+               "(segments, beat, dt, tolerance, preconditioner, tables)", b);
+    CF_REQUIRE(!a.dynamic_phase || same_table(a.gen_phase_force_refs, c.gen_phase_force_refs, a.n_gen_phase_refs),
+               "cf_batch_create: array %d has different generalised phase forces", b);
+    CF_REQUIRE(!a.dynamic_angle || same_table(a.gen_angle_force_refs, c.gen_angle_force_refs, a.n_gen_angle_refs),
+               "cf_batch_create: array %d has different generalised angle forces", b);
+    CF_REQUIRE(!a.s_values_ref || same_table(a.s_values_ref, c.s_values_ref, a.s_ref_rows * a.s_ref_cols),
+               "cf_batch_create: array %d has a different arclength table", b);
+    return CF_OK;
+}
+
+int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
+    const cf_sim_config &c0 = cfgs[0];
+    e->common = c0;
+    e->device = c0.device;
+    e->B = B;
+    cudaDeviceProp prop;
+    CF_CUDA(cudaGetDeviceProperties(&prop, e->device));
+    e->num_sms = prop.multiProcessorCount;
+    CF_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    CF_CUDA(cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking));
+
+    SimDev &d = e->d;
+    const int ns = c0.n_seg;
+    const int dp = c0.dynamic_phase ? 1 : 0, da = c0.dynamic_angle ? 1 : 0;
+    // placement of every array in the batch
+    e->arr.resize(B);
+    int fil = 0, seg = 0, mi_max = 1;
+    long long voff = 0, poff = 0, item0 = 0;
+    std::vector<int> fil_arr, rb_arr, h_seg0(B), h_n(B), h_nb(B);
+    std::vector<long long> h_poff(B), h_item0(B);
+    for (int b = 0; b < B; ++b) {
+        ArrayInfo &a = e->arr[b];
+        a.F = cfgs[b].n_fil;
+        a.N = a.F * ns;
+        a.n = 3 * a.N + a.F * (dp + da);
+        a.fil0 = fil;
+        a.seg0 = seg;
+        a.po = dp ? 3 * a.N : -1;
+        a.ao = da ? 3 * a.N + (dp ? a.F : 0) : -1;
+        a.max_iter = std::min(a.n, c0.gmres_max_iter);
+        a.nb = (a.N + 31) / 32;
+        a.voff = voff;
+        a.vlen = (static_cast<long long>(a.n) + kRowPad - 1) / kRowPad * kRowPad;
+        a.poff = poff;
+        a.chunk0 = 0;
+        a.nchunk = 0;
+        for (int q = 0; q < a.F; ++q) fil_arr.push_back(b);
+        for (long long q = 0; q < a.vlen / kRowUnit; ++q) rb_arr.push_back(b);
+        h_seg0[b] = a.seg0;
+        h_n[b] = a.N;
+        h_nb[b] = a.nb;
+        h_poff[b] = a.poff;
+        h_item0[b] = item0;
+        fil += a.F;
+        seg += a.N;
+        voff += a.vlen;
+        poff += static_cast<long long>(a.N) * a.nb;
+        item0 += static_cast<long long>(a.nb) * (a.nb + 1) / 2;
+        mi_max = std::max(mi_max, a.max_iter);
+    }
+    CF_REQUIRE(voff < (1LL << 31), "cf_batch_create: the batch vectors exceed 2^31 rows");
+    d.B = B;
+    d.F = fil;
+    d.nseg = ns;
+    d.N = seg;
+    d.nrows = voff;
+    d.ldq = voff;
+    d.mi_max = mi_max;
+    d.ldh = mi_max + 1;
+    d.hstride = static_cast<long long>(mi_max + 2) * (mi_max + 1);
+    d.sstride = mi_max + 2;
+    d.flexible = 0;
+    d.precond = c0.precond == CF_PRECOND_BLOCK_DIAG ? 1 : 0;
+    d.dyn_phase = dp;
+    d.dyn_angle = da;
+    d.dt = c0.dt;
+    d.L = c0.seg_sep * (ns - 1);  // FIL_LENGTH = DL*(NSEG_PER_CILIA-1), RSEG = 1
+    d.spring = c0.spring_factor;
+    d.tol = c0.gmres_tol;
+    d.s_tol = (c0.s_tol_factor > 0 ? c0.s_tol_factor : 0.1) / ns;
+    // Wall frame: rot_mat of (1/sqrt2, 0, -1/sqrt2, 0) maps the reference x axis to e_z.
+    const double R[9] = {0, 0, -1, 0, 1, 0, 1, 0, 0};
+    std::memcpy(d.R, R, sizeof(R));
+    d.beat = beat_table(c0.beat);
+    d.s_rows = c0.s_values_ref ? c0.s_ref_rows : 0;
+    d.s_cols = c0.s_values_ref ? c0.s_ref_cols : 0;
+    d.n_phase_refs = dp ? c0.n_gen_phase_refs : 0;
+    d.n_angle_refs = da ? c0.n_gen_angle_refs : 0;
+
+    // per-filament state, array by array
+    const int F = fil;
+    std::vector<double> omega(F), ph(F, 0.0), an(F, 0.0), base(3 * static_cast<size_t>(F)), zeros(F, 0.0);
+    for (int b = 0; b < B; ++b) {
+        const ArrayInfo &a = e->arr[b];
+        const cf_sim_config &c = cfgs[b];
+        for (int q = 0; q < a.F; ++q) {
+            omega[a.fil0 + q] = c.omega0 ? c.omega0[q] : 2.0 * 3.14159265358979323846;
+            if (c.phase0) ph[a.fil0 + q] = c.phase0[q];
+            if (c.angle0) an[a.fil0 + q] = c.angle0[q];
+        }
+        std::copy(c.base_pos, c.base_pos + 3 * static_cast<size_t>(a.F), base.begin() + 3 * static_cast<size_t>(a.fil0));
+    }
+    CF_TRY(eng_upload(e, const_cast<double **>(&d.s_table), c0.s_values_ref, static_cast<size_t>(d.s_rows) * d.s_cols));
+    CF_TRY(eng_upload(e, const_cast<double **>(&d.phase_refs), c0.gen_phase_force_refs, d.n_phase_refs));
+    CF_TRY(eng_upload(e, const_cast<double **>(&d.angle_refs), c0.gen_angle_force_refs, d.n_angle_refs));
+    CF_TRY(eng_upload(e, const_cast<double **>(&d.omega0), omega.data(), F));
+    CF_TRY(eng_upload(e, const_cast<double **>(&d.base), base.data(), base.size()));
+    CF_TRY(eng_upload(e, &d.phase, ph.data(), F));
+    CF_TRY(eng_upload(e, &d.angle, an.data(), F));
+    CF_TRY(eng_upload(e, &d.phase_dot, omega.data(), F));  // phase_dot = omega0 (filament.cpp:472)
+    CF_TRY(eng_upload(e, &d.angle_dot, zeros.data(), F));
+
+    const size_t N = seg, nr = voff, mi = mi_max, ldq = voff;
+    CF_TRY(eng_alloc(e, &d.x4, N));
+    CF_TRY(eng_alloc(e, &d.f4, N));
+    CF_TRY(eng_alloc(e, &d.xd, 3 * N));
+    CF_TRY(eng_alloc(e, &d.s_cur, N));
+    CF_TRY(eng_alloc(e, &d.kp, 3 * N));
+    CF_TRY(eng_alloc(e, &d.ka, 3 * N));
+    CF_TRY(eng_alloc(e, &d.gram, 3 * static_cast<size_t>(F)));
+    CF_TRY(eng_alloc(e, &d.rhs, nr));
+    CF_TRY(eng_alloc(e, &d.sol, nr));
+    CF_TRY(eng_alloc(e, &d.w, nr));
+    CF_TRY(eng_alloc(e, &d.z, nr));
+    CF_TRY(eng_alloc(e, &d.t, nr));
+    CF_TRY(eng_alloc(e, &d.Q, (mi + 1) * ldq));
+    d.Z = nullptr;
+    const size_t sm = static_cast<size_t>(B) * d.sstride;
+    CF_TRY(eng_alloc(e, &d.H, static_cast<size_t>(B) * d.hstride));
+    CF_TRY(eng_alloc(e, &d.cs, sm));
+    CF_TRY(eng_alloc(e, &d.sn, sm));
+    CF_TRY(eng_alloc(e, &d.beta, sm));
+    CF_TRY(eng_alloc(e, &d.h1, sm));
+    CF_TRY(eng_alloc(e, &d.h2, sm));
+    CF_TRY(eng_alloc(e, &d.y, sm));
+    CF_TRY(eng_alloc(e, &d.ctl, B));
+    CF_TRY(eng_alloc(e, &d.lc, 1));
+    CF_TRY(eng_alloc(e, &d.active, B));
+    CF_TRY(eng_alloc(e, &d.iter_log, static_cast<size_t>(B) * kIterLogCap));
+    CF_TRY(eng_alloc(e, &e->err, 1));
+    d.iter_log_cap = kIterLogCap;
+    // placement tables
+    CF_TRY(eng_alloc(e, &e->d_arr, B));
+    d.arr = e->d_arr;
+    CF_TRY(eng_upload(e, const_cast<int **>(&d.fil_arr), fil_arr.data(), fil_arr.size()));
+    CF_TRY(eng_upload(e, const_cast<int **>(&d.rb_arr), rb_arr.data(), rb_arr.size()));
+    size_t max_chunks = 0;
+    for (const ArrayInfo &a : e->arr) max_chunks += (a.n + kMinDotsChunk - 1) / kMinDotsChunk;
+    CF_TRY(eng_alloc(e, &e->d_chunk_arr, max_chunks));
+    d.chunk_arr = e->d_chunk_arr;
+    CF_TRY(eng_alloc(e, &d.dots_partial, (mi + 1) * max_chunks));
+    CF_TRY(eng_alloc(e, &d.norm_partial, std::max<size_t>(F, nr / kRowUnit)));
+    // pair kernel work list
+    int *p_seg0, *p_n, *p_nb;
+    long long *p_poff, *p_item0;
+    CF_TRY(eng_upload(e, &p_seg0, h_seg0.data(), B));
+    CF_TRY(eng_upload(e, &p_n, h_n.data(), B));
+    CF_TRY(eng_upload(e, &p_nb, h_nb.data(), B));
+    CF_TRY(eng_upload(e, &p_poff, h_poff.data(), B));
+    CF_TRY(eng_upload(e, &p_item0, h_item0.data(), B));
+    float4 *partial;
+    CF_TRY(eng_alloc(e, &partial, static_cast<size_t>(poff)));
+    d.partial = partial;
+    SymBatchParams &p = e->pair;
+    p.x = d.x4;
+    p.f = d.f4;
+    p.partial = partial;
+    p.seg0 = p_seg0;
+    p.n = p_n;
+    p.nb = p_nb;
+    p.poff = p_poff;
+    p.item0 = p_item0;
+    p.active = d.active;
+    p.B = B;
+    p.items = item0;
+
+    CF_CUDA(cudaMemset(d.iter_log, 0, sizeof(int) * static_cast<size_t>(B) * kIterLogCap));
+    CF_CUDA(cudaMemset(d.ctl, 0, sizeof(GmresCtl) * B));
+    CF_CUDA(cudaMemset(d.lc, 0, sizeof(LoopCtl)));
+    CF_CUDA(cudaMemset(e->err, 0, sizeof(int)));
+    CF_CUDA(cudaMemset(d.H, 0, sizeof(double) * static_cast<size_t>(B) * d.hstride));
+    // initial solution: lambda = 0, phase rate = omega0, angle rate = 0
+    std::vector<double> sol(nr, 0.0);
+    if (dp)
+        for (int b = 0; b < B; ++b)
+            for (int q = 0; q < e->arr[b].F; ++q) sol[e->arr[b].voff + e->arr[b].po + q] = omega[e->arr[b].fil0 + q];
+    CF_CUDA(cudaMemcpy(d.sol, sol.data(), nr * sizeof(double), cudaMemcpyHostToDevice));
+    CF_CUDA(cudaMemset(d.rhs, 0, nr * sizeof(double)));
+    CF_CUDA(cudaMemset(d.w, 0, nr * sizeof(double)));
+
+    // launch shapes
+    e->fil_threads = std::min(256, std::max(64, (3 * ns + 31) / 32 * 32));
+    e->kin_smem = sizeof(double) * (2 * (10 * ns + 1) + ns);
+    e->pre_smem = sizeof(double) * 3 * ns;
+    e->givens_smem = sizeof(double) * 3 * (d.mi_max + 2);
+    e->epi_grid = (seg + 255) / 256;
+    if (e->givens_smem > 48 * 1024) {
+        const int gs = static_cast<int>(e->givens_smem);
+        CF_CUDA(cudaFuncSetAttribute(update_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
+        CF_CUDA(cudaFuncSetAttribute(update_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
+        CF_CUDA(cudaFuncSetAttribute(update_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
+        CF_CUDA(cudaFuncSetAttribute(update_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
+    }
+    if (e->kin_smem > 48 * 1024)
+        CF_CUDA(cudaFuncSetAttribute(kinematics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(e->kin_smem)));
+    CF_TRY(apply_tuning(e, Tuning{}));
+    const char *ng = std::getenv("CUFIL_NO_GRAPH");
+    e->use_graph = !(ng && ng[0] == '1');
+    return CF_OK;
+}
+
+void engine_release(Engine *e) {
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    for (void *p : e->allocations) cudaFree(p);
+    if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    e->allocations.clear();
+}
+
+template <typename H>
+int create_handle(const cf_sim_config *cfgs, int B, H **out, const char *who) {
+    clear_error();
+    CF_REQUIRE(cfgs && out && B > 0, "%s: bad arguments", who);
+    *out = nullptr;
+    for (int b = 0; b < B; ++b) {
+        CF_TRY(validate(&cfgs[b], who));
+        if (b) CF_TRY(validate_shared(cfgs[0], cfgs[b], b));
+    }
+    CF_CUDA(cudaSetDevice(cfgs[0].device));
+    H *h = new (std::nothrow) H();
+    if (!h) return set_error(CF_ENOMEM, "%s: host allocation failed", who);
+    const int rc = engine_init(h, cfgs, B);
+    if (rc != CF_OK) {
+        std::string msg = cf_last_error();
+        engine_release(h);
+        delete h;
+        set_error(rc, "%s", msg.c_str());
+        return rc;
+    }
+    *out = h;
+    return CF_OK;
+}
+
+// --------------------------------------------------------------- autotuner
+// Times one kernel configuration: `launch` issued `reps` times between two
+// events on the engine's stream, after two untimed launches.
+template <typename Fn>
+int time_launches(Engine *e, Fn launch, int reps, float *ms) {
+    for (int r = 0; r < 2; ++r) CF_TRY(launch());
+    cudaEvent_t a, b;
+    CF_CUDA(cudaEventCreate(&a));
+    CF_CUDA(cudaEventCreate(&b));
+    CF_CUDA(cudaEventRecord(a, e->stream));
+    int rc = CF_OK;
+    for (int r = 0; r < reps && rc == CF_OK; ++r) rc = launch();
+    cudaEventRecord(b, e->stream);
+    cudaEventSynchronize(b);
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CF_TRY(rc);
+    *ms = t / reps;
+    return CF_OK;
+}
+
+__global__ void set_k_kernel(LoopCtl *lc, int k) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) lc->k = k;
+}
+
+// Picks the launch shapes of the iteration kernels by timing them on the
+// batch as it stands (every array active, basis index k_rep): the pair
+// kernel's residency target, the dot-product row chunk and grid, and the
+// grid of the row-block updates.  Only scratch buffers are written (the
+// mobility partials, w with a zero update, h1, the dot partials); the filament
+// state and the solution are untouched.
+int engine_autotune(Engine *e, int k_hint, int *choice) {
+    SimDev &d = e->d;
+    CF_CUDA(cudaStreamSynchronize(e->stream));
+    int k_rep = k_hint;
+    if (k_rep <= 0) {
+        k_rep = 100;
+        if (e->stepped) {
+            std::vector<GmresCtl> c;
+            CF_TRY(read_ctls(e, c));
+            int mx = 0;
+            for (const GmresCtl &g : c) mx = std::max(mx, iters_of(g));
+            if (mx > 0) k_rep = (mx + 1) / 2;
+        }
+    }
+    k_rep = std::max(0, std::min(k_rep, d.mi_max - 1));
+    CF_TRY(launch_step_begin(e, -1, e->stream));
+    set_k_kernel<<<1, 1, 0, e->stream>>>(d.lc, k_rep);
+    CF_CHECK_LAUNCH("set_k_kernel");
+    CF_CUDA(cudaMemsetAsync(d.h1, 0, sizeof(double) * static_cast<size_t>(e->B) * d.sstride, e->stream));
+    const int reps = 5;
+    Tuning best = e->tune;
+    float t;
+    // pair kernel
+    {
+        float bt = 1e30f;
+        for (int c : {2, 4, 6, 8}) {
+            const int grid = pair_grid_for(e->pair.items, e->num_sms, c);
+            CF_TRY(time_launches(e, [&] { return rpy_launch_sym_batch(e->pair, grid, e->stream); }, reps, &t));
+            if (t < bt * 0.98f) {
+                bt = t;
+                best.pair_ctas_per_sm = c;
+            }
+        }
+    }
+    // dot products: the chunk tables change with the chunk size
+    {
+        float bt = 1e30f;
+        Tuning trial = best;
+        for (int chunk : {1024, 2048, 4096, 8192}) {
+            for (int bps : {1, 2, 4}) {
+                trial.dots_chunk = chunk;
+                trial.dots_blocks_per_sm = bps;
+                CF_TRY(apply_tuning(e, trial));
+                CF_TRY(time_launches(
+                    e,
+                    [&] {
+                        dots_kernel<<<e->dots_grid, 256, 0, e->stream>>>(e->d, e->d.h1);
+                        CF_CHECK_LAUNCH("dots_kernel");
+                        return CF_OK;
+                    },
+                    reps, &t));
+                if (t < bt * 0.98f) {
+                    bt = t;
+                    best.dots_chunk = chunk;
+                    best.dots_blocks_per_sm = bps;
+                }
+            }
+        }
+        CF_TRY(apply_tuning(e, best));
+        CF_CUDA(cudaMemsetAsync(d.h1, 0, sizeof(double) * static_cast<size_t>(e->B) * d.sstride, e->stream));
+    }
+    // row-tile updates (w -= Q h with h = 0: the timing of the real update, w unchanged):
+    // tile height and grid
+    {
+        float bt = 1e30f;
+        for (int rows : {32, 64, 128, 256}) {
+            for (int bps : {2, 4, 8, 16}) {
+                const long long ntiles = d.nrows / rows;
+                const int grid = static_cast<int>(std::max(1LL, std::min(ntiles, 1LL * e->num_sms * bps)));
+                CF_TRY(time_launches(
+                    e, [&] { return launch_update(e, e->d.h1, 0, 0, e->stream, rows, grid); }, reps, &t));
+                if (t < bt * 0.98f) {
+                    bt = t;
+                    best.update_rows = rows;
+                    best.update_blocks_per_sm = bps;
+                }
+            }
+        }
+    }
+    CF_TRY(apply_tuning(e, best));
+    CF_CUDA(cudaStreamSynchronize(e->stream));
+    if (choice) {
+        choice[0] = best.pair_ctas_per_sm;
+        choice[1] = best.dots_chunk;
+        choice[2] = best.dots_blocks_per_sm;
+        choice[3] = best.update_blocks_per_sm;
+        choice[4] = best.update_rows;
+    }
+    return CF_OK;
+}
+
+int engine_set_tuning(Engine *e, const int *choice) {
+    CF_REQUIRE(choice, "null tuning");
+    Tuning t;
+    t.pair_ctas_per_sm = choice[0];
+    t.dots_chunk = choice[1];
+    t.dots_blocks_per_sm = choice[2];
+    t.update_blocks_per_sm = choice[3];
+    t.update_rows = choice[4];
+    CF_REQUIRE(t.pair_ctas_per_sm >= 1 && t.pair_ctas_per_sm <= 8, "tuning: pair CTAs per SM must be 1..8");
+    CF_REQUIRE(t.dots_chunk >= kMinDotsChunk && t.dots_chunk % 256 == 0 && t.dots_chunk <= (1 << 20),
+               "tuning: dot chunk must be a multiple of 256 in [%d, 2^20]", kMinDotsChunk);
+    CF_REQUIRE(t.dots_blocks_per_sm >= 1 && t.dots_blocks_per_sm <= 16, "tuning: dot blocks per SM must be 1..16");
+    CF_REQUIRE(t.update_blocks_per_sm >= 1 && t.update_blocks_per_sm <= 32,
+               "tuning: update blocks per SM must be 1..32");
+    CF_REQUIRE(t.update_rows == 32 || t.update_rows == 64 || t.update_rows == 128 || t.update_rows == 256,
+               "tuning: update tile rows must be 32, 64, 128 or 256");
+    CF_CUDA(cudaStreamSynchronize(e->stream));
+    return apply_tuning(e, t);
+}
+
+void engine_get_tuning(const Engine *e, int *choice) {
+    choice[0] = e->tune.pair_ctas_per_sm;
+    choice[1] = e->tune.dots_chunk;
+    choice[2] = e->tune.dots_blocks_per_sm;
+    choice[3] = e->tune.update_blocks_per_sm;
+    choice[4] = e->tune.update_rows;
+}
+
+// Filament-state copies for arrays [b0, b1) (all filaments of those arrays).
+int copy_state_out(Engine *e, double *phase, double *angle, double *phase_dot, double *angle_dot) {
+    const size_t bytes = sizeof(double) * e->d.F;
+    if (phase) CF_CUDA(cudaMemcpyAsync(phase, e->d.phase, bytes, cudaMemcpyDeviceToHost, e->stream));
+    if (angle) CF_CUDA(cudaMemcpyAsync(angle, e->d.angle, bytes, cudaMemcpyDeviceToHost, e->stream));
+    if (phase_dot) CF_CUDA(cudaMemcpyAsync(phase_dot, e->d.phase_dot, bytes, cudaMemcpyDeviceToHost, e->stream));
+    if (angle_dot) CF_CUDA(cudaMemcpyAsync(angle_dot, e->d.angle_dot, bytes, cudaMemcpyDeviceToHost, e->stream));
+    CF_CUDA(cudaStreamSynchronize(e->stream));
+    return CF_OK;
+}
+
+int copy_state_in(Engine *e, const double *phase, const double *angle, const double *phase_dot,
+                  const double *angle_dot) {
+    SimDev &d = e->d;
+    const size_t bytes = sizeof(double) * d.F;
+    if (phase) CF_CUDA(cudaMemcpyAsync(d.phase, phase, bytes, cudaMemcpyHostToDevice, e->stream));
+    if (angle) CF_CUDA(cudaMemcpyAsync(d.angle, angle, bytes, cudaMemcpyHostToDevice, e->stream));
+    // the rates are both filament state and the GMRES warm start (mobility_solver.cpp:2298-2388)
+    for (int b = 0; b < e->B; ++b) {
+        const ArrayInfo &a = e->arr[b];
+        const size_t fb = sizeof(double) * a.F;
+        if (phase_dot) {
+            CF_CUDA(cudaMemcpyAsync(d.phase_dot + a.fil0, phase_dot + a.fil0, fb, cudaMemcpyHostToDevice, e->stream));
+            if (a.po >= 0)
+                CF_CUDA(cudaMemcpyAsync(d.sol + a.voff + a.po, phase_dot + a.fil0, fb, cudaMemcpyHostToDevice,
+                                        e->stream));
+        }
+        if (angle_dot) {
+            CF_CUDA(cudaMemcpyAsync(d.angle_dot + a.fil0, angle_dot + a.fil0, fb, cudaMemcpyHostToDevice, e->stream));
+            if (a.ao >= 0)
+                CF_CUDA(cudaMemcpyAsync(d.sol + a.voff + a.ao, angle_dot + a.fil0, fb, cudaMemcpyHostToDevice,
+                                        e->stream));
+        }
+    }
+    return CF_OK;
 }
 
 }  // namespace
 
+// ===================================================================== cf_sim
 extern "C" int cf_sim_create(const cf_sim_config *cfg, cf_sim **out) {
-    clear_error();
-    CF_REQUIRE(cfg && out, "cf_sim_create: null argument");
-    *out = nullptr;
-    CF_REQUIRE(cfg->n_fil > 0 && cfg->n_seg >= 2 && cfg->n_seg <= 256,
-               "cf_sim_create: need n_fil > 0 and 2 <= n_seg <= 256 (got %d, %d)", cfg->n_fil, cfg->n_seg);
-    CF_REQUIRE(static_cast<long long>(cfg->n_fil) * cfg->n_seg < (1LL << 26), "cf_sim_create: too many segments");
-    CF_REQUIRE(cfg->beat == CF_BEAT_FULFORD_BLAKE || cfg->beat == CF_BEAT_FULFORD_BLAKE_ORIGINAL,
-               "cf_sim_create: unknown beat %d", cfg->beat);
-    CF_REQUIRE(cfg->precond == CF_PRECOND_NONE || cfg->precond == CF_PRECOND_BLOCK_DIAG,
-               "cf_sim_create: preconditioner %d not available in this entry point", cfg->precond);
-    CF_REQUIRE(cfg->dt > 0 && cfg->seg_sep > 0, "cf_sim_create: dt and seg_sep must be positive");
-    CF_REQUIRE(cfg->gmres_tol > 0 && cfg->gmres_max_iter > 0, "cf_sim_create: bad GMRES tolerance / cap");
-    CF_REQUIRE(cfg->base_pos, "cf_sim_create: base_pos is required");
-    CF_REQUIRE(!cfg->dynamic_phase || (cfg->gen_phase_force_refs && cfg->n_gen_phase_refs >= 2),
-               "cf_sim_create: dynamic phase needs the reference generalised phase forces");
-    CF_REQUIRE(!cfg->dynamic_angle || (cfg->gen_angle_force_refs && cfg->n_gen_angle_refs >= 2),
-               "cf_sim_create: dynamic angle needs the reference generalised angle forces");
-    CF_REQUIRE(!cfg->s_values_ref || (cfg->s_ref_rows >= 1 && cfg->s_ref_cols >= 2),
-               "cf_sim_create: bad arclength table shape");
-    CF_CUDA(cudaSetDevice(cfg->device));
-    cf_sim *s = new (std::nothrow) cf_sim();
-    if (!s) return set_error(CF_ENOMEM, "cf_sim_create: host allocation failed");
-    s->cfg = *cfg;
-    int rc = CF_OK;
-    do {
-        cudaDeviceProp prop;
-        if ((rc = cuda_status(cudaGetDeviceProperties(&prop, cfg->device), "cudaGetDeviceProperties", __FILE__,
-                              __LINE__)))
-            break;
-        s->num_sms = prop.multiProcessorCount;
-        if ((rc = cuda_status(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate",
-                              __FILE__, __LINE__)))
-            break;
-        if ((rc = cuda_status(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking), "cudaStreamCreate",
-                              __FILE__, __LINE__)))
-            break;
-        SimDev &d = s->d;
-        const int F = cfg->n_fil, ns = cfg->n_seg, N = F * ns;
-        d.F = F;
-        d.nseg = ns;
-        d.N = N;
-        d.po = cfg->dynamic_phase ? 3 * N : -1;
-        d.ao = cfg->dynamic_angle ? 3 * N + (cfg->dynamic_phase ? F : 0) : -1;
-        d.n = 3 * N + F * ((cfg->dynamic_phase ? 1 : 0) + (cfg->dynamic_angle ? 1 : 0));
-        d.ldq = (d.n + 31) / 32 * 32;
-        d.max_iter = std::min(d.n, cfg->gmres_max_iter);
-        d.ldh = d.max_iter + 1;
-        d.flexible = 0;
-        d.precond = cfg->precond == CF_PRECOND_BLOCK_DIAG ? 1 : 0;
-        d.dt = cfg->dt;
-        d.L = cfg->seg_sep * (ns - 1);  // FIL_LENGTH = DL*(NSEG_PER_CILIA-1), RSEG = 1
-        d.spring = cfg->spring_factor;
-        d.tol = cfg->gmres_tol;
-        d.s_tol = (cfg->s_tol_factor > 0 ? cfg->s_tol_factor : 0.1) / ns;
-        // Wall frame: rot_mat of (1/sqrt2, 0, -1/sqrt2, 0) maps the reference x axis to e_z.
-        const double R[9] = {0, 0, -1, 0, 1, 0, 1, 0, 0};
-        std::memcpy(d.R, R, sizeof(R));
-        d.beat = beat_table(cfg->beat);
-        d.s_rows = cfg->s_values_ref ? cfg->s_ref_rows : 0;
-        d.s_cols = cfg->s_values_ref ? cfg->s_ref_cols : 0;
-        d.n_phase_refs = cfg->dynamic_phase ? cfg->n_gen_phase_refs : 0;
-        d.n_angle_refs = cfg->dynamic_angle ? cfg->n_gen_angle_refs : 0;
-
-        std::vector<double> omega(F, 2.0 * 3.14159265358979323846), ph(F, 0.0), an(F, 0.0);
-        if (cfg->omega0) std::copy(cfg->omega0, cfg->omega0 + F, omega.begin());
-        if (cfg->phase0) std::copy(cfg->phase0, cfg->phase0 + F, ph.begin());
-        if (cfg->angle0) std::copy(cfg->angle0, cfg->angle0 + F, an.begin());
-        std::vector<double> zeros(F, 0.0);
-        const double *cst;
-        if ((rc = sim_upload(s, const_cast<double **>(&d.s_table), cfg->s_values_ref,
-                             static_cast<size_t>(d.s_rows) * d.s_cols)) ||
-            (rc = sim_upload(s, const_cast<double **>(&d.phase_refs), cfg->gen_phase_force_refs, d.n_phase_refs)) ||
-            (rc = sim_upload(s, const_cast<double **>(&d.angle_refs), cfg->gen_angle_force_refs, d.n_angle_refs)) ||
-            (rc = sim_upload(s, const_cast<double **>(&d.omega0), omega.data(), F)) ||
-            (rc = sim_upload(s, const_cast<double **>(&d.base), cfg->base_pos, 3 * static_cast<size_t>(F))) ||
-            (rc = sim_upload(s, &d.phase, ph.data(), F)) || (rc = sim_upload(s, &d.angle, an.data(), F)) ||
-            (rc = sim_upload(s, &d.phase_dot, omega.data(), F)) ||  // phase_dot = omega0 (filament.cpp:472)
-            (rc = sim_upload(s, &d.angle_dot, zeros.data(), F)))
-            break;
-        (void)cst;
-        const size_t n = d.n, ldq = d.ldq, mi = d.max_iter;
-        if ((rc = sim_alloc(s, &d.x4, N)) || (rc = sim_alloc(s, &d.xd, 3 * N)) || (rc = sim_alloc(s, &d.s_cur, N)) || (rc = sim_alloc(s, &d.kp, 3 * N)) ||
-            (rc = sim_alloc(s, &d.ka, 3 * N)) || (rc = sim_alloc(s, &d.gram, 3 * F)) ||
-            (rc = sim_alloc(s, &d.rhs, n)) || (rc = sim_alloc(s, &d.sol, n)) || (rc = sim_alloc(s, &d.w, n)) ||
-            (rc = sim_alloc(s, &d.z, n)) || (rc = sim_alloc(s, &d.t, n)) || (rc = sim_alloc(s, &d.y, mi + 1)) ||
-            (rc = sim_alloc(s, &d.Q, (mi + 1) * ldq)) || (rc = sim_alloc(s, &d.H, (mi + 2) * (mi + 1))) ||
-            (rc = sim_alloc(s, &d.cs, mi + 1)) || (rc = sim_alloc(s, &d.sn, mi + 1)) ||
-            (rc = sim_alloc(s, &d.beta, mi + 2)) || (rc = sim_alloc(s, &d.h1, mi + 2)) ||
-            (rc = sim_alloc(s, &d.h2, mi + 2)) || (rc = sim_alloc(s, &d.f4, N)) || (rc = sim_alloc(s, &d.ctl, 1)) ||
-            (rc = sim_alloc(s, &d.iter_log, kIterLogCap)) ||
-            (rc = sim_alloc(s, &s->err, 1)))
-            break;
-        d.Z = nullptr;
-        d.iter_log_cap = kIterLogCap;
-        if ((rc = cuda_status(cudaMemset(d.iter_log, 0, sizeof(int) * kIterLogCap), "cudaMemset", __FILE__, __LINE__)))
-            break;
-        // initial solution: lambda = 0, phase rate = omega0, angle rate = 0
-        std::vector<double> sol(n, 0.0);
-        if (d.po >= 0)
-            for (int m = 0; m < F; ++m) sol[d.po + m] = omega[m];
-        if ((rc = cuda_status(cudaMemcpy(d.sol, sol.data(), n * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy",
-                              __FILE__, __LINE__)))
-            break;
-        // pair-kernel plan (wall, 3x3, segments on segments)
-        RpyBlockDesc &desc = s->desc;
-        desc.wall = 1;
-        desc.vd = 3;
-        desc.fd = 3;
-        desc.self_set = 1;
-        desc.xt = d.x4;
-        desc.nt = N;
-        desc.at = 1.0f;
-        desc.xs = d.x4;
-        desc.fs = d.f4;
-        desc.ts = nullptr;
-        desc.ns = N;
-        desc.as = 1.0f;
-        desc.mu = 1.0f;
-        s->plan = rpy_plan_for(desc, s->num_sms);
-        if ((rc = sim_alloc(s, &s->partial, s->plan.scratch_float4))) break;
-        d.partial = s->partial;
-        d.nsplit = s->plan.nsplit;
-        // launch shapes
-        s->fil_threads = std::min(256, std::max(64, (3 * ns + 31) / 32 * 32));
-        s->kin_smem = sizeof(double) * (2 * (10 * ns + 1) + ns);
-        s->pre_smem = sizeof(double) * 3 * ns;
-        s->givens_smem = sizeof(double) * 3 * (d.max_iter + 2);
-        d.dots_chunk = 4096;
-        d.dots_nchunk = (d.n + d.dots_chunk - 1) / d.dots_chunk;
-        s->dots_grid = 2 * s->num_sms;
-        s->update_grid = std::min(8 * s->num_sms, (d.n + 31) / 32);
-        if ((rc = sim_alloc(s, &d.dots_partial, (mi + 1) * d.dots_nchunk)) ||
-            (rc = sim_alloc(s, &d.norm_partial, std::max(F, std::max(s->update_grid, s->dots_grid)))))
-            break;
-        if ((rc = cuda_status(cudaMemset(d.ctl, 0, sizeof(GmresCtl)), "cudaMemset", __FILE__, __LINE__)) ||
-            (rc = cuda_status(cudaMemset(s->err, 0, sizeof(int)), "cudaMemset", __FILE__, __LINE__)) ||
-            (rc = cuda_status(cudaMemset(d.H, 0, sizeof(double) * (mi + 2) * (mi + 1)), "cudaMemset", __FILE__,
-                              __LINE__)))
-            break;
-        if (s->givens_smem > 48 * 1024) {
-            if ((rc = cuda_status(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       static_cast<int>(s->givens_smem)),
-                                  "cudaFuncSetAttribute", __FILE__, __LINE__)))
-                break;
-        }
-        if (s->kin_smem > 48 * 1024) {
-            if ((rc = cuda_status(cudaFuncSetAttribute(kinematics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       static_cast<int>(s->kin_smem)),
-                                  "cudaFuncSetAttribute", __FILE__, __LINE__)))
-                break;
-        }
-        const char *ng = std::getenv("CUFIL_NO_GRAPH");
-        s->use_graph = !(ng && ng[0] == '1');
-    } while (0);
-    if (rc != CF_OK) {
-        std::string msg = cf_last_error();
-        cf_sim_destroy(s);
-        set_error(rc, "%s", msg.c_str());
-        return rc;
-    }
-    *out = s;
-    return CF_OK;
+    return create_handle<cf_sim>(cfg, 1, out, "cf_sim_create");
 }
 
 extern "C" int cf_sim_destroy(cf_sim *s) {
     if (!s) return CF_OK;
-    cudaSetDevice(s->cfg.device);
-    if (s->stream) cudaStreamSynchronize(s->stream);
-    if (s->exec) cudaGraphExecDestroy(s->exec);
-    if (s->graph) cudaGraphDestroy(s->graph);
-    for (void *p : s->allocations) cudaFree(p);
-    if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    engine_release(s);
     delete s;
     return CF_OK;
 }
@@ -443,19 +874,19 @@ extern "C" int cf_sim_step_async(cf_sim *s, int nt) {
     clear_error();
     CF_REQUIRE(s, "null handle");
     CF_REQUIRE(nt >= 0, "cf_sim_step: nt must be >= 0");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
+    CF_CUDA(cudaSetDevice(s->device));
     return run_step(s, nt);
 }
 
 extern "C" int cf_sim_last_solve(cf_sim *s, int *iters, double *relres) {
     clear_error();
     CF_REQUIRE(s, "null handle");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
-    GmresCtl c;
-    CF_TRY(read_ctl(s, &c));
-    if (iters) *iters = (c.status == kGmresConverged || c.status == kGmresMaxIter) ? c.iters : 0;
-    if (relres) *relres = c.relres;
-    return status_of(c);
+    CF_CUDA(cudaSetDevice(s->device));
+    std::vector<GmresCtl> c;
+    CF_TRY(read_ctls(s, c));
+    if (iters) *iters = iters_of(c[0]);
+    if (relres) *relres = c[0].relres;
+    return status_of(c[0], 0, 1);
 }
 
 extern "C" int cf_sim_step(cf_sim *s, int nt, int *iters, double *relres) {
@@ -466,20 +897,14 @@ extern "C" int cf_sim_step(cf_sim *s, int nt, int *iters, double *relres) {
 extern "C" int cf_sim_get_state(cf_sim *s, double *phase, double *angle, double *phase_dot, double *angle_dot) {
     clear_error();
     CF_REQUIRE(s, "null handle");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
-    const size_t b = sizeof(double) * s->d.F;
-    if (phase) CF_CUDA(cudaMemcpyAsync(phase, s->d.phase, b, cudaMemcpyDeviceToHost, s->stream));
-    if (angle) CF_CUDA(cudaMemcpyAsync(angle, s->d.angle, b, cudaMemcpyDeviceToHost, s->stream));
-    if (phase_dot) CF_CUDA(cudaMemcpyAsync(phase_dot, s->d.phase_dot, b, cudaMemcpyDeviceToHost, s->stream));
-    if (angle_dot) CF_CUDA(cudaMemcpyAsync(angle_dot, s->d.angle_dot, b, cudaMemcpyDeviceToHost, s->stream));
-    CF_CUDA(cudaStreamSynchronize(s->stream));
-    return CF_OK;
+    CF_CUDA(cudaSetDevice(s->device));
+    return copy_state_out(s, phase, angle, phase_dot, angle_dot);
 }
 
 extern "C" int cf_sim_get_segments(cf_sim *s, float *x_segs, float *f_segs) {
     clear_error();
     CF_REQUIRE(s, "null handle");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
+    CF_CUDA(cudaSetDevice(s->device));
     const int N = s->d.N;
     std::vector<double> buf(3 * static_cast<size_t>(N));
     if (x_segs) {
@@ -499,7 +924,7 @@ extern "C" int cf_sim_get_segments(cf_sim *s, float *x_segs, float *f_segs) {
 extern "C" int cf_sim_get_directions(cf_sim *s, double *k_phase, double *k_angle) {
     clear_error();
     CF_REQUIRE(s, "null handle");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
+    CF_CUDA(cudaSetDevice(s->device));
     const size_t b = sizeof(double) * 3 * s->d.N;
     if (k_phase) CF_CUDA(cudaMemcpyAsync(k_phase, s->d.kp, b, cudaMemcpyDeviceToHost, s->stream));
     if (k_angle) CF_CUDA(cudaMemcpyAsync(k_angle, s->d.ka, b, cudaMemcpyDeviceToHost, s->stream));
@@ -510,13 +935,13 @@ extern "C" int cf_sim_get_directions(cf_sim *s, double *k_phase, double *k_angle
 extern "C" int cf_sim_get_arclengths(cf_sim *s, double *s_values) {
     clear_error();
     CF_REQUIRE(s && s_values, "null argument");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
+    CF_CUDA(cudaSetDevice(s->device));
     CF_CUDA(cudaMemcpyAsync(s_values, s->d.s_cur, sizeof(double) * s->d.N, cudaMemcpyDeviceToHost, s->stream));
     CF_CUDA(cudaStreamSynchronize(s->stream));
     return CF_OK;
 }
 
-extern "C" int cf_sim_system_size(cf_sim *s) { return s ? s->d.n : -1; }
+extern "C" int cf_sim_system_size(cf_sim *s) { return s ? s->arr[0].n : -1; }
 
 extern "C" int cf_sim_stream(cf_sim *s, void **stream) {
     clear_error();
@@ -529,35 +954,21 @@ extern "C" int cf_sim_set_state(cf_sim *s, const double *phase, const double *an
                                 const double *angle_dot) {
     clear_error();
     CF_REQUIRE(s, "null handle");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
-    const size_t b = sizeof(double) * s->d.F;
-    if (phase) CF_CUDA(cudaMemcpyAsync(s->d.phase, phase, b, cudaMemcpyHostToDevice, s->stream));
-    if (angle) CF_CUDA(cudaMemcpyAsync(s->d.angle, angle, b, cudaMemcpyHostToDevice, s->stream));
-    // the rates are both filament state and the GMRES warm start (mobility_solver.cpp:2298-2388)
-    if (phase_dot) {
-        CF_CUDA(cudaMemcpyAsync(s->d.phase_dot, phase_dot, b, cudaMemcpyHostToDevice, s->stream));
-        if (s->d.po >= 0)
-            CF_CUDA(cudaMemcpyAsync(s->d.sol + s->d.po, phase_dot, b, cudaMemcpyHostToDevice, s->stream));
-    }
-    if (angle_dot) {
-        CF_CUDA(cudaMemcpyAsync(s->d.angle_dot, angle_dot, b, cudaMemcpyHostToDevice, s->stream));
-        if (s->d.ao >= 0)
-            CF_CUDA(cudaMemcpyAsync(s->d.sol + s->d.ao, angle_dot, b, cudaMemcpyHostToDevice, s->stream));
-    }
-    return CF_OK;
+    CF_CUDA(cudaSetDevice(s->device));
+    return copy_state_in(s, phase, angle, phase_dot, angle_dot);
 }
 
 extern "C" int cf_sim_iteration_log(cf_sim *s, int *iters, int n) {
     clear_error();
     CF_REQUIRE(s && iters && n >= 0 && n <= kIterLogCap, "cf_sim_iteration_log: bad arguments");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
+    CF_CUDA(cudaSetDevice(s->device));
     CF_CUDA(cudaMemcpyAsync(iters, s->d.iter_log, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream));
     CF_CUDA(cudaStreamSynchronize(s->stream));
     return CF_OK;
 }
 
 extern "C" int cf_sim_launches_per_step(cf_sim *s, int iters) {
-    // set_nt + kinematics, rhs, tiles, epilogue, residual + 7 per iteration + backsub, combine, finish
+    // step_begin + kinematics, rhs, pair, epilogue, residual + 7 per iteration + backsub, combine, finish
     (void)s;
     return 1 + 5 + 7 * iters + 3;
 }
@@ -565,9 +976,8 @@ extern "C" int cf_sim_launches_per_step(cf_sim *s, int iters) {
 extern "C" int cf_sim_initial_guess(cf_sim *s, int nt) {
     clear_error();
     CF_REQUIRE(s, "null handle");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
-    set_nt_kernel<<<1, 1, 0, s->stream>>>(s->d.ctl, nt);
-    CF_CHECK_LAUNCH("set_nt_kernel");
+    CF_CUDA(cudaSetDevice(s->device));
+    CF_TRY(launch_step_begin(s, nt, s->stream));
     CF_TRY(launch_kinematics(s, s->stream));
     CF_CUDA(cudaStreamSynchronize(s->stream));
     return CF_OK;
@@ -576,11 +986,11 @@ extern "C" int cf_sim_initial_guess(cf_sim *s, int nt) {
 extern "C" int cf_sim_assemble_rhs(cf_sim *s, int nt, double *rhs) {
     clear_error();
     CF_REQUIRE(s && rhs, "null argument");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
-    set_nt_kernel<<<1, 1, 0, s->stream>>>(s->d.ctl, nt);
+    CF_CUDA(cudaSetDevice(s->device));
+    CF_TRY(launch_step_begin(s, nt, s->stream));
     rhs_kernel<<<s->d.F, s->fil_threads, 0, s->stream>>>(s->d);
     CF_CHECK_LAUNCH("rhs_kernel");
-    CF_CUDA(cudaMemcpyAsync(rhs, s->d.rhs, sizeof(double) * s->d.n, cudaMemcpyDeviceToHost, s->stream));
+    CF_CUDA(cudaMemcpyAsync(rhs, s->d.rhs, sizeof(double) * s->arr[0].n, cudaMemcpyDeviceToHost, s->stream));
     CF_CUDA(cudaStreamSynchronize(s->stream));
     return CF_OK;
 }
@@ -588,8 +998,8 @@ extern "C" int cf_sim_assemble_rhs(cf_sim *s, int nt, double *rhs) {
 extern "C" int cf_sim_apply_preconditioner(cf_sim *s, const double *in, double *out) {
     clear_error();
     CF_REQUIRE(s && in && out, "null argument");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
-    const size_t b = sizeof(double) * s->d.n;
+    CF_CUDA(cudaSetDevice(s->device));
+    const size_t b = sizeof(double) * s->arr[0].n;
     CF_CUDA(cudaMemcpyAsync(s->d.t, in, b, cudaMemcpyHostToDevice, s->stream));
     precond_kernel<<<s->d.F, s->fil_threads, s->pre_smem, s->stream>>>(s->d, s->d.t, s->d.t);
     CF_CHECK_LAUNCH("precond_kernel");
@@ -601,8 +1011,9 @@ extern "C" int cf_sim_apply_preconditioner(cf_sim *s, const double *in, double *
 extern "C" int cf_sim_system_matvec(cf_sim *s, const double *in, double *out) {
     clear_error();
     CF_REQUIRE(s && in && out, "null argument");
-    CF_CUDA(cudaSetDevice(s->cfg.device));
-    const size_t b = sizeof(double) * s->d.n;
+    CF_CUDA(cudaSetDevice(s->device));
+    const size_t b = sizeof(double) * s->arr[0].n;
+    CF_TRY(launch_step_begin(s, -1, s->stream));  // every array active for the product
     CF_CUDA(cudaMemcpyAsync(s->d.z, in, b, cudaMemcpyHostToDevice, s->stream));
     pack_forces_kernel<<<(s->d.N + 255) / 256, 256, 0, s->stream>>>(s->d, s->d.z);
     CF_CHECK_LAUNCH("pack_forces_kernel");
@@ -610,6 +1021,155 @@ extern "C" int cf_sim_system_matvec(cf_sim *s, const double *in, double *out) {
     CF_CHECK_LAUNCH("filament_rows_kernel");
     CF_TRY(launch_matvec_tail(s, s->d.z, s->d.w, s->stream));
     CF_CUDA(cudaMemcpyAsync(out, s->d.w, b, cudaMemcpyDeviceToHost, s->stream));
-    GmresCtl c;
-    return read_ctl(s, &c);
+    LoopCtl lc;
+    return read_loop(s, &lc);
+}
+
+extern "C" int cf_sim_autotune(cf_sim *s, int k_hint, int *choice) {
+    clear_error();
+    CF_REQUIRE(s, "null handle");
+    CF_CUDA(cudaSetDevice(s->device));
+    return engine_autotune(s, k_hint, choice);
+}
+
+extern "C" int cf_sim_set_tuning(cf_sim *s, const int *choice) {
+    clear_error();
+    CF_REQUIRE(s, "null handle");
+    CF_CUDA(cudaSetDevice(s->device));
+    return engine_set_tuning(s, choice);
+}
+
+extern "C" int cf_sim_get_tuning(cf_sim *s, int *choice) {
+    clear_error();
+    CF_REQUIRE(s && choice, "null argument");
+    engine_get_tuning(s, choice);
+    return CF_OK;
+}
+
+// =================================================================== cf_batch
+extern "C" int cf_batch_create(const cf_sim_config *cfgs, int n_arrays, cf_batch **out) {
+    return create_handle<cf_batch>(cfgs, n_arrays, out, "cf_batch_create");
+}
+
+extern "C" int cf_batch_destroy(cf_batch *bt) {
+    if (!bt) return CF_OK;
+    engine_release(bt);
+    delete bt;
+    return CF_OK;
+}
+
+extern "C" int cf_batch_shape(cf_batch *bt, int *n_arrays, int *n_fil, int *n_seg, int *sizes) {
+    clear_error();
+    CF_REQUIRE(bt, "null handle");
+    if (n_arrays) *n_arrays = bt->B;
+    if (n_fil) *n_fil = bt->d.F;
+    if (n_seg) *n_seg = bt->d.N;
+    if (sizes)
+        for (int b = 0; b < bt->B; ++b) sizes[b] = bt->arr[b].n;
+    return CF_OK;
+}
+
+extern "C" int cf_batch_step_async(cf_batch *bt, int nt) {
+    clear_error();
+    CF_REQUIRE(bt, "null handle");
+    CF_REQUIRE(nt >= 0, "cf_batch_step: nt must be >= 0");
+    CF_CUDA(cudaSetDevice(bt->device));
+    return run_step(bt, nt);
+}
+
+extern "C" int cf_batch_last_solve(cf_batch *bt, int *iters, double *relres, int *status) {
+    clear_error();
+    CF_REQUIRE(bt, "null handle");
+    CF_CUDA(cudaSetDevice(bt->device));
+    std::vector<GmresCtl> c;
+    CF_TRY(read_ctls(bt, c));
+    for (int b = 0; b < bt->B; ++b) {
+        if (iters) iters[b] = iters_of(c[b]);
+        if (relres) relres[b] = c[b].relres;
+        if (status) status[b] = c[b].status;
+    }
+    return batch_status(c);
+}
+
+extern "C" int cf_batch_step(cf_batch *bt, int nt, int *iters, double *relres) {
+    CF_TRY(cf_batch_step_async(bt, nt));
+    return cf_batch_last_solve(bt, iters, relres, nullptr);
+}
+
+extern "C" int cf_batch_get_state(cf_batch *bt, double *phase, double *angle, double *phase_dot, double *angle_dot) {
+    clear_error();
+    CF_REQUIRE(bt, "null handle");
+    CF_CUDA(cudaSetDevice(bt->device));
+    return copy_state_out(bt, phase, angle, phase_dot, angle_dot);
+}
+
+extern "C" int cf_batch_set_state(cf_batch *bt, const double *phase, const double *angle, const double *phase_dot,
+                                  const double *angle_dot) {
+    clear_error();
+    CF_REQUIRE(bt, "null handle");
+    CF_CUDA(cudaSetDevice(bt->device));
+    return copy_state_in(bt, phase, angle, phase_dot, angle_dot);
+}
+
+extern "C" int cf_batch_get_segments(cf_batch *bt, double *x_segs) {
+    clear_error();
+    CF_REQUIRE(bt && x_segs, "null argument");
+    CF_CUDA(cudaSetDevice(bt->device));
+    CF_CUDA(cudaMemcpyAsync(x_segs, bt->d.xd, sizeof(double) * 3 * bt->d.N, cudaMemcpyDeviceToHost, bt->stream));
+    CF_CUDA(cudaStreamSynchronize(bt->stream));
+    return CF_OK;
+}
+
+extern "C" int cf_batch_get_solution(cf_batch *bt, int array, double *sol) {
+    clear_error();
+    CF_REQUIRE(bt && sol && array >= 0 && array < bt->B, "cf_batch_get_solution: bad arguments");
+    CF_CUDA(cudaSetDevice(bt->device));
+    const ArrayInfo &a = bt->arr[array];
+    CF_CUDA(cudaMemcpyAsync(sol, bt->d.sol + a.voff, sizeof(double) * a.n, cudaMemcpyDeviceToHost, bt->stream));
+    CF_CUDA(cudaStreamSynchronize(bt->stream));
+    return CF_OK;
+}
+
+extern "C" int cf_batch_iteration_log(cf_batch *bt, int array, int *iters, int n) {
+    clear_error();
+    CF_REQUIRE(bt && iters && array >= 0 && array < bt->B && n >= 0 && n <= kIterLogCap,
+               "cf_batch_iteration_log: bad arguments");
+    CF_CUDA(cudaSetDevice(bt->device));
+    CF_CUDA(cudaMemcpyAsync(iters, bt->d.iter_log + static_cast<size_t>(array) * kIterLogCap, sizeof(int) * n,
+                            cudaMemcpyDeviceToHost, bt->stream));
+    CF_CUDA(cudaStreamSynchronize(bt->stream));
+    return CF_OK;
+}
+
+extern "C" int cf_batch_stream(cf_batch *bt, void **stream) {
+    clear_error();
+    CF_REQUIRE(bt && stream, "null argument");
+    *stream = static_cast<void *>(bt->stream);
+    return CF_OK;
+}
+
+extern "C" int cf_batch_launches_per_step(cf_batch *bt, int loop_iters) {
+    (void)bt;
+    return 1 + 5 + 7 * loop_iters + 3;
+}
+
+extern "C" int cf_batch_autotune(cf_batch *bt, int k_hint, int *choice) {
+    clear_error();
+    CF_REQUIRE(bt, "null handle");
+    CF_CUDA(cudaSetDevice(bt->device));
+    return engine_autotune(bt, k_hint, choice);
+}
+
+extern "C" int cf_batch_set_tuning(cf_batch *bt, const int *choice) {
+    clear_error();
+    CF_REQUIRE(bt, "null handle");
+    CF_CUDA(cudaSetDevice(bt->device));
+    return engine_set_tuning(bt, choice);
+}
+
+extern "C" int cf_batch_get_tuning(cf_batch *bt, int *choice) {
+    clear_error();
+    CF_REQUIRE(bt && choice, "null argument");
+    engine_get_tuning(bt, choice);
+    return CF_OK;
 }

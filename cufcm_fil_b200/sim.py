@@ -30,40 +30,47 @@ class GmresResult:
     status: int
 
 
+def _sim_config(keep: list, *, bases, nseg=20, seg_sep=2.6, beat=_lib.CF_BEAT_FULFORD_BLAKE, dt=1.0 / 300,
+                dynamic_phase=True, dynamic_angle=True, spring_factor=0.01, gmres_tol=1e-6, gmres_max_iter=350,
+                precond=_lib.CF_PRECOND_BLOCK_DIAG, omega0=None, phase0=None, angle0=None, phase_refs=None,
+                angle_refs=None, s_table=None, s_tol_factor=0.0, device=0):
+    """cf_sim_config of one array; the arrays it points to are appended to `keep` (kept alive by the caller)."""
+    bases = np.ascontiguousarray(bases, np.float64).reshape(-1, 3)
+    keep.append(bases)
+    f = bases.shape[0]
+
+    def arr(x, n=None):
+        if x is None:
+            return None
+        a = np.ascontiguousarray(x, np.float64).ravel()
+        if n is not None:
+            assert a.size == n, (a.size, n)
+        keep.append(a)
+        return a
+
+    om, ph, an = arr(omega0, f), arr(phase0, f), arr(angle0, f)
+    pr, ar = arr(phase_refs), arr(angle_refs)
+    st = None if s_table is None else np.ascontiguousarray(s_table, np.float64)
+    if st is not None:
+        keep.append(st)
+    return _lib.SimConfig(
+        n_fil=f, n_seg=int(nseg), seg_sep=float(seg_sep), beat=int(beat), dynamic_phase=int(bool(dynamic_phase)),
+        dynamic_angle=int(bool(dynamic_angle)), dt=float(dt), spring_factor=float(spring_factor),
+        gmres_tol=float(gmres_tol), gmres_max_iter=int(gmres_max_iter), precond=int(precond),
+        base_pos=_p(bases), omega0=_p(om), phase0=_p(ph), angle0=_p(an),
+        gen_phase_force_refs=_p(pr), n_gen_phase_refs=0 if pr is None else pr.size,
+        gen_angle_force_refs=_p(ar), n_gen_angle_refs=0 if ar is None else ar.size,
+        s_values_ref=_p(st), s_ref_rows=0 if st is None else st.shape[0],
+        s_ref_cols=0 if st is None else st.shape[1], s_tol_factor=float(s_tol_factor), device=int(device))
+
+
 class WallCiliaSimulation:
-    def __init__(self, *, bases, nseg=20, seg_sep=2.6, beat=_lib.CF_BEAT_FULFORD_BLAKE, dt=1.0 / 300,
-                 dynamic_phase=True, dynamic_angle=True, spring_factor=0.01, gmres_tol=1e-6, gmres_max_iter=350,
-                 precond=_lib.CF_PRECOND_BLOCK_DIAG, omega0=None, phase0=None, angle0=None, phase_refs=None,
-                 angle_refs=None, s_table=None, s_tol_factor=0.0, device=0):
+    def __init__(self, *, bases, nseg=20, **kw):
         self.bases = np.ascontiguousarray(bases, np.float64).reshape(-1, 3)
         self.n_fil = self.bases.shape[0]
         self.nseg = int(nseg)
-        f = self.n_fil
         self._keep = []
-
-        def arr(x, n=None):
-            if x is None:
-                return None
-            a = np.ascontiguousarray(x, np.float64).ravel()
-            if n is not None:
-                assert a.size == n, (a.size, n)
-            self._keep.append(a)
-            return a
-
-        om, ph, an = arr(omega0, f), arr(phase0, f), arr(angle0, f)
-        pr, ar = arr(phase_refs), arr(angle_refs)
-        st = None if s_table is None else np.ascontiguousarray(s_table, np.float64)
-        if st is not None:
-            self._keep.append(st)
-        cfg = _lib.SimConfig(
-            n_fil=f, n_seg=self.nseg, seg_sep=float(seg_sep), beat=int(beat), dynamic_phase=int(bool(dynamic_phase)),
-            dynamic_angle=int(bool(dynamic_angle)), dt=float(dt), spring_factor=float(spring_factor),
-            gmres_tol=float(gmres_tol), gmres_max_iter=int(gmres_max_iter), precond=int(precond),
-            base_pos=_p(self.bases), omega0=_p(om), phase0=_p(ph), angle0=_p(an),
-            gen_phase_force_refs=_p(pr), n_gen_phase_refs=0 if pr is None else pr.size,
-            gen_angle_force_refs=_p(ar), n_gen_angle_refs=0 if ar is None else ar.size,
-            s_values_ref=_p(st), s_ref_rows=0 if st is None else st.shape[0],
-            s_ref_cols=0 if st is None else st.shape[1], s_tol_factor=float(s_tol_factor), device=int(device))
+        cfg = _sim_config(self._keep, bases=self.bases, nseg=nseg, **kw)
         h = ctypes.c_void_p()
         _lib.call("cf_sim_create", ctypes.byref(cfg), ctypes.byref(h))
         self._h = h
@@ -150,6 +157,21 @@ class WallCiliaSimulation:
     def launches_per_step(self, iters: int) -> int:
         return _lib.load().cf_sim_launches_per_step(self._h, int(iters))
 
+    def autotune(self, k_hint: int = 0) -> dict:
+        """Times the iteration kernels' launch shapes on the current state and keeps the fastest."""
+        c = np.zeros(len(_TUNING_KEYS), np.int32)
+        _lib.call("cf_sim_autotune", self._h, int(k_hint), ctypes.c_void_p(c.ctypes.data))
+        return _tuning_dict(c)
+
+    def tuning(self) -> dict:
+        c = np.zeros(len(_TUNING_KEYS), np.int32)
+        _lib.call("cf_sim_get_tuning", self._h, ctypes.c_void_p(c.ctypes.data))
+        return _tuning_dict(c)
+
+    def set_tuning(self, **kw):
+        c = _tuning_array(self.tuning(), kw)
+        _lib.call("cf_sim_set_tuning", self._h, ctypes.c_void_p(c.ctypes.data))
+
     def state(self):
         f = self.n_fil
         ph, an, pd, ad = (np.zeros(f) for _ in range(4))
@@ -217,3 +239,145 @@ def arclength_table(beat=_lib.CF_BEAT_FULFORD_BLAKE, nseg=20, seg_sep=2.6, steps
             sim.initial_guess(nt)
             out[nt] = sim.arclengths()[0]
     return out
+
+
+_TUNING_KEYS = ("pair_ctas_per_sm", "dots_chunk", "dots_blocks_per_sm", "update_blocks_per_sm", "update_rows")
+
+
+def _tuning_dict(c) -> dict:
+    return {k: int(v) for k, v in zip(_TUNING_KEYS, c)}
+
+
+def _tuning_array(cur: dict, kw: dict) -> np.ndarray:
+    unknown = set(kw) - set(_TUNING_KEYS)
+    if unknown:
+        raise ValueError(f"unknown tuning keys {sorted(unknown)}")
+    cur = dict(cur, **kw)
+    return np.asarray([cur[k] for k in _TUNING_KEYS], np.int32)
+
+
+class WallCiliaBatch:
+    """Many independent wall arrays of uneven size stepped together (cf_batch).
+
+    ``arrays`` is a list of per-array keyword dicts for the array-specific
+    settings (``bases`` and optionally ``omega0``, ``phase0``, ``angle0``);
+    every other setting is shared and given as keyword arguments, with the
+    same meaning as for :class:`WallCiliaSimulation`.  Each array runs its own
+    GMRES; per-array results come back as arrays of length ``n_arrays`` and
+    per-filament state is split into one array per cilia array."""
+
+    def __init__(self, arrays, nseg=20, **shared):
+        self._keep = []
+        cfgs = (_lib.SimConfig * len(arrays))()
+        self.n_fils = []
+        for b, spec in enumerate(arrays):
+            merged = dict(shared, **spec)
+            merged.setdefault("nseg", nseg)
+            cfgs[b] = _sim_config(self._keep, **merged)
+            self.n_fils.append(cfgs[b].n_fil)
+        self.n_arrays = len(arrays)
+        self.nseg = int(nseg)
+        h = ctypes.c_void_p()
+        _lib.call("cf_batch_create", cfgs, len(arrays), ctypes.byref(h))
+        self._h = h
+        sizes = np.zeros(self.n_arrays, np.int32)
+        nf, ns = ctypes.c_int(), ctypes.c_int()
+        _lib.call("cf_batch_shape", self._h, None, ctypes.byref(nf), ctypes.byref(ns), _p(sizes))
+        self.sizes = sizes
+        self.n_fil_total = nf.value
+        self.n_seg_total = ns.value
+        self._fil_split = np.cumsum(self.n_fils)[:-1]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.call("cf_batch_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step(self, nt: int):
+        """One implicit step of every array; returns (iterations, relative residuals, status code)."""
+        it = np.zeros(self.n_arrays, np.int32)
+        rel = np.zeros(self.n_arrays)
+        rc = _lib.call("cf_batch_step", self._h, int(nt), _p(it), _p(rel),
+                       ok=(_lib.CF_OK, _lib.CF_NOT_CONVERGED))
+        return it, rel, rc
+
+    def step_async(self, nt: int):
+        _lib.call("cf_batch_step_async", self._h, int(nt))
+
+    def last_solve(self):
+        """(iterations, relative residuals, per-array GMRES status, worst status code)."""
+        it = np.zeros(self.n_arrays, np.int32)
+        rel = np.zeros(self.n_arrays)
+        st = np.zeros(self.n_arrays, np.int32)
+        rc = _lib.call("cf_batch_last_solve", self._h, _p(it), _p(rel), _p(st),
+                       ok=(_lib.CF_OK, _lib.CF_NOT_CONVERGED, _lib.CF_NONFINITE))
+        return it, rel, st, rc
+
+    def state(self):
+        """Filament state, one list entry per array: dicts of phase, angle, phase_dot, angle_dot."""
+        f = self.n_fil_total
+        ph, an, pd, ad = (np.zeros(f) for _ in range(4))
+        _lib.call("cf_batch_get_state", self._h, _p(ph), _p(an), _p(pd), _p(ad))
+        parts = [np.split(a, self._fil_split) for a in (ph, an, pd, ad)]
+        return [dict(phase=p, angle=a, phase_dot=q, angle_dot=r) for p, a, q, r in zip(*parts)]
+
+    def set_state(self, phase=None, angle=None, phase_dot=None, angle_dot=None):
+        """Per-filament state concatenated over the arrays (float64; any may be None)."""
+        keep = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (phase, angle, phase_dot,
+                                                                                      angle_dot)]
+        _lib.call("cf_batch_set_state", self._h, *(_p(a) for a in keep))
+        _lib.call("cf_batch_get_state", self._h, None, None, None, None)  # waits for the uploads
+
+    def segments(self):
+        """Segment positions per array, [n_fil * nseg, 3] float64 each."""
+        x = np.zeros(3 * self.n_seg_total)
+        _lib.call("cf_batch_get_segments", self._h, _p(x))
+        x = x.reshape(-1, 3)
+        return np.split(x, np.cumsum(self.n_fils)[:-1] * self.nseg)
+
+    def tips(self):
+        return [s.reshape(-1, self.nseg, 3)[:, -1, :] for s in self.segments()]
+
+    def solution(self, array: int) -> np.ndarray:
+        out = np.zeros(int(self.sizes[array]))
+        _lib.call("cf_batch_get_solution", self._h, int(array), _p(out))
+        return out
+
+    def iteration_log(self, array: int, n: int) -> np.ndarray:
+        out = np.zeros(n, np.int32)
+        _lib.call("cf_batch_iteration_log", self._h, int(array), _p(out), int(n))
+        return out
+
+    def stream_handle(self) -> int:
+        h = ctypes.c_void_p()
+        _lib.call("cf_batch_stream", self._h, ctypes.byref(h))
+        return h.value or 0
+
+    def launches_per_step(self, loop_iters: int) -> int:
+        return _lib.load().cf_batch_launches_per_step(self._h, int(loop_iters))
+
+    def autotune(self, k_hint: int = 0) -> dict:
+        c = np.zeros(len(_TUNING_KEYS), np.int32)
+        _lib.call("cf_batch_autotune", self._h, int(k_hint), _p(c))
+        return _tuning_dict(c)
+
+    def tuning(self) -> dict:
+        c = np.zeros(len(_TUNING_KEYS), np.int32)
+        _lib.call("cf_batch_get_tuning", self._h, _p(c))
+        return _tuning_dict(c)
+
+    def set_tuning(self, **kw):
+        c = _tuning_array(self.tuning(), kw)
+        _lib.call("cf_batch_set_tuning", self._h, _p(c))

@@ -269,6 +269,56 @@ CF_API int cf_sim_apply_preconditioner(cf_sim *s, const double *in, double *out)
 /* system_matrix_mult_new: out = A in (host vectors, system size). */
 CF_API int cf_sim_system_matvec(cf_sim *s, const double *in, double *out);
 
+/* Launch shapes of the iteration kernels: choice[5] = {pair-kernel CTAs per
+ * SM, dot-product row chunk, dot-product blocks per SM, update blocks per SM,
+ * update tile rows (32, 64, 128 or 256)}.
+ * cf_sim_autotune times the candidates on the handle's current state (basis
+ * index k_hint, <= 0: half the last step's iterations) and keeps the fastest;
+ * only scratch buffers are written.  choice may be NULL. */
+CF_API int cf_sim_autotune(cf_sim *s, int k_hint, int *choice);
+CF_API int cf_sim_set_tuning(cf_sim *s, const int *choice);
+CF_API int cf_sim_get_tuning(cf_sim *s, int *choice);
+
+/* ------------------------------------------------------------------------
+ * Batches of independent arrays (periodic-orbit / bisection sweeps): many
+ * wall arrays of uneven size stepped together, one graph launch per step for
+ * the whole batch.  Each array is described by its own cf_sim_config; every
+ * field except n_fil, base_pos, omega0, phase0 and angle0 must equal array
+ * 0's.  Per-filament arrays (state) are concatenated array by array.  Each
+ * array runs its own GMRES (own Krylov basis, Hessenberg matrix and stopping
+ * test); arrays that stopped are masked out of the remaining iterations, so
+ * every array gets the result its own cf_sim would give.
+ * ------------------------------------------------------------------------ */
+typedef struct cf_batch cf_batch;
+
+CF_API int cf_batch_create(const cf_sim_config *cfgs, int n_arrays, cf_batch **out);
+CF_API int cf_batch_destroy(cf_batch *b);
+/* Arrays, filaments and segments in the batch; sizes[n_arrays] = system sizes (may be NULL). */
+CF_API int cf_batch_shape(cf_batch *b, int *n_arrays, int *n_fil, int *n_seg, int *sizes);
+/* One implicit step nt of every array; iters/relres [n_arrays] may be NULL.
+ * Returns CF_NONFINITE if any array met a non-finite value, else
+ * CF_NOT_CONVERGED if any array stopped at its cap. */
+CF_API int cf_batch_step(cf_batch *b, int nt, int *iters, double *relres);
+CF_API int cf_batch_step_async(cf_batch *b, int nt);
+/* Result of the last solve per array (status: 1 converged, 2 cap, 3 non-finite,
+ * 4 initial guess good, 5 zero right-hand side); any pointer may be NULL. */
+CF_API int cf_batch_last_solve(cf_batch *b, int *iters, double *relres, int *status);
+CF_API int cf_batch_get_state(cf_batch *b, double *phase, double *angle, double *phase_dot, double *angle_dot);
+CF_API int cf_batch_set_state(cf_batch *b, const double *phase, const double *angle, const double *phase_dot,
+                              const double *angle_dot);
+/* Segment positions [3*N_s total], FP64, array by array. */
+CF_API int cf_batch_get_segments(cf_batch *b, double *x_segs);
+/* Saddle-point solution of one array [its system size]. */
+CF_API int cf_batch_get_solution(cf_batch *b, int array, double *sol);
+CF_API int cf_batch_iteration_log(cf_batch *b, int array, int *iters, int n);
+CF_API int cf_batch_stream(cf_batch *b, void **stream);
+/* Kernels launched by one step whose GMRES loop ran loop_iters iterations
+ * (the largest iteration count in the batch). */
+CF_API int cf_batch_launches_per_step(cf_batch *b, int loop_iters);
+CF_API int cf_batch_autotune(cf_batch *b, int k_hint, int *choice);
+CF_API int cf_batch_set_tuning(cf_batch *b, const int *choice);
+CF_API int cf_batch_get_tuning(cf_batch *b, int *choice);
+
 #ifdef __cplusplus
 }
 #endif
