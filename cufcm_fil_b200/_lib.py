@@ -26,6 +26,7 @@ CF_BEAT_FULFORD_BLAKE_ORIGINAL = 4
 CF_PRECOND_NONE = 0
 CF_PRECOND_BLOCK_DIAG = 1
 CF_PRECOND_LEARNED = 2
+CF_PRECOND_LINE = 3
 
 _STATUS_NAMES = {0: "CF_OK", 1: "CF_EINVAL", 2: "CF_ENOMEM", 3: "CF_ECUDA", 4: "CF_NOT_CONVERGED",
                  5: "CF_NONFINITE", 6: "CF_TIMEOUT", 7: "CF_ENOTSUP"}
@@ -56,7 +57,8 @@ class SimConfig(ctypes.Structure):
                 ("gen_phase_force_refs", ctypes.c_void_p), ("n_gen_phase_refs", ctypes.c_int),
                 ("gen_angle_force_refs", ctypes.c_void_p), ("n_gen_angle_refs", ctypes.c_int),
                 ("s_values_ref", ctypes.c_void_p), ("s_ref_rows", ctypes.c_int), ("s_ref_cols", ctypes.c_int),
-                ("s_tol_factor", ctypes.c_double), ("device", ctypes.c_int)]
+                ("s_tol_factor", ctypes.c_double), ("device", ctypes.c_int),
+                ("line_patch", ctypes.c_int), ("precond_refresh", ctypes.c_int)]
 
 
 class FcmConfig(ctypes.Structure):

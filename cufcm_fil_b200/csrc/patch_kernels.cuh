@@ -1,0 +1,310 @@
+// patch_kernels.cuh -- line-patch block-Jacobi preconditioner of the implicit step.
+//
+// Filaments are grouped into patches of up to P neighbours along a lattice
+// line in the beat direction (the beat plane of the wall frame is y-z, so a
+// patch is a run of filaments with equal x, consecutive in y).  Each patch's
+// saddle-point block
+//     [ M_pp   -K_p ]      M_pp : wall RPY mobility of all segments of the patch
+//     [ -K_p^T   0  ]      K_p  : velocity directions (K_phase, K_angle) per filament
+// -- the same operator as system_matrix_mult_new (mobility_solver.cpp:1887-2105)
+// restricted to the patch -- is assembled in FP32 and inverted in place by a
+// blocked Gauss-Jordan elimination without pivoting, in per-filament order
+// ([3*nseg lambda | phase rate | angle rate] per filament): every 62-unknown
+// filament block is eliminated lambda-first, so the rate pivots are Schur
+// complements -k^T M^-1 k and stay away from zero.  The preconditioner is
+// P^-1 r = blockdiag(A_pp^-1) r; it replaces apply_preconditioner_new
+// (mobility_solver.cpp:1102-1243), whose block-diagonal form (6 pi a on the
+// forces, a 2x2 Schur solve for the rates) remains the fallback of any patch
+// whose inverse is not finite.  The GMRES residual is always formed with the
+// exact operator, so the patch inverses change only the iteration count.
+//
+// Cost: one refresh is sum_p n_p^3 FP32 FMAs (n_p = 62 * filaments), done as
+// ceil(n/32) rounds of (a) inverting the 32x32 pivot block and scaling the
+// pivot rows (one block per patch) and (b) a rank-32 update of the rest of the
+// matrix in 64x64 tiles.  One application is a dense n_p x n_p product per
+// patch, reading the FP32 inverses once.
+#pragma once
+
+#include "rpy_pairs.cuh"
+#include "sim_kernels.cuh"
+
+namespace cufil {
+
+constexpr int kGjBlock = 32;  // pivot block of the Gauss-Jordan rounds
+constexpr int kGjTile = 64;   // tile of the rank-32 updates
+
+struct PatchDev {
+    int np;                  // patches
+    int nbf;                 // unknowns per filament (3*nseg + rate rows)
+    int max_n;               // largest patch system
+    const int *fil0;         // first entry of each patch in `fils` [np]
+    const int *nf;           // filaments per patch [np]
+    const int *fils;         // filament ids (batch numbering), patch by patch
+    const long long *moff;   // first float of each patch matrix [np]
+    const long long *roff;   // first entry of each patch in `rows` [np]
+    const long long *rows;   // batch-vector row of each local unknown
+    float *A;                // patch matrices, then their inverses (row-major n x n)
+    float *cbuf;             // pivot-column copies, [np][max_n][kGjBlock]
+    int *ok;                 // [np] 1 when the inverse is finite
+};
+
+// Mobility entries: one thread per (target segment, source segment) pair of a
+// patch; writes the 3x3 block into the lambda rows / columns.
+__global__ void patch_mobility_kernel(SimDev d, PatchDev P) {
+    const int p = blockIdx.y;
+    const int nfp = P.nf[p];
+    const int ns = nfp * d.nseg;
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<long long>(ns) * ns) return;
+    const int si = static_cast<int>(t / ns), sj = static_cast<int>(t - static_cast<long long>(si) * ns);
+    const int ai = si / d.nseg, ki = si - ai * d.nseg;
+    const int aj = sj / d.nseg, kj = sj - aj * d.nseg;
+    const int gi = P.fils[P.fil0[p] + ai] * d.nseg + ki;
+    const int gj = P.fils[P.fil0[p] + aj] * d.nseg + kj;
+    const int n = nfp * P.nbf;
+    float *A = P.A + P.moff[p];
+    const long long r0 = static_cast<long long>(ai) * P.nbf + 3 * ki;
+    const long long c0 = static_cast<long long>(aj) * P.nbf + 3 * kj;
+    const float zi = static_cast<float>(d.xd[3 * gi + 2]);
+    for (int c = 0; c < 3; ++c) {
+        float f[3] = {0.0f, 0.0f, 0.0f}, v[3] = {0.0f, 0.0f, 0.0f};
+        f[c] = 1.0f;
+        if (gi == gj) {
+            wall_self_f32<3, 3>(zi, f, v);
+        } else {
+            const float dx = static_cast<float>(d.xd[3 * gi] - d.xd[3 * gj]);
+            const float dy = static_cast<float>(d.xd[3 * gi + 1] - d.xd[3 * gj + 1]);
+            const float dz = static_cast<float>(d.xd[3 * gi + 2] - d.xd[3 * gj + 2]);
+            wall_pair_f32<3, 3>(dx, dy, dz, zi, static_cast<float>(d.xd[3 * gj + 2]), f, v);
+        }
+        for (int q = 0; q < 3; ++q) A[(r0 + q) * n + c0 + c] = v[q];
+    }
+}
+
+// Rate entries -K / -K^T of each filament of a patch (one block per patch).
+__global__ void patch_rates_kernel(SimDev d, PatchDev P) {
+    const int p = blockIdx.x;
+    const int nfp = P.nf[p];
+    const int n = nfp * P.nbf;
+    const int nl = 3 * d.nseg;
+    float *A = P.A + P.moff[p];
+    for (int e = threadIdx.x; e < nfp * nl; e += blockDim.x) {
+        const int a = e / nl, li = e - a * nl;
+        const int g3 = 3 * P.fils[P.fil0[p] + a] * d.nseg + li;  // entry of kp / ka
+        const long long r = static_cast<long long>(a) * P.nbf + li;
+        long long c = static_cast<long long>(a) * P.nbf + nl;
+        if (d.dyn_phase) {
+            const float v = -static_cast<float>(d.kp[g3]);
+            A[r * n + c] = v;
+            A[c * n + r] = v;
+            ++c;
+        }
+        if (d.dyn_angle) {
+            const float v = -static_cast<float>(d.ka[g3]);
+            A[r * n + c] = v;
+            A[c * n + r] = v;
+        }
+    }
+}
+
+// Round K of the blocked Gauss-Jordan inversion, part (a), one block per
+// patch: copies the pivot columns of the other rows to cbuf, inverts the
+// pivot block D in shared memory, scales the pivot rows by D^-1 and stores
+// D^-1 in place.  A non-finite or zero pivot clears the patch's ok flag.
+__global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
+    __shared__ float D[kGjBlock][kGjBlock + 1];
+    __shared__ float col[kGjBlock];
+    __shared__ float inv_piv;
+    const int p = blockIdx.x;
+    const int n = P.nf[p] * P.nbf;
+    const int k0 = K * kGjBlock;
+    if (k0 >= n) return;
+    const int b = min(kGjBlock, n - k0);
+    float *A = P.A + P.moff[p];
+    float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    if (K == 0 && threadIdx.x == 0) P.ok[p] = 1;
+    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) D[e / kGjBlock][e % kGjBlock] = 0.0f;
+    for (int e = threadIdx.x; e < n * kGjBlock; e += blockDim.x) {
+        const int i = e / kGjBlock, s = e - i * kGjBlock;
+        cb[e] = (s < b && (i < k0 || i >= k0 + b)) ? A[static_cast<size_t>(i) * n + k0 + s] : 0.0f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+        const int r = e / b, s = e - r * b;
+        D[r][s] = A[static_cast<size_t>(k0 + r) * n + k0 + s];
+    }
+    __syncthreads();
+    for (int t = 0; t < b; ++t) {
+        if (threadIdx.x < b) col[threadIdx.x] = D[threadIdx.x][t];
+        if (threadIdx.x == 0) {
+            const float piv = D[t][t];
+            if (!(fabsf(piv) > 0.0f) || !isfinite(piv)) P.ok[p] = 0;
+            inv_piv = 1.0f / piv;
+        }
+        __syncthreads();
+        const float ip = inv_piv;
+        for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+            const int r = e / b, s = e - r * b;
+            if (r == t) {
+                D[r][s] = (s == t) ? ip : D[r][s] * ip;
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+            const int r = e / b, s = e - r * b;
+            if (r != t) D[r][s] = (s == t) ? -col[r] * ip : D[r][s] - col[r] * D[t][s];
+        }
+        __syncthreads();
+    }
+    // pivot rows outside the pivot columns: A[K, j] <- D^-1 A[K, j]
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        if (j >= k0 && j < k0 + b) continue;
+        float tmp[kGjBlock];
+#pragma unroll
+        for (int s = 0; s < kGjBlock; ++s) tmp[s] = s < b ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
+        for (int r = 0; r < b; ++r) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int s = 0; s < kGjBlock; ++s) acc += D[r][s] * tmp[s];  // zero beyond b
+            A[static_cast<size_t>(k0 + r) * n + j] = acc;
+        }
+    }
+    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+        const int r = e / b, s = e - r * b;
+        A[static_cast<size_t>(k0 + r) * n + k0 + s] = D[r][s];
+    }
+}
+
+// Round K, part (b): every row outside the pivot rows, in 64x64 tiles:
+//   A[i, j] -= C_i . A[K, j]   (j outside the pivot columns; A[K, j] scaled in (a))
+//   A[i, K]  = -C_i . D^-1     (pivot columns; D^-1 stored in A[K, K])
+// with C_i the row's old pivot-column entries from cbuf.  grid = (tiles, patches).
+__global__ void __launch_bounds__(256) gj_update_kernel(PatchDev P, int K) {
+    __shared__ float Cs[kGjTile][kGjBlock + 1];
+    __shared__ float Rs[kGjBlock][kGjTile + 1];
+    const int p = blockIdx.y;
+    const int n = P.nf[p] * P.nbf;
+    const int k0 = K * kGjBlock;
+    if (k0 >= n) return;
+    const int b = min(kGjBlock, n - k0);
+    const int T = (n + kGjTile - 1) / kGjTile;
+    if (static_cast<int>(blockIdx.x) >= T * T) return;
+    const int ti = blockIdx.x / T, tj = blockIdx.x - ti * T;
+    const int row0 = ti * kGjTile, col0 = tj * kGjTile;
+    if (row0 >= k0 && row0 + kGjTile <= k0 + b) return;  // the whole tile is pivot rows
+    float *A = P.A + P.moff[p];
+    const float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    for (int e = threadIdx.x; e < kGjTile * kGjBlock; e += blockDim.x) {
+        const int r = e / kGjBlock, s = e - r * kGjBlock;
+        const int i = row0 + r;
+        Cs[r][s] = (i < n) ? cb[static_cast<size_t>(i) * kGjBlock + s] : 0.0f;  // zero beyond b
+    }
+    for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
+        const int s = e / kGjTile, c = e - s * kGjTile;
+        const int j = col0 + c;
+        Rs[s][c] = (s < b && j < n) ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0f;
+#pragma unroll 8
+    for (int s = 0; s < kGjBlock; ++s) {
+        float cr[4], rr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) cr[u] = Cs[ty * 4 + u][s];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) rr[v] = Rs[s][tx * 4 + v];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] += cr[u] * rr[v];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int i = row0 + ty * 4 + u;
+        if (i >= n || (i >= k0 && i < k0 + b)) continue;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int j = col0 + tx * 4 + v;
+            if (j >= n) continue;
+            float *a = A + static_cast<size_t>(i) * n + j;
+            *a = (j >= k0 && j < k0 + b) ? -acc[u][v] : *a - acc[u][v];
+        }
+    }
+}
+
+// Clears a patch's ok flag if its inverse holds a non-finite entry.
+__global__ void patch_check_kernel(PatchDev P) {
+    const int p = blockIdx.y;
+    const int n = P.nf[p] * P.nbf;
+    const long long nn = static_cast<long long>(n) * n;
+    const float *A = P.A + P.moff[p];
+    bool bad = false;
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < nn;
+         e += static_cast<long long>(gridDim.x) * blockDim.x)
+        bad |= !isfinite(A[e]);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) P.ok[p] = 0;
+}
+
+// out = blockdiag(A_pp^-1) in over the patches (in and out must differ).
+// grid = (row chunks of 64, patches); the block gathers the patch's rows of
+// `in` into shared memory, each warp forms 8 output rows with the lanes
+// striding the (coalesced) matrix row.  A patch without a finite inverse uses
+// the block-diagonal preconditioner instead (first row chunk only).
+// Dynamic shared memory: max(max_n, 3*nseg) doubles.
+// With `masked`, patches of arrays whose GMRES stopped are skipped.
+__global__ void __launch_bounds__(256) patch_apply_kernel(SimDev d, PatchDev P, const double *in, double *out,
+                                                          int masked) {
+    extern __shared__ double xs[];
+    __shared__ double sm32[32];
+    const int p = blockIdx.y;
+    const int n = P.nf[p] * P.nbf;
+    const int r0 = blockIdx.x * 64;
+    if (r0 >= n) return;
+    if (masked && !d.active[d.fil_arr[P.fils[P.fil0[p]]]]) return;
+    if (!P.ok[p]) {
+        if (blockIdx.x != 0) return;
+        for (int a = 0; a < P.nf[p]; ++a) {
+            const int m = P.fils[P.fil0[p] + a];
+            precond_block(d, m, fil_rows(d, m), in, out, xs, sm32);
+            __syncthreads();
+        }
+        return;
+    }
+    const long long *rows = P.rows + P.roff[p];
+    for (int c = threadIdx.x; c < n; c += blockDim.x) xs[c] = in[rows[c]];
+    __syncthreads();
+    const float *A = P.A + P.moff[p];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int rr = 0; rr < 8; ++rr) {
+        const int r = r0 + warp * 8 + rr;
+        if (r >= n) break;
+        const float *ar = A + static_cast<size_t>(r) * n;
+        double acc = 0.0;
+        for (int c = lane; c < n; c += 32) acc += static_cast<double>(__ldg(ar + c)) * xs[c];
+        acc = warp_sum(acc);
+        if (lane == 0) out[rows[r]] = acc;
+    }
+}
+
+// After a patch application: packs the force rows of z for the pair kernel
+// and writes the filament rows of A z (one block per filament), the work that
+// arnoldi_precond_kernel does itself with the block-diagonal preconditioner.
+__global__ void pack_rows_kernel(SimDev d, const double *z, double *w) {
+    __shared__ double sm32[32];
+    const int m = blockIdx.x;
+    const FilRows fr = fil_rows(d, m);
+    if (!d.active[fr.b]) return;
+    for (int kk = threadIdx.x; kk < d.nseg; kk += blockDim.x) {
+        const long long r = fr.lam + 3 * kk;
+        d.f4[m * d.nseg + kk] = make_float4(static_cast<float>(z[r]), static_cast<float>(z[r + 1]),
+                                            static_cast<float>(z[r + 2]), 0.0f);
+    }
+    filament_rows(d, fr, z, w, sm32);
+}
+
+}  // namespace cufil

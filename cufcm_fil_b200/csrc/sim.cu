@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "rpy_kernels.cuh"
 #include "sim_kernels.cuh"
+#include "patch_kernels.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -67,6 +68,15 @@ struct Engine {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle handle = 0;
+    // line-patch preconditioner
+    bool line = false;
+    PatchDev P{};
+    long long patch_floats = 0;
+    int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_tiles = 1, apply_chunks = 1;
+    bool refreshed_last = false;
+    size_t apply_smem = 0;
+    cudaGraph_t rgraph = nullptr;
+    cudaGraphExec_t rexec = nullptr;
     std::vector<void *> allocations;
 };
 
@@ -215,8 +225,60 @@ int launch_combine(Engine *e, cudaStream_t st) {
     return CF_OK;
 }
 
+// Assembles and inverts every patch block for the current kinematics.
+int launch_refresh(Engine *e, cudaStream_t st) {
+    const PatchDev &P = e->P;
+    CF_CUDA(cudaMemsetAsync(P.A, 0, sizeof(float) * e->patch_floats, st));
+    patch_mobility_kernel<<<dim3(e->mob_grid, P.np), 256, 0, st>>>(e->d, P);
+    CF_CHECK_LAUNCH("patch_mobility_kernel");
+    patch_rates_kernel<<<P.np, 256, 0, st>>>(e->d, P);
+    CF_CHECK_LAUNCH("patch_rates_kernel");
+    for (int K = 0; K < e->gj_rounds; ++K) {
+        gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, K);
+        CF_CHECK_LAUNCH("gj_pivot_kernel");
+        gj_update_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P, K);
+        CF_CHECK_LAUNCH("gj_update_kernel");
+    }
+    patch_check_kernel<<<dim3(32, P.np), 256, 0, st>>>(P);
+    CF_CHECK_LAUNCH("patch_check_kernel");
+    return CF_OK;
+}
+
+int refresh_launches(const Engine *e) { return e->line ? 3 + 2 * e->gj_rounds : 0; }
+
+int launch_patch_apply(Engine *e, const double *in, double *out, int masked, cudaStream_t st) {
+    patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), 256, e->apply_smem, st>>>(e->d, e->P, in, out, masked);
+    CF_CHECK_LAUNCH("patch_apply_kernel");
+    return CF_OK;
+}
+
+// Refreshes the patch inverses when the step calls for it (graph-captured once).
+int maybe_refresh(Engine *e, int nt) {
+    e->refreshed_last = false;
+    if (!e->line) return CF_OK;
+    const bool due = e->last_refresh_nt < 0 || nt < e->last_refresh_nt || nt - e->last_refresh_nt >= e->refresh_every;
+    if (!due) return CF_OK;
+    if (e->use_graph && !e->rexec) {
+        CF_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = launch_refresh(e, e->stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+        if (rc != CF_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        CF_TRY(cuda_status(ce, "cudaStreamEndCapture(refresh)", __FILE__, __LINE__));
+        e->rgraph = g;
+        CF_CUDA(cudaGraphInstantiate(&e->rexec, e->rgraph, 0));
+    }
+    if (e->rexec) CF_CUDA(cudaGraphLaunch(e->rexec, e->stream));
+    else CF_TRY(launch_refresh(e, e->stream));
+    e->last_refresh_nt = nt;
+    e->refreshed_last = true;
+    return CF_OK;
+}
+
 int launch_prologue(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
-    CF_TRY(launch_kinematics(e, st));
     rhs_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d);
     CF_CHECK_LAUNCH("rhs_kernel");
     CF_TRY(launch_matvec_tail(e, e->d.sol, e->d.w, st));
@@ -228,6 +290,11 @@ int launch_prologue(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
 int launch_body(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
     arnoldi_precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, h);
     CF_CHECK_LAUNCH("arnoldi_precond_kernel");
+    if (e->line) {  // z = P^-1 Q_k from the copy in t, then the rows arnoldi_precond leaves to us
+        CF_TRY(launch_patch_apply(e, e->d.t, e->d.z, 1, st));
+        pack_rows_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.z, e->d.w);
+        CF_CHECK_LAUNCH("pack_rows_kernel");
+    }
     CF_TRY(launch_matvec_tail(e, e->d.z, e->d.w, st));
     dots_kernel<<<e->dots_grid, 256, 0, st>>>(e->d, e->d.h1);
     CF_CHECK_LAUNCH("dots_kernel");
@@ -241,6 +308,7 @@ int launch_finish(Engine *e, cudaStream_t st) {
     backsub_kernel<<<e->B, 256, sizeof(double) * (e->d.mi_max + 1), st>>>(e->d);
     CF_CHECK_LAUNCH("backsub_kernel");
     CF_TRY(launch_combine(e, st));
+    if (e->line) CF_TRY(launch_patch_apply(e, e->d.t, e->d.z, 0, st));
     finish_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d);
     CF_CHECK_LAUNCH("finish_kernel");
     return CF_OK;
@@ -357,6 +425,8 @@ int batch_status(const std::vector<GmresCtl> &c) {
 
 int run_step(Engine *e, int nt) {
     CF_TRY(launch_step_begin(e, nt, e->stream));
+    CF_TRY(launch_kinematics(e, e->stream));
+    CF_TRY(maybe_refresh(e, nt));
     e->stepped = true;
     if (e->use_graph) {
         if (!e->exec) {
@@ -395,8 +465,12 @@ int validate(const cf_sim_config *cfg, const char *who) {
     CF_REQUIRE(static_cast<long long>(cfg->n_fil) * cfg->n_seg < (1LL << 26), "%s: too many segments", who);
     CF_REQUIRE(cfg->beat == CF_BEAT_FULFORD_BLAKE || cfg->beat == CF_BEAT_FULFORD_BLAKE_ORIGINAL,
                "%s: unknown beat %d", who, cfg->beat);
-    CF_REQUIRE(cfg->precond == CF_PRECOND_NONE || cfg->precond == CF_PRECOND_BLOCK_DIAG,
+    CF_REQUIRE(cfg->precond == CF_PRECOND_NONE || cfg->precond == CF_PRECOND_BLOCK_DIAG ||
+                   cfg->precond == CF_PRECOND_LINE,
                "%s: preconditioner %d not available in this entry point", who, cfg->precond);
+    CF_REQUIRE(cfg->line_patch >= 0 && cfg->line_patch <= 32, "%s: line_patch must be 0..32 (got %d)", who,
+               cfg->line_patch);
+    CF_REQUIRE(cfg->precond_refresh >= 0, "%s: precond_refresh must be >= 0", who);
     CF_REQUIRE(cfg->dt > 0 && cfg->seg_sep > 0, "%s: dt and seg_sep must be positive", who);
     CF_REQUIRE(cfg->gmres_tol > 0 && cfg->gmres_max_iter > 0, "%s: bad GMRES tolerance / cap", who);
     CF_REQUIRE(cfg->base_pos, "%s: base_pos is required", who);
@@ -416,6 +490,7 @@ int validate_shared(const cf_sim_config &a, const cf_sim_config &c, int b) {
                       a.spring_factor == c.spring_factor && a.gmres_tol == c.gmres_tol &&
                       a.gmres_max_iter == c.gmres_max_iter && a.precond == c.precond &&
                       a.s_tol_factor == c.s_tol_factor && a.device == c.device &&
+                      a.line_patch == c.line_patch && a.precond_refresh == c.precond_refresh &&
                       a.n_gen_phase_refs == c.n_gen_phase_refs && a.n_gen_angle_refs == c.n_gen_angle_refs &&
                       a.s_ref_rows == c.s_ref_rows && a.s_ref_cols == c.s_ref_cols &&
                       (a.s_values_ref == nullptr) == (c.s_values_ref == nullptr);
@@ -427,6 +502,84 @@ int validate_shared(const cf_sim_config &a, const cf_sim_config &c, int b) {
                "cf_batch_create: array %d has different generalised angle forces", b);
     CF_REQUIRE(!a.s_values_ref || same_table(a.s_values_ref, c.s_values_ref, a.s_ref_rows * a.s_ref_cols),
                "cf_batch_create: array %d has a different arclength table", b);
+    return CF_OK;
+}
+
+// Line patches: within each array, filaments with equal base x (a lattice line
+// along y, the beat direction of the wall frame) sorted by y and cut into
+// runs of at most line_patch filaments of near-equal length.
+int build_patches(Engine *e, const cf_sim_config *cfgs) {
+    SimDev &d = e->d;
+    const int Pmax = cfgs[0].line_patch > 0 ? cfgs[0].line_patch : 32;
+    const int nl = 3 * d.nseg;
+    const int nbf = nl + d.dyn_phase + d.dyn_angle;
+    std::vector<int> fil0, nf, fils;
+    std::vector<long long> moff, roff, rows;
+    long long mo = 0, ro = 0;
+    int max_n = 0, max_nf = 0;
+    for (int b = 0; b < e->B; ++b) {
+        const ArrayInfo &a = e->arr[b];
+        const double *bp = cfgs[b].base_pos;
+        std::vector<int> idx(a.F);
+        for (int q = 0; q < a.F; ++q) idx[q] = q;
+        std::sort(idx.begin(), idx.end(), [&](int u, int v) {
+            if (bp[3 * u] != bp[3 * v]) return bp[3 * u] < bp[3 * v];
+            return bp[3 * u + 1] < bp[3 * v + 1];
+        });
+        size_t s0 = 0;
+        while (s0 < idx.size()) {
+            const double x0 = bp[3 * idx[s0]];
+            size_t s1 = s0 + 1;
+            while (s1 < idx.size() && std::fabs(bp[3 * idx[s1]] - x0) <= 1e-6 * (1.0 + std::fabs(x0))) ++s1;
+            const int L = static_cast<int>(s1 - s0);
+            const int c = (L + Pmax - 1) / Pmax, base = L / c, extra = L % c;
+            size_t pos = s0;
+            for (int q = 0; q < c; ++q) {
+                const int sz = base + (q < extra ? 1 : 0);
+                fil0.push_back(static_cast<int>(fils.size()));
+                nf.push_back(sz);
+                const int n = sz * nbf;
+                moff.push_back(mo);
+                roff.push_back(ro);
+                mo += static_cast<long long>(n) * n;
+                ro += n;
+                max_n = std::max(max_n, n);
+                max_nf = std::max(max_nf, sz);
+                for (int u = 0; u < sz; ++u) {
+                    const int lm = idx[pos + u];
+                    fils.push_back(a.fil0 + lm);
+                    const long long lam = a.voff + static_cast<long long>(nl) * lm;
+                    for (int li = 0; li < nl; ++li) rows.push_back(lam + li);
+                    if (a.po >= 0) rows.push_back(a.voff + a.po + lm);
+                    if (a.ao >= 0) rows.push_back(a.voff + a.ao + lm);
+                }
+                pos += sz;
+            }
+            s0 = s1;
+        }
+    }
+    PatchDev &P = e->P;
+    P.np = static_cast<int>(nf.size());
+    P.nbf = nbf;
+    P.max_n = max_n;
+    CF_TRY(eng_upload(e, const_cast<int **>(&P.fil0), fil0.data(), fil0.size()));
+    CF_TRY(eng_upload(e, const_cast<int **>(&P.nf), nf.data(), nf.size()));
+    CF_TRY(eng_upload(e, const_cast<int **>(&P.fils), fils.data(), fils.size()));
+    CF_TRY(eng_upload(e, const_cast<long long **>(&P.moff), moff.data(), moff.size()));
+    CF_TRY(eng_upload(e, const_cast<long long **>(&P.roff), roff.data(), roff.size()));
+    CF_TRY(eng_upload(e, const_cast<long long **>(&P.rows), rows.data(), rows.size()));
+    CF_TRY(eng_alloc(e, &P.A, static_cast<size_t>(mo)));
+    CF_TRY(eng_alloc(e, &P.cbuf, static_cast<size_t>(P.np) * max_n * kGjBlock));
+    CF_TRY(eng_alloc(e, &P.ok, P.np));
+    e->patch_floats = mo;
+    const long long ns = static_cast<long long>(max_nf) * d.nseg;
+    e->mob_grid = static_cast<int>((ns * ns + 255) / 256);
+    e->gj_rounds = (max_n + kGjBlock - 1) / kGjBlock;
+    const int T = (max_n + kGjTile - 1) / kGjTile;
+    e->gj_tiles = T * T;
+    e->apply_chunks = (max_n + 63) / 64;
+    e->apply_smem = sizeof(double) * std::max(max_n, 3 * d.nseg);
+    e->refresh_every = cfgs[0].precond_refresh > 0 ? cfgs[0].precond_refresh : 1;
     return CF_OK;
 }
 
@@ -492,7 +645,9 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     d.hstride = static_cast<long long>(mi_max + 2) * (mi_max + 1);
     d.sstride = mi_max + 2;
     d.flexible = 0;
-    d.precond = c0.precond == CF_PRECOND_BLOCK_DIAG ? 1 : 0;
+    d.precond = (c0.precond == CF_PRECOND_BLOCK_DIAG || c0.precond == CF_PRECOND_LINE) ? 1 : 0;
+    d.line = c0.precond == CF_PRECOND_LINE ? 1 : 0;
+    e->line = d.line != 0;
     d.dyn_phase = dp;
     d.dyn_angle = da;
     d.dt = c0.dt;
@@ -626,6 +781,7 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     if (e->kin_smem > 48 * 1024)
         CF_CUDA(cudaFuncSetAttribute(kinematics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(e->kin_smem)));
+    if (e->line) CF_TRY(build_patches(e, cfgs));
     CF_TRY(apply_tuning(e, Tuning{}));
     const char *ng = std::getenv("CUFIL_NO_GRAPH");
     e->use_graph = !(ng && ng[0] == '1');
@@ -637,6 +793,8 @@ void engine_release(Engine *e) {
     if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->exec) cudaGraphExecDestroy(e->exec);
     if (e->graph) cudaGraphDestroy(e->graph);
+    if (e->rexec) cudaGraphExecDestroy(e->rexec);
+    if (e->rgraph) cudaGraphDestroy(e->rgraph);
     for (void *p : e->allocations) cudaFree(p);
     if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -967,11 +1125,17 @@ extern "C" int cf_sim_iteration_log(cf_sim *s, int *iters, int n) {
     return CF_OK;
 }
 
-extern "C" int cf_sim_launches_per_step(cf_sim *s, int iters) {
-    // step_begin + kinematics, rhs, pair, epilogue, residual + 7 per iteration + backsub, combine, finish
-    (void)s;
-    return 1 + 5 + 7 * iters + 3;
+namespace {
+// step_begin + kinematics, rhs, pair, epilogue, residual + 7 per iteration + backsub, combine, finish;
+// the line-patch preconditioner adds 2 per iteration, 1 in the finish and the refresh when it ran.
+int launches_for(const Engine *e, int iters) {
+    int n = 1 + 5 + 7 * iters + 3;
+    if (e && e->line) n += 2 * iters + 1 + (e->refreshed_last ? refresh_launches(e) : 0);
+    return n;
 }
+}  // namespace
+
+extern "C" int cf_sim_launches_per_step(cf_sim *s, int iters) { return launches_for(s, iters); }
 
 extern "C" int cf_sim_initial_guess(cf_sim *s, int nt) {
     clear_error();
@@ -1001,6 +1165,14 @@ extern "C" int cf_sim_apply_preconditioner(cf_sim *s, const double *in, double *
     CF_CUDA(cudaSetDevice(s->device));
     const size_t b = sizeof(double) * s->arr[0].n;
     CF_CUDA(cudaMemcpyAsync(s->d.t, in, b, cudaMemcpyHostToDevice, s->stream));
+    if (s->line) {  // patch inverses of the current kinematics
+        CF_TRY(launch_refresh(s, s->stream));
+        s->last_refresh_nt = -1;
+        CF_TRY(launch_patch_apply(s, s->d.t, s->d.z, 0, s->stream));
+        CF_CUDA(cudaMemcpyAsync(out, s->d.z, b, cudaMemcpyDeviceToHost, s->stream));
+        CF_CUDA(cudaStreamSynchronize(s->stream));
+        return CF_OK;
+    }
     precond_kernel<<<s->d.F, s->fil_threads, s->pre_smem, s->stream>>>(s->d, s->d.t, s->d.t);
     CF_CHECK_LAUNCH("precond_kernel");
     CF_CUDA(cudaMemcpyAsync(out, s->d.t, b, cudaMemcpyDeviceToHost, s->stream));
@@ -1148,10 +1320,7 @@ extern "C" int cf_batch_stream(cf_batch *bt, void **stream) {
     return CF_OK;
 }
 
-extern "C" int cf_batch_launches_per_step(cf_batch *bt, int loop_iters) {
-    (void)bt;
-    return 1 + 5 + 7 * loop_iters + 3;
-}
+extern "C" int cf_batch_launches_per_step(cf_batch *bt, int loop_iters) { return launches_for(bt, loop_iters); }
 
 extern "C" int cf_batch_autotune(cf_batch *bt, int k_hint, int *choice) {
     clear_error();

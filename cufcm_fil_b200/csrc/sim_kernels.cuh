@@ -101,7 +101,8 @@ struct SimDev {
     long long hstride;        // Hessenberg block per array
     int sstride;              // small per-array vectors (cs, sn, beta, h1, h2, y)
     int flexible;             // keep Z = P^{-1} Q (nonlinear preconditioner)
-    int precond;              // 0: none, 1: block-diagonal
+    int precond;              // 0: none, 1: block-diagonal (also the fallback of the patch preconditioner)
+    int line;                 // line-patch preconditioner (patch_kernels.cuh) applied between kernels
     int dyn_phase, dyn_angle; // rate blocks present
     int s_rows, s_cols;       // arclength table (0 rows: bisection)
     int n_phase_refs, n_angle_refs;
@@ -587,6 +588,14 @@ __global__ void arnoldi_precond_kernel(SimDev d, cudaGraphConditionalHandle h) {
         if (fr.pr >= 0) q[fr.pr] = src[fr.pr] * sc;
         if (fr.ar >= 0) q[fr.ar] = src[fr.ar] * sc;
     }
+    if (d.line) {  // the patch preconditioner runs next, from a fixed copy of Q_k
+        for (int j = threadIdx.x; j < nb; j += blockDim.x) d.t[fr.lam + j] = q[fr.lam + j];
+        if (threadIdx.x == 0) {
+            if (fr.pr >= 0) d.t[fr.pr] = q[fr.pr];
+            if (fr.ar >= 0) d.t[fr.ar] = q[fr.ar];
+        }
+        return;
+    }
     __syncthreads();
     double *zout = d.flexible ? d.Z + static_cast<size_t>(k) * d.ldq : d.z;
     precond_block(d, m, fr, q, zout, smp, sm32);
@@ -1046,23 +1055,24 @@ __global__ void finish_kernel(SimDev d) {
     const int st = ctl->status;
     const int nb = 3 * d.nseg;
     const bool iterated = st == kGmresConverged || st == kGmresMaxIter;
-    if (iterated && !d.flexible) precond_block(d, m, fr, d.t, d.t, smp, sm32);
+    if (iterated && !d.flexible && !d.line) precond_block(d, m, fr, d.t, d.t, smp, sm32);
     __syncthreads();
+    const double *dx = d.line ? d.z : d.t;  // the patch preconditioner left P^-1 t in z
     const bool reset = st == kGmresZeroRhs || (iterated && ctl->zero_guess);
     const bool add = iterated;
     for (int j = threadIdx.x; j < nb; j += blockDim.x) {
         const double base = reset ? 0.0 : d.sol[fr.lam + j];
-        d.sol[fr.lam + j] = base + (add ? d.t[fr.lam + j] : 0.0);
+        d.sol[fr.lam + j] = base + (add ? dx[fr.lam + j] : 0.0);
     }
     if (threadIdx.x == 0) {
         if (fr.pr >= 0) {
             const double base = reset ? 0.0 : d.sol[fr.pr];
-            d.sol[fr.pr] = base + (add ? d.t[fr.pr] : 0.0);
+            d.sol[fr.pr] = base + (add ? dx[fr.pr] : 0.0);
             d.phase_dot[m] = d.sol[fr.pr];
         }
         if (fr.ar >= 0) {
             const double base = reset ? 0.0 : d.sol[fr.ar];
-            d.sol[fr.ar] = base + (add ? d.t[fr.ar] : 0.0);
+            d.sol[fr.ar] = base + (add ? dx[fr.ar] : 0.0);
             d.angle_dot[m] = d.sol[fr.ar];
         }
     }

@@ -33,7 +33,7 @@ class GmresResult:
 def _sim_config(keep: list, *, bases, nseg=20, seg_sep=2.6, beat=_lib.CF_BEAT_FULFORD_BLAKE, dt=1.0 / 300,
                 dynamic_phase=True, dynamic_angle=True, spring_factor=0.01, gmres_tol=1e-6, gmres_max_iter=350,
                 precond=_lib.CF_PRECOND_BLOCK_DIAG, omega0=None, phase0=None, angle0=None, phase_refs=None,
-                angle_refs=None, s_table=None, s_tol_factor=0.0, device=0):
+                angle_refs=None, s_table=None, s_tol_factor=0.0, device=0, line_patch=0, precond_refresh=0):
     """cf_sim_config of one array; the arrays it points to are appended to `keep` (kept alive by the caller)."""
     bases = np.ascontiguousarray(bases, np.float64).reshape(-1, 3)
     keep.append(bases)
@@ -61,7 +61,8 @@ def _sim_config(keep: list, *, bases, nseg=20, seg_sep=2.6, beat=_lib.CF_BEAT_FU
         gen_phase_force_refs=_p(pr), n_gen_phase_refs=0 if pr is None else pr.size,
         gen_angle_force_refs=_p(ar), n_gen_angle_refs=0 if ar is None else ar.size,
         s_values_ref=_p(st), s_ref_rows=0 if st is None else st.shape[0],
-        s_ref_cols=0 if st is None else st.shape[1], s_tol_factor=float(s_tol_factor), device=int(device))
+        s_ref_cols=0 if st is None else st.shape[1], s_tol_factor=float(s_tol_factor), device=int(device),
+        line_patch=int(line_patch), precond_refresh=int(precond_refresh))
 
 
 class WallCiliaSimulation:

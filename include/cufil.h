@@ -195,6 +195,7 @@ typedef struct cf_sim cf_sim;
 #define CF_PRECOND_NONE 0
 #define CF_PRECOND_BLOCK_DIAG 1          /* apply_preconditioner_new */
 #define CF_PRECOND_LEARNED 2             /* per-filament MLP (flexible GMRES) */
+#define CF_PRECOND_LINE 3                /* block-Jacobi over line patches along the beat direction */
 
 typedef struct cf_sim_config {
     int n_fil;              /* NFIL (one swimmer: the wall) */
@@ -225,6 +226,11 @@ typedef struct cf_sim_config {
      * reference's 0.1, filament.cpp:1143). */
     double s_tol_factor;
     int device;
+    /* CF_PRECOND_LINE: filaments per patch (runs of equal base x, consecutive
+     * in y, the beat direction of the wall frame; at most 32, 0 selects 32) and
+     * the number of steps between refreshes of the patch inverses (0 selects 1). */
+    int line_patch;
+    int precond_refresh;
 } cf_sim_config;
 
 CF_API int cf_sim_create(const cf_sim_config *cfg, cf_sim **out);

@@ -162,6 +162,62 @@ class WallCilia:
                 out[sl] = r1 + SEG_MOB_INV * out[ao + m] * ka
         return out
 
+    # -- line-patch block-Jacobi preconditioner --------------------------------
+    # Not a reference routine: the engine's CF_PRECOND_LINE restated in FP64 for
+    # its parity tests.  Patches come from line_patches(); each patch's saddle
+    # block (the system_matrix_mult_new operator restricted to the patch) is
+    # inverted exactly.
+    def patch_block(self, fils):
+        """Dense saddle block of the filaments `fils`, per-filament order [3*nseg lambda | rates]."""
+        ns = self.nseg
+        n3, po, ao = self._offsets()
+        nr = int(po is not None) + int(ao is not None)
+        nbf = 3 * ns + nr
+        segs = np.concatenate([np.arange(f * ns, (f + 1) * ns) for f in fils])
+        x = self.x[segs]
+        nl = len(segs)
+        M = np.zeros((3 * nl, 3 * nl))
+        for c in range(3 * nl):
+            f = np.zeros((nl, 3))
+            f.flat[c] = 1.0
+            M[:, c] = rpy_apply(x, x, f, wall=1, vdof=3, fdof=3, self_by_index=True, nthreads=self.nthreads).ravel()
+        nf = len(fils)
+        A = np.zeros((nbf * nf, nbf * nf))
+        for a in range(nf):
+            for b in range(nf):
+                A[nbf * a:nbf * a + 3 * ns, nbf * b:nbf * b + 3 * ns] = M[3 * ns * a:3 * ns * (a + 1),
+                                                                         3 * ns * b:3 * ns * (b + 1)]
+            cols = []
+            if po is not None:
+                cols.append(self.kp[fils[a] * ns:(fils[a] + 1) * ns].ravel())
+            if ao is not None:
+                cols.append(self.ka[fils[a] * ns:(fils[a] + 1) * ns].ravel())
+            for q, k in enumerate(cols):
+                A[nbf * a:nbf * a + 3 * ns, nbf * a + 3 * ns + q] = -k
+                A[nbf * a + 3 * ns + q, nbf * a:nbf * a + 3 * ns] = -k
+        return A
+
+    def patch_rows(self, fils):
+        """Saddle-vector rows of the patch unknowns, in the order of patch_block."""
+        ns = self.nseg
+        n3, po, ao = self._offsets()
+        rows = []
+        for f in fils:
+            rows.extend(range(3 * ns * f, 3 * ns * (f + 1)))
+            if po is not None:
+                rows.append(po + f)
+            if ao is not None:
+                rows.append(ao + f)
+        return np.asarray(rows)
+
+    def line_patch_precond(self, v, line_patch=32):
+        out = np.zeros(self.size)
+        v = np.asarray(v, float)
+        for fils in line_patches(self.bases, line_patch):
+            rows = self.patch_rows(fils)
+            out[rows] = np.linalg.solve(self.patch_block(fils), v[rows])
+        return out
+
     # -- mobility product (Mss_mult, wall, 3x3) -----------------------------
     def mobility(self, lam):
         f = np.asarray(lam, float).reshape(-1, 3)
@@ -289,6 +345,30 @@ class WallCilia:
 
     def tips(self):
         return self.x.reshape(self.nfil, self.nseg, 3)[:, -1, :].copy()
+
+
+def line_patches(bases, line_patch=32):
+    """Filament groups of the line-patch preconditioner: filaments with equal base x (a
+    lattice line along y, the beat direction of the wall frame) sorted by y, cut into runs
+    of at most `line_patch` filaments of near-equal length (the longer runs first)."""
+    b = np.asarray(bases, float).reshape(-1, 3)
+    order = sorted(range(b.shape[0]), key=lambda i: (b[i, 0], b[i, 1]))
+    out, s0 = [], 0
+    while s0 < len(order):
+        x0 = b[order[s0], 0]
+        s1 = s0 + 1
+        while s1 < len(order) and abs(b[order[s1], 0] - x0) <= 1e-6 * (1.0 + abs(x0)):
+            s1 += 1
+        L = s1 - s0
+        c = -(-L // line_patch)
+        base, extra = divmod(L, c)
+        pos = s0
+        for q in range(c):
+            sz = base + (1 if q < extra else 0)
+            out.append(order[pos:pos + sz])
+            pos += sz
+        s0 = s1
+    return out
 
 
 def write_generalised_forces_run(shape_sequence: int, nseg: int = 20, seg_sep: float = 2.6, steps: int = 300,
