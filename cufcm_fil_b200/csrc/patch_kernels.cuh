@@ -19,9 +19,9 @@
 // exact operator, so the patch inverses change only the iteration count.
 //
 // Cost: one refresh is sum_p n_p^3 FP32 FMAs (n_p = 62 * filaments), done as
-// ceil(n/32) rounds of (a) inverting the 32x32 pivot block and scaling the
-// pivot rows (one block per patch) and (b) a rank-32 update of the rest of the
-// matrix in 64x64 tiles.  One application is a dense n_p x n_p product per
+// ceil(n/64) rounds of (a) inverting the 64x64 pivot block (one block per
+// patch), (b) scaling the pivot rows and saving the pivot columns (one thread
+// per column) and (c) a rank-64 update of the matrix in 64x64 tiles.  One application is a dense n_p x n_p product per
 // patch, reading the FP32 inverses once.
 #pragma once
 
@@ -30,8 +30,8 @@
 
 namespace cufil {
 
-constexpr int kGjBlock = 32;  // pivot block of the Gauss-Jordan rounds
-constexpr int kGjTile = 64;   // tile of the rank-32 updates
+constexpr int kGjBlock = 64;  // pivot block of the Gauss-Jordan rounds
+constexpr int kGjTile = 64;   // tile of the rank-64 updates
 
 struct PatchDev {
     int np;                  // patches
@@ -45,6 +45,8 @@ struct PatchDev {
     const long long *rows;   // batch-vector row of each local unknown
     float *A;                // patch matrices, then their inverses (row-major n x n)
     float *cbuf;             // pivot-column copies, [np][max_n][kGjBlock]
+    float *rbuf;             // scaled pivot rows, [np][kGjBlock][max_n]
+    float *dinv;             // inverted pivot blocks, [np][kGjBlock][kGjBlock]
     int *ok;                 // [np] 1 when the inverse is finite
 };
 
@@ -108,9 +110,9 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
 }
 
 // Round K of the blocked Gauss-Jordan inversion, part (a), one block per
-// patch: copies the pivot columns of the other rows to cbuf, inverts the
-// pivot block D in shared memory, scales the pivot rows by D^-1 and stores
-// D^-1 in place.  A non-finite or zero pivot clears the patch's ok flag.
+// patch: inverts the pivot block D = A[K, K] (b <= 64) in shared memory and
+// stores D^-1 (zero-padded to 64 x 64) in dinv.  A non-finite or zero pivot
+// clears the patch's ok flag.
 __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     __shared__ float D[kGjBlock][kGjBlock + 1];
     __shared__ float col[kGjBlock];
@@ -120,18 +122,11 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     const int k0 = K * kGjBlock;
     if (k0 >= n) return;
     const int b = min(kGjBlock, n - k0);
-    float *A = P.A + P.moff[p];
-    float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    const float *A = P.A + P.moff[p];
     if (K == 0 && threadIdx.x == 0) P.ok[p] = 1;
-    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) D[e / kGjBlock][e % kGjBlock] = 0.0f;
-    for (int e = threadIdx.x; e < n * kGjBlock; e += blockDim.x) {
-        const int i = e / kGjBlock, s = e - i * kGjBlock;
-        cb[e] = (s < b && (i < k0 || i >= k0 + b)) ? A[static_cast<size_t>(i) * n + k0 + s] : 0.0f;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-        const int r = e / b, s = e - r * b;
-        D[r][s] = A[static_cast<size_t>(k0 + r) * n + k0 + s];
+    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) {
+        const int r = e / kGjBlock, c = e - r * kGjBlock;
+        D[r][c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : 0.0f;
     }
     __syncthreads();
     for (int t = 0; t < b; ++t) {
@@ -143,43 +138,71 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
         }
         __syncthreads();
         const float ip = inv_piv;
-        for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-            const int r = e / b, s = e - r * b;
-            if (r == t) {
-                D[r][s] = (s == t) ? ip : D[r][s] * ip;
-            }
-        }
+        for (int c = threadIdx.x; c < b; c += blockDim.x) D[t][c] = (c == t) ? ip : D[t][c] * ip;
         __syncthreads();
         for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-            const int r = e / b, s = e - r * b;
-            if (r != t) D[r][s] = (s == t) ? -col[r] * ip : D[r][s] - col[r] * D[t][s];
+            const int r = e / b, c = e - r * b;
+            if (r != t) D[r][c] = (c == t) ? -col[r] * ip : D[r][c] - col[r] * D[t][c];
         }
         __syncthreads();
     }
-    // pivot rows outside the pivot columns: A[K, j] <- D^-1 A[K, j]
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        if (j >= k0 && j < k0 + b) continue;
-        float tmp[kGjBlock];
-#pragma unroll
-        for (int s = 0; s < kGjBlock; ++s) tmp[s] = s < b ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
-        for (int r = 0; r < b; ++r) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int s = 0; s < kGjBlock; ++s) acc += D[r][s] * tmp[s];  // zero beyond b
-            A[static_cast<size_t>(k0 + r) * n + j] = acc;
-        }
-    }
-    for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-        const int r = e / b, s = e - r * b;
-        A[static_cast<size_t>(k0 + r) * n + k0 + s] = D[r][s];
-    }
+    float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
+    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) dv[e] = D[e / kGjBlock][e % kGjBlock];
 }
 
-// Round K, part (b): every row outside the pivot rows, in 64x64 tiles:
-//   A[i, j] -= C_i . A[K, j]   (j outside the pivot columns; A[K, j] scaled in (a))
-//   A[i, K]  = -C_i . D^-1     (pivot columns; D^-1 stored in A[K, K])
-// with C_i the row's old pivot-column entries from cbuf.  grid = (tiles, patches).
-__global__ void __launch_bounds__(256) gj_update_kernel(PatchDev P, int K) {
+// Round K, part (b), one thread per column j (and per row i = j) of a patch:
+//   rbuf[s][j] = (D^-1 A[K, j])_s   for j outside the pivot columns,
+//   rbuf[s][j] = D^-1[s][j - k0]     for j inside them (the new pivot block),
+//   cbuf[i][s] = A[i, k0 + s]        for rows i outside the pivot rows (old values).
+// grid = (ceil(max_n / 256), patches).
+__global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
+    __shared__ float Dv[kGjBlock][kGjBlock + 1];
+    const int p = blockIdx.y;
+    const int n = P.nf[p] * P.nbf;
+    const int k0 = K * kGjBlock;
+    if (k0 >= n) return;
+    const int b = min(kGjBlock, n - k0);
+    const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
+    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) Dv[e / kGjBlock][e % kGjBlock] = dv[e];
+    __syncthreads();
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const float *A = P.A + P.moff[p];
+    float *rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
+    float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    const bool in_block = j >= k0 && j < k0 + b;
+    float a[kGjBlock];
+#pragma unroll
+    for (int s = 0; s < kGjBlock; ++s) a[s] = (!in_block && s < b) ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
+    for (int r0 = 0; r0 < kGjBlock; r0 += 16) {
+#pragma unroll
+        for (int r = r0; r < r0 + 16; ++r) {
+            float acc = 0.0f;
+            if (in_block) {
+                acc = Dv[r][j - k0];
+            } else {
+#pragma unroll
+                for (int s = 0; s < kGjBlock; ++s) acc += Dv[r][s] * a[s];
+            }
+            rb[static_cast<size_t>(r) * n + j] = acc;  // rows r >= b hold zeros (D^-1 is zero-padded)
+        }
+    }
+    const int i = j;  // the same thread copies the old pivot columns of row i
+    const bool pivot_row = i >= k0 && i < k0 + b;
+#pragma unroll 8
+    for (int s = 0; s < kGjBlock; ++s)
+        cb[static_cast<size_t>(i) * kGjBlock + s] = (!pivot_row && s < b) ? A[static_cast<size_t>(i) * n + k0 + s] : 0.0f;
+}
+
+// Round K, part (c), 64x64 tiles of the whole matrix:
+//   pivot rows       A[i, j] = rbuf[i - k0][j]
+//   other rows       A[i, j] -= C_i . rbuf[:, j]   (j outside the pivot columns)
+//                    A[i, j]  = -C_i . rbuf[:, j]  (pivot columns: -C_i D^-1)
+// with C_i = cbuf[i][:].  Each thread owns 4 rows x 4 columns of the tile
+// (columns interleaved by 16, so every load and store of a half-warp is one
+// contiguous run) and loads each of its rows of A in one batch.
+// grid = (tiles, patches).
+__global__ void __launch_bounds__(256, 5) gj_update_kernel(PatchDev P, int K) {
     __shared__ float Cs[kGjTile][kGjBlock + 1];
     __shared__ float Rs[kGjBlock][kGjTile + 1];
     const int p = blockIdx.y;
@@ -191,21 +214,21 @@ __global__ void __launch_bounds__(256) gj_update_kernel(PatchDev P, int K) {
     if (static_cast<int>(blockIdx.x) >= T * T) return;
     const int ti = blockIdx.x / T, tj = blockIdx.x - ti * T;
     const int row0 = ti * kGjTile, col0 = tj * kGjTile;
-    if (row0 >= k0 && row0 + kGjTile <= k0 + b) return;  // the whole tile is pivot rows
-    float *A = P.A + P.moff[p];
-    const float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    float *__restrict__ A = P.A + P.moff[p];
+    const float *__restrict__ cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    const float *__restrict__ rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int e = threadIdx.x; e < kGjTile * kGjBlock; e += blockDim.x) {
         const int r = e / kGjBlock, s = e - r * kGjBlock;
         const int i = row0 + r;
-        Cs[r][s] = (i < n) ? cb[static_cast<size_t>(i) * kGjBlock + s] : 0.0f;  // zero beyond b
+        Cs[r][s] = (i < n) ? cb[static_cast<size_t>(i) * kGjBlock + s] : 0.0f;
     }
     for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
         const int s = e / kGjTile, c = e - s * kGjTile;
         const int j = col0 + c;
-        Rs[s][c] = (s < b && j < n) ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
+        Rs[s][c] = (j < n) ? rb[static_cast<size_t>(s) * n + j] : 0.0f;
     }
     __syncthreads();
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     float acc[4][4];
 #pragma unroll
     for (int u = 0; u < 4; ++u)
@@ -217,7 +240,7 @@ __global__ void __launch_bounds__(256) gj_update_kernel(PatchDev P, int K) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) cr[u] = Cs[ty * 4 + u][s];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) rr[v] = Rs[s][tx * 4 + v];
+        for (int v = 0; v < 4; ++v) rr[v] = Rs[s][v * 16 + tx];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -226,13 +249,21 @@ __global__ void __launch_bounds__(256) gj_update_kernel(PatchDev P, int K) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         const int i = row0 + ty * 4 + u;
-        if (i >= n || (i >= k0 && i < k0 + b)) continue;
+        if (i >= n) continue;
+        const bool pivot_row = i >= k0 && i < k0 + b;
+        float *__restrict__ ar = A + static_cast<size_t>(i) * n;
+        float old[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const int j = col0 + tx * 4 + v;
+            const int j = col0 + v * 16 + tx;
+            old[v] = (!pivot_row && j < n) ? ar[j] : 0.0f;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int j = col0 + v * 16 + tx;
             if (j >= n) continue;
-            float *a = A + static_cast<size_t>(i) * n + j;
-            *a = (j >= k0 && j < k0 + b) ? -acc[u][v] : *a - acc[u][v];
+            ar[j] = pivot_row ? Rs[i - k0][v * 16 + tx]
+                              : ((j >= k0 && j < k0 + b) ? -acc[u][v] : old[v] - acc[u][v]);
         }
     }
 }

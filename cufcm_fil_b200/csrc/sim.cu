@@ -188,7 +188,7 @@ int launch_step_begin(Engine *e, int nt, cudaStream_t st) {
 
 int launch_matvec_tail(Engine *e, const double *v, double *out, cudaStream_t st) {
     CF_TRY(rpy_launch_sym_batch(e->pair, e->pair_grid, st));
-    saddle_epilogue_kernel<<<e->epi_grid, 256, 0, st>>>(e->d, v, out);
+    saddle_epilogue_kernel<<<e->epi_grid, 32 * kEpiWarps, 0, st>>>(e->d, v, out);
     CF_CHECK_LAUNCH("saddle_epilogue_kernel");
     return CF_OK;
 }
@@ -233,9 +233,12 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     CF_CHECK_LAUNCH("patch_mobility_kernel");
     patch_rates_kernel<<<P.np, 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_rates_kernel");
+    const int cols = (P.max_n + 255) / 256;
     for (int K = 0; K < e->gj_rounds; ++K) {
         gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_pivot_kernel");
+        gj_prep_kernel<<<dim3(cols, P.np), 256, 0, st>>>(P, K);
+        CF_CHECK_LAUNCH("gj_prep_kernel");
         gj_update_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_update_kernel");
     }
@@ -244,7 +247,7 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     return CF_OK;
 }
 
-int refresh_launches(const Engine *e) { return e->line ? 3 + 2 * e->gj_rounds : 0; }
+int refresh_launches(const Engine *e) { return e->line ? 3 + 3 * e->gj_rounds : 0; }
 
 int launch_patch_apply(Engine *e, const double *in, double *out, int masked, cudaStream_t st) {
     patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), 256, e->apply_smem, st>>>(e->d, e->P, in, out, masked);
@@ -570,6 +573,8 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     CF_TRY(eng_upload(e, const_cast<long long **>(&P.rows), rows.data(), rows.size()));
     CF_TRY(eng_alloc(e, &P.A, static_cast<size_t>(mo)));
     CF_TRY(eng_alloc(e, &P.cbuf, static_cast<size_t>(P.np) * max_n * kGjBlock));
+    CF_TRY(eng_alloc(e, &P.rbuf, static_cast<size_t>(P.np) * max_n * kGjBlock));
+    CF_TRY(eng_alloc(e, &P.dinv, static_cast<size_t>(P.np) * kGjBlock * kGjBlock));
     CF_TRY(eng_alloc(e, &P.ok, P.np));
     e->patch_floats = mo;
     const long long ns = static_cast<long long>(max_nf) * d.nseg;
@@ -770,7 +775,7 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     e->kin_smem = sizeof(double) * (2 * (10 * ns + 1) + ns);
     e->pre_smem = sizeof(double) * 3 * ns;
     e->givens_smem = sizeof(double) * 3 * (d.mi_max + 2);
-    e->epi_grid = (seg + 255) / 256;
+    e->epi_grid = (seg + 31) / 32;
     if (e->givens_smem > 48 * 1024) {
         const int gs = static_cast<int>(e->givens_smem);
         CF_CUDA(cudaFuncSetAttribute(update_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));

@@ -623,42 +623,48 @@ __global__ void filament_rows_kernel(SimDev d, const double *v, double *out) {
 }
 
 // Segment rows of out = A v (system_matrix_mult_new): reduces the mobility
-// partials of v's force part (one thread per segment; the slot-major partials
-// make every load of a warp one contiguous run), adds the FP64 wall self block
-// and the -K rate terms.  The filament rows are written by the kernel that
-// produced v.
-__global__ void saddle_epilogue_kernel(SimDev d, const double *v, double *out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.N) return;
-    const int m = i / d.nseg;
-    const int b = d.fil_arr[m];
-    if (!d.active[b]) return;
+// partials of v's force part, adds the FP64 wall self block and the -K rate
+// terms.  A block of 8 warps takes 32 consecutive segments: lane l of every
+// warp serves segment 32*blockIdx.x + l, warp w sums the partial slots
+// s = w, w + 8, ... (the slot-major layout makes every warp load one
+// contiguous run), and warp 0 combines the 8 sums in a fixed order.  The
+// filament rows are written by the kernel that produced v.
+constexpr int kEpiWarps = 8;
+__global__ void __launch_bounds__(32 * kEpiWarps) saddle_epilogue_kernel(SimDev d, const double *v, double *out) {
+    __shared__ double red[kEpiWarps][3][32];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane;
+    int b = -1;
+    if (i < d.N) {
+        b = d.fil_arr[i / d.nseg];
+        if (!d.active[b]) b = -1;
+    }
+    double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+    if (b >= 0) {
+        const ArrayInfo &a = d.arr[b];
+        const size_t n = a.N;
+        const float4 *pt = d.partial + a.poff + (i - a.seg0);
+        for (int s = wp; s < a.nb; s += kEpiWarps) {
+            const float4 q = __ldcs(pt + s * n);
+            u0 += q.x;
+            u1 += q.y;
+            u2 += q.z;
+        }
+    }
+    red[wp][0][lane] = u0;
+    red[wp][1][lane] = u1;
+    red[wp][2][lane] = u2;
+    __syncthreads();
+    if (wp != 0 || b < 0) return;
+    double u[3] = {0.0, 0.0, 0.0};
+    for (int w = 0; w < kEpiWarps; ++w)
+        for (int c = 0; c < 3; ++c) u[c] += red[w][c][lane];
     const ArrayInfo &a = d.arr[b];
-    const int ls = i - a.seg0;
-    const size_t n = a.N;
-    const float4 *pt = d.partial + a.poff + ls;
-    double u0 = 0.0, u1 = 0.0, u2 = 0.0, w0 = 0.0, w1 = 0.0, w2 = 0.0;
-    int s = 0;
-    for (; s + 1 < a.nb; s += 2) {
-        const float4 q = __ldcs(pt + s * n), r = __ldcs(pt + (s + 1) * n);
-        u0 += q.x;
-        u1 += q.y;
-        u2 += q.z;
-        w0 += r.x;
-        w1 += r.y;
-        w2 += r.z;
-    }
-    if (s < a.nb) {
-        const float4 q = __ldcs(pt + s * n);
-        u0 += q.x;
-        u1 += q.y;
-        u2 += q.z;
-    }
+    const int m = i / d.nseg;
     const int lm = m - a.fil0;
-    const long long row = a.voff + 3LL * ls;
+    const long long row = a.voff + 3LL * (i - a.seg0);
     const double vp = a.po >= 0 ? v[a.voff + a.po + lm] : 0.0;
     const double va = a.ao >= 0 ? v[a.voff + a.ao + lm] : 0.0;
-    double u[3] = {u0 + w0, u1 + w1, u2 + w2};
     const double f[3] = {v[row], v[row + 1], v[row + 2]};
     wall_self_f64(d.xd[3 * i + 2], f, u);
     for (int c = 0; c < 3; ++c) out[row + c] = u[c] - vp * d.kp[3 * i + c] - va * d.ka[3 * i + c];
