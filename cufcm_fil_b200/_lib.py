@@ -119,6 +119,8 @@ SIGNATURES = {
     "cf_sim_apply_preconditioner": [_vp, _vp, _vp],
     "cf_sim_system_matvec": [_vp, _vp, _vp],
     "cf_sim_autotune": [_vp, _i, _vp],
+    "cf_sim_refresh_preconditioner": [_vp],
+    "cf_sim_precond_info": [_vp, _vp, _vp, _vp, _vp],
     "cf_sim_set_tuning": [_vp, _vp],
     "cf_sim_get_tuning": [_vp, _vp],
     "cf_batch_create": [_vp, _i, ctypes.POINTER(_vp)],

@@ -114,40 +114,51 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
 // stores D^-1 (zero-padded to 64 x 64) in dinv.  A non-finite or zero pivot
 // clears the patch's ok flag.
 __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
+    static_assert(kGjBlock * 4 == 256, "one row per 4 threads");
     __shared__ float D[kGjBlock][kGjBlock + 1];
-    __shared__ float col[kGjBlock];
-    __shared__ float inv_piv;
     const int p = blockIdx.x;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
     if (k0 >= n) return;
     const int b = min(kGjBlock, n - k0);
     const float *A = P.A + P.moff[p];
+    const int r = threadIdx.x >> 2, cq = threadIdx.x & 3;  // row r, columns cq + 4q
     if (K == 0 && threadIdx.x == 0) P.ok[p] = 1;
-    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) {
-        const int r = e / kGjBlock, c = e - r * kGjBlock;
+#pragma unroll
+    for (int q = 0; q < kGjBlock / 4; ++q) {
+        const int c = cq + 4 * q;
         D[r][c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : 0.0f;
     }
     __syncthreads();
     for (int t = 0; t < b; ++t) {
-        if (threadIdx.x < b) col[threadIdx.x] = D[threadIdx.x][t];
-        if (threadIdx.x == 0) {
-            const float piv = D[t][t];
-            if (!(fabsf(piv) > 0.0f) || !isfinite(piv)) P.ok[p] = 0;
-            inv_piv = 1.0f / piv;
+        const float colr = D[r][t];
+        const float piv = D[t][t];
+        const float ip = 1.0f / piv;
+        if (threadIdx.x == 0 && (!(fabsf(piv) > 0.0f) || !isfinite(piv))) P.ok[p] = 0;
+        __syncthreads();
+        if (r == t) {
+#pragma unroll
+            for (int q = 0; q < kGjBlock / 4; ++q) {
+                const int c = cq + 4 * q;
+                D[t][c] = (c == t) ? ip : D[t][c] * ip;
+            }
         }
         __syncthreads();
-        const float ip = inv_piv;
-        for (int c = threadIdx.x; c < b; c += blockDim.x) D[t][c] = (c == t) ? ip : D[t][c] * ip;
-        __syncthreads();
-        for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-            const int r = e / b, c = e - r * b;
-            if (r != t) D[r][c] = (c == t) ? -col[r] * ip : D[r][c] - col[r] * D[t][c];
+        if (r != t && r < b) {
+#pragma unroll
+            for (int q = 0; q < kGjBlock / 4; ++q) {
+                const int c = cq + 4 * q;
+                D[r][c] = (c == t) ? -colr * ip : D[r][c] - colr * D[t][c];
+            }
         }
         __syncthreads();
     }
     float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
-    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) dv[e] = D[e / kGjBlock][e % kGjBlock];
+#pragma unroll
+    for (int q = 0; q < kGjBlock / 4; ++q) {
+        const int c = cq + 4 * q;
+        dv[r * kGjBlock + c] = D[r][c];
+    }
 }
 
 // Round K, part (b), one thread per column j (and per row i = j) of a patch:

@@ -1202,6 +1202,37 @@ extern "C" int cf_sim_system_matvec(cf_sim *s, const double *in, double *out) {
     return read_loop(s, &lc);
 }
 
+extern "C" int cf_sim_refresh_preconditioner(cf_sim *s) {
+    clear_error();
+    CF_REQUIRE(s, "null handle");
+    CF_REQUIRE(s->line, "cf_sim_refresh_preconditioner: the handle does not use CF_PRECOND_LINE");
+    CF_CUDA(cudaSetDevice(s->device));
+    CF_TRY(launch_refresh(s, s->stream));
+    s->last_refresh_nt = -1;  // the next step refreshes again for its own kinematics
+    return CF_OK;
+}
+
+extern "C" int cf_sim_precond_info(cf_sim *s, int *n_patches, int *max_n, double *refresh_flops,
+                                   double *apply_bytes) {
+    clear_error();
+    CF_REQUIRE(s, "null handle");
+    double fl = 0.0, by = 0.0;
+    if (s->line) {
+        std::vector<int> nf(s->P.np);
+        CF_CUDA(cudaMemcpy(nf.data(), s->P.nf, sizeof(int) * nf.size(), cudaMemcpyDeviceToHost));
+        for (int f : nf) {
+            const double n = static_cast<double>(f) * s->P.nbf;
+            fl += 2.0 * n * n * n;        // Gauss-Jordan inversion: n^3 multiply-adds
+            by += 4.0 * n * n + 16.0 * n; // FP32 inverse read once, FP64 vector gathered and scattered
+        }
+    }
+    if (n_patches) *n_patches = s->line ? s->P.np : 0;
+    if (max_n) *max_n = s->line ? s->P.max_n : 0;
+    if (refresh_flops) *refresh_flops = fl;
+    if (apply_bytes) *apply_bytes = by;
+    return CF_OK;
+}
+
 extern "C" int cf_sim_autotune(cf_sim *s, int k_hint, int *choice) {
     clear_error();
     CF_REQUIRE(s, "null handle");

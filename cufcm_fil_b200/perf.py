@@ -1,0 +1,90 @@
+"""Measurement entry points (the command lines of the committed profiles).
+
+  python -m cufcm_fil_b200.perf step --nx 16 --precond line --steps 2
+      implicit steps of the benchmark lattice (lattice_simulation); with
+      CUFIL_NO_GRAPH=1 every kernel is an ordinary launch, which is what a
+      profiler's launch list needs.
+  python -m cufcm_fil_b200.perf fcm --grid 512 --reps 5
+      the sphere-with-cilia FCM workload (1000 cilia x 20 segments + 10 000
+      body blobs, box 1024a): stage times of one apply and the achieved
+      bandwidth of spreading and interpolation against their algorithmic bytes
+      (spread: N ngd^3 x 3 read-modify-writes of 4 bytes each way; gather:
+      N ngd^3 x 3 reads of 4 bytes).
+Each prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+from . import _lib
+
+
+def run_steps(nx: int, precond: str, steps: int, line_patch: int = 0):
+    from .sim import lattice_simulation
+    code = {"line": _lib.CF_PRECOND_LINE, "block": _lib.CF_PRECOND_BLOCK_DIAG, "none": _lib.CF_PRECOND_NONE}[precond]
+    with lattice_simulation(nx, precond=code, line_patch=line_patch) as sim:
+        its = [sim.step(nt).iterations for nt in range(steps)]
+    return {"nx": nx, "precond": precond, "steps": steps, "gmres_iterations": its}
+
+
+def run_fcm(grid: int, reps: int, hbm_gbs: float | None = None):
+    import torch
+    from . import workloads
+    from .fcm import FcmSolver
+    segs, blobs = workloads.sphere_with_cilia()
+    Y = np.concatenate([segs, blobs])
+    n = Y.shape[0]
+    F = np.random.default_rng(11).standard_normal((n, 3))
+    kw = dict(rh=1.0, alpha=1.0, beta=10.0, eta=6.0, nx=grid, ny=grid, nz=grid, boxsize=1024.0)
+    Yd = torch.as_tensor(Y.astype(np.float32).ravel(), device="cuda")
+    Fd = torch.as_tensor(F.astype(np.float32).ravel(), device="cuda")
+    Vd = torch.empty_like(Fd)
+    with FcmSolver(n, **kw) as s:
+        info = s.info()
+        s.set_timing(True)
+        for _ in range(2):
+            s.apply_device(Yd, Fd, Vd)
+        torch.cuda.synchronize()
+        acc = {k: 0.0 for k in FcmSolver.STAGES}
+        for _ in range(reps):
+            s.apply_device(Yd, Fd, Vd)
+            torch.cuda.synchronize()
+            for k, v in s.stage_times().items():
+                acc[k] += v / reps
+    ngd3 = int(info["ngd"]) ** 3
+    spread_bytes = n * ngd3 * 3 * 8
+    gather_bytes = n * ngd3 * 3 * 4
+    out = {"grid": grid, "particles": n, "ngd": int(info["ngd"]), "stage_ms": acc,
+           "total_ms": sum(acc.values()),
+           "spread_GBps": spread_bytes / (acc["spread"] * 1e-3) / 1e9 if acc["spread"] > 0 else None,
+           "gather_GBps": gather_bytes / (acc["gather"] * 1e-3) / 1e9 if acc["gather"] > 0 else None}
+    if hbm_gbs:
+        out["spread_frac"] = out["spread_GBps"] / hbm_gbs
+        out["gather_frac"] = out["gather_GBps"] / hbm_gbs
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m cufcm_fil_b200.perf")
+    sub = ap.add_subparsers(dest="what", required=True)
+    st = sub.add_parser("step")
+    st.add_argument("--nx", type=int, default=16)
+    st.add_argument("--precond", choices=["line", "block", "none"], default="line")
+    st.add_argument("--steps", type=int, default=2)
+    st.add_argument("--line-patch", type=int, default=0)
+    fc = sub.add_parser("fcm")
+    fc.add_argument("--grid", type=int, default=512)
+    fc.add_argument("--reps", type=int, default=5)
+    fc.add_argument("--hbm-gbs", type=float, default=None)
+    a = ap.parse_args(argv)
+    if a.what == "step":
+        print(json.dumps(run_steps(a.nx, a.precond, a.steps, a.line_patch)))
+    else:
+        print(json.dumps(run_fcm(a.grid, a.reps, a.hbm_gbs)))
+
+
+if __name__ == "__main__":
+    main()

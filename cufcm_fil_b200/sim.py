@@ -158,6 +158,17 @@ class WallCiliaSimulation:
     def launches_per_step(self, iters: int) -> int:
         return _lib.load().cf_sim_launches_per_step(self._h, int(iters))
 
+    def refresh_preconditioner(self):
+        """CF_PRECOND_LINE: rebuilds the patch inverses for the current kinematics (asynchronous)."""
+        _lib.call("cf_sim_refresh_preconditioner", self._h)
+
+    def precond_info(self) -> dict:
+        np_, mx = ctypes.c_int(), ctypes.c_int()
+        fl, by = ctypes.c_double(), ctypes.c_double()
+        _lib.call("cf_sim_precond_info", self._h, ctypes.byref(np_), ctypes.byref(mx), ctypes.byref(fl),
+                  ctypes.byref(by))
+        return dict(patches=np_.value, max_n=mx.value, refresh_flops=fl.value, apply_bytes=by.value)
+
     def autotune(self, k_hint: int = 0) -> dict:
         """Times the iteration kernels' launch shapes on the current state and keeps the fastest."""
         c = np.zeros(len(_TUNING_KEYS), np.int32)
@@ -382,3 +393,25 @@ class WallCiliaBatch:
     def set_tuning(self, **kw):
         c = _tuning_array(self.tuning(), kw)
         _lib.call("cf_batch_set_tuning", self._h, _p(c))
+
+
+def lattice_simulation(nx: int = 16, *, spacing: float = 20.0, nseg: int = 20, seg_sep: float = 2.6, seed: int = 2024,
+                       s_table=None, **kw) -> WallCiliaSimulation:
+    """The benchmark array: nx x nx Fulford-Blake cilia on a square wall lattice (bases at z = seg_sep/2),
+    phases U(0, 2 pi) and angles N(0, 0.05) from `seed`, dt = T/300, spring factor 0.01, the reference's
+    generalised-force tables and the device-generated arclength table; other keywords go to
+    WallCiliaSimulation (precond, gmres_tol, line_patch, device, ...)."""
+    from pathlib import Path
+    from . import workloads
+    data = np.load(Path(__file__).resolve().parent / "data" / "fulford_blake_nseg20_sep2.6.npz")
+    F = nx * nx
+    rng = np.random.default_rng(seed)
+    phase0 = rng.uniform(0.0, 2.0 * math.pi, F)
+    angle0 = rng.normal(0.0, 0.05, F)
+    if s_table is None:
+        s_table = arclength_table(nseg=nseg, seg_sep=seg_sep, steps=300)
+    args = dict(nseg=nseg, seg_sep=seg_sep, dt=1.0 / 300, phase0=phase0, angle0=angle0, spring_factor=0.01,
+                phase_refs=data["phase"], angle_refs=data["angle"], s_table=s_table)
+    args.update(kw)
+    return WallCiliaSimulation(bases=workloads.lattice_bases(F, nx, spacing, 0.5 * seg_sep), **args)
+

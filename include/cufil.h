@@ -282,6 +282,13 @@ CF_API int cf_sim_system_matvec(cf_sim *s, const double *in, double *out);
  * index k_hint, <= 0: half the last step's iterations) and keeps the fastest;
  * only scratch buffers are written.  choice may be NULL. */
 CF_API int cf_sim_autotune(cf_sim *s, int k_hint, int *choice);
+/* CF_PRECOND_LINE: rebuilds the patch inverses for the current kinematics
+ * (asynchronous, on the handle's stream); no counterpart in the reference,
+ * whose preconditioner has no set-up.  cf_sim_precond_info reports the patch
+ * count, the largest patch system, the FLOPs of one rebuild (2 n^3 per patch)
+ * and the bytes one application moves; any pointer may be NULL. */
+CF_API int cf_sim_refresh_preconditioner(cf_sim *s);
+CF_API int cf_sim_precond_info(cf_sim *s, int *n_patches, int *max_n, double *refresh_flops, double *apply_bytes);
 CF_API int cf_sim_set_tuning(cf_sim *s, const int *choice);
 CF_API int cf_sim_get_tuning(cf_sim *s, int *choice);
 
