@@ -123,6 +123,15 @@ SIGNATURES = {
     "cf_sim_precond_info": [_vp, _vp, _vp, _vp, _vp],
     "cf_sim_set_tuning": [_vp, _vp],
     "cf_sim_get_tuning": [_vp, _vp],
+    "cf_mlp_create": [_i, _i, _i, _i, ctypes.c_ulonglong, _i, ctypes.POINTER(_vp)],
+    "cf_mlp_destroy": [_vp],
+    "cf_mlp_num_params": [_vp],
+    "cf_mlp_forward": [_vp, _vp, _i, _vp, _vp],
+    "cf_mlp_gradients": [_vp, _vp, _vp, _i, _vp, _vp],
+    "cf_mlp_train_step": [_vp, _vp, _vp, _i, ctypes.c_float, _vp],
+    "cf_mlp_get_params": [_vp, _vp],
+    "cf_mlp_set_params": [_vp, _vp],
+    "cf_mlp_stream": [_vp, ctypes.POINTER(_vp)],
     "cf_batch_create": [_vp, _i, ctypes.POINTER(_vp)],
     "cf_batch_destroy": [_vp],
     "cf_batch_shape": [_vp, _vp, _vp, _vp, _vp],
@@ -140,7 +149,7 @@ SIGNATURES = {
     "cf_batch_set_tuning": [_vp, _vp],
     "cf_batch_get_tuning": [_vp, _vp],
 }
-_RESTYPES = {"cf_last_error": ctypes.c_char_p}
+_RESTYPES = {"cf_last_error": ctypes.c_char_p, "cf_mlp_num_params": ctypes.c_longlong}
 
 _lib = None
 

@@ -1,0 +1,412 @@
+// mlp.cu -- cf_mlp: a small fully connected network (in -> H -> H -> out, ReLU)
+// with its own forward, backward and Adam kernels, used as a learned
+// per-filament correction inside flexible GMRES (CF_PRECOND_LEARNED).
+// No counterpart in the reference.
+//
+// Every product is one GEMM kernel: C[M x N] = op(A)[M x K] op(B)[K x N] with
+// FP32 operands in memory, rounded to BF16 while they are staged in shared
+// memory, multiplied on the tensor cores by mma.sync m16n8k16 (BF16 x BF16,
+// FP32 accumulate), and an FP32 epilogue (bias, ReLU, or the ReLU mask of the
+// backward pass).  Forward:  A1 = relu(X W1 + b1), A2 = relu(A1 W2 + b2),
+// Y = A2 W3 + b3.  Backward of the mean squared error:
+//   dY = 2 (Y - T) / (n out)      dW3 = A2^T dY    db3 = colsum dY
+//   dZ2 = (dY W3^T) o [A2 > 0]    dW2 = A1^T dZ2   db2 = colsum dZ2
+//   dZ1 = (dZ2 W2^T) o [A1 > 0]   dW1 = X^T dZ1    db1 = colsum dZ1
+// then one Adam step on FP32 master weights.  Reductions (loss, bias
+// gradients) are fixed-order: results do not depend on the launch.
+#include "common.cuh"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace cufil {
+namespace {
+
+constexpr int kTm = 64, kTn = 64, kTk = 32, kPad = 8;
+
+enum Epi : int { kEpiStore = 0, kEpiBias = 1, kEpiBiasRelu = 2, kEpiReluMask = 3 };
+
+struct GemmArgs {
+    const float *A, *B;
+    float *C;
+    const float *bias;  // [N] (kEpiBias, kEpiBiasRelu)
+    const float *mask;  // [M x N], ldc (kEpiReluMask): keep where mask > 0
+    int lda, ldb, ldc;
+    int M, N, K;
+    int ta, tb, epi;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+}
+
+// 64x64 tile of C per block of 4 warps (each warp 32x32 = 2 x 4 mma tiles).
+// Shared memory holds the tile of op(A) as [m][k] and of op(B) as [n][k], so
+// that both fragments read consecutive k pairs.
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
+    __shared__ __nv_bfloat16 As[kTm][kTk + kPad];
+    __shared__ __nv_bfloat16 Bs[kTn][kTk + kPad];
+    const int m0 = blockIdx.y * kTm, n0 = blockIdx.x * kTn;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int gq = lane >> 2, tq = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
+    for (int k0 = 0; k0 < g.K; k0 += kTk) {
+        // op(A)(m, k): A[m*lda + k] or A[k*lda + m]; consecutive threads walk the memory-contiguous index
+        for (int e = threadIdx.x; e < kTm * kTk; e += blockDim.x) {
+            int m, k;
+            if (g.ta) { k = e / kTm; m = e - k * kTm; } else { m = e / kTk; k = e - m * kTk; }
+            const int gm = m0 + m, gk = k0 + k;
+            float v = 0.0f;
+            if (gm < g.M && gk < g.K) v = g.ta ? g.A[static_cast<size_t>(gk) * g.lda + gm] : g.A[static_cast<size_t>(gm) * g.lda + gk];
+            As[m][k] = __float2bfloat16_rn(v);
+        }
+        // op(B)(k, n): B[k*ldb + n] or B[n*ldb + k]
+        for (int e = threadIdx.x; e < kTn * kTk; e += blockDim.x) {
+            int n, k;
+            if (g.tb) { n = e / kTk; k = e - n * kTk; } else { k = e / kTn; n = e - k * kTn; }
+            const int gn = n0 + n, gk = k0 + k;
+            float v = 0.0f;
+            if (gn < g.N && gk < g.K) v = g.tb ? g.B[static_cast<size_t>(gn) * g.ldb + gk] : g.B[static_cast<size_t>(gk) * g.ldb + gn];
+            Bs[n][k] = __float2bfloat16_rn(v);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < kTk; ks += 16) {
+            uint32_t af[2][4], bf[4][2];
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                const int r = wm + mt * 16 + gq;
+                af[mt][0] = pack_bf16(As[r][ks + 2 * tq], As[r][ks + 2 * tq + 1]);
+                af[mt][1] = pack_bf16(As[r + 8][ks + 2 * tq], As[r + 8][ks + 2 * tq + 1]);
+                af[mt][2] = pack_bf16(As[r][ks + 2 * tq + 8], As[r][ks + 2 * tq + 9]);
+                af[mt][3] = pack_bf16(As[r + 8][ks + 2 * tq + 8], As[r + 8][ks + 2 * tq + 9]);
+            }
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int c = wn + nt * 8 + gq;
+                bf[nt][0] = pack_bf16(Bs[c][ks + 2 * tq], Bs[c][ks + 2 * tq + 1]);
+                bf[nt][1] = pack_bf16(Bs[c][ks + 2 * tq + 8], Bs[c][ks + 2 * tq + 9]);
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    float *d = acc[mt][nt];
+                    asm volatile(
+                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                        : "r"(af[mt][0]), "r"(af[mt][1]), "r"(af[mt][2]), "r"(af[mt][3]), "r"(bf[nt][0]),
+                          "r"(bf[nt][1]));
+                }
+        }
+        __syncthreads();
+    }
+    // epilogue: accumulator (row g / g+8, columns 2t, 2t+1) of each mma tile
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const int row = m0 + wm + mt * 16 + gq + (h >> 1) * 8;
+                const int col = n0 + wn + nt * 8 + 2 * tq + (h & 1);
+                if (row >= g.M || col >= g.N) continue;
+                float v = acc[mt][nt][h];
+                const size_t o = static_cast<size_t>(row) * g.ldc + col;
+                if (g.epi == kEpiBias || g.epi == kEpiBiasRelu) v += g.bias[col];
+                if (g.epi == kEpiBiasRelu) v = fmaxf(v, 0.0f);
+                if (g.epi == kEpiReluMask && !(g.mask[o] > 0.0f)) v = 0.0f;
+                g.C[o] = v;
+            }
+}
+
+// dY = 2 (Y - T) / (n * out) and per-block partial sums of (Y - T)^2.
+__global__ void __launch_bounds__(256) mse_kernel(const float *Y, const float *T, float *dY, long long count,
+                                                  float scale, double *partial) {
+    __shared__ double sm[8];
+    double s = 0.0;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float d = Y[i] - T[i];
+        dY[i] = 2.0f * d * scale;
+        s += static_cast<double>(d) * d;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += sm[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// db[j] = sum_i dZ[i][j], rows summed in order by one thread per column.
+__global__ void colsum_kernel(const float *dZ, int n, int cols, float *db) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= cols) return;
+    float s = 0.0f;
+    for (int i = 0; i < n; ++i) s += dZ[static_cast<size_t>(i) * cols + j];
+    db[j] = s;
+}
+
+__global__ void adam_kernel(float *p, const float *gr, float *m, float *v, long long count, float lr, float b1,
+                            float b2, float c1, float c2, float eps) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float gi = gr[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+}  // namespace
+
+int gemm_bf16(const float *A, int lda, int ta, const float *B, int ldb, int tb, float *C, int ldc, int M, int N, int K,
+              const float *bias, const float *mask, int epi, cudaStream_t st) {
+    if (M <= 0 || N <= 0) return CF_OK;
+    GemmArgs g{A, B, C, bias, mask, lda, ldb, ldc, M, N, K, ta, tb, epi};
+    dim3 grid((N + kTn - 1) / kTn, (M + kTm - 1) / kTm);
+    gemm_bf16_kernel<<<grid, 128, 0, st>>>(g);
+    CF_CHECK_LAUNCH("gemm_bf16_kernel");
+    return CF_OK;
+}
+
+}  // namespace cufil
+
+using namespace cufil;
+
+struct cf_mlp {
+    int in = 0, hid = 0, out = 0, max_batch = 0, device = 0;
+    long long nparam = 0;
+    float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    float *W1, *b1, *W2, *b2, *W3, *b3;      // views into params
+    float *gW1, *gb1, *gW2, *gb2, *gW3, *gb3; // views into grads
+    float *A1 = nullptr, *A2 = nullptr, *Y = nullptr, *dY = nullptr, *dZ2 = nullptr, *dZ1 = nullptr;
+    double *partial = nullptr;
+    int loss_blocks = 256;
+    long long step = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void *> allocations;
+};
+
+namespace {
+
+template <typename T>
+int mlp_alloc(cf_mlp *h, T **p, size_t n) {
+    void *q = nullptr;
+    CF_CUDA(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)));
+    h->allocations.push_back(q);
+    *p = static_cast<T *>(q);
+    return CF_OK;
+}
+
+void set_views(cf_mlp *h) {
+    const long long in = h->in, hd = h->hid, out = h->out;
+    float *p = h->params, *g = h->grads;
+    const long long off[6] = {0, in * hd, in * hd + hd, in * hd + hd + hd * hd, in * hd + 2 * hd + hd * hd,
+                              in * hd + 2 * hd + hd * hd + hd * out};
+    h->W1 = p + off[0]; h->b1 = p + off[1]; h->W2 = p + off[2]; h->b2 = p + off[3]; h->W3 = p + off[4]; h->b3 = p + off[5];
+    h->gW1 = g + off[0]; h->gb1 = g + off[1]; h->gW2 = g + off[2]; h->gb2 = g + off[3]; h->gW3 = g + off[4];
+    h->gb3 = g + off[5];
+}
+
+int forward(cf_mlp *h, const float *x, int n, float *y, cudaStream_t st) {
+    CF_TRY(gemm_bf16(x, h->in, 0, h->W1, h->hid, 0, h->A1, h->hid, n, h->hid, h->in, h->b1, nullptr, kEpiBiasRelu, st));
+    CF_TRY(gemm_bf16(h->A1, h->hid, 0, h->W2, h->hid, 0, h->A2, h->hid, n, h->hid, h->hid, h->b2, nullptr,
+                     kEpiBiasRelu, st));
+    return gemm_bf16(h->A2, h->hid, 0, h->W3, h->out, 0, y, h->out, n, h->out, h->hid, h->b3, nullptr, kEpiBias, st);
+}
+
+// Forward + backward into h->grads; the loss (mean squared error) into *loss when asked (synchronises).
+int backward(cf_mlp *h, const float *x, const float *t, int n, double *loss) {
+    cudaStream_t st = h->stream;
+    CF_TRY(forward(h, x, n, h->Y, st));
+    const long long cnt = static_cast<long long>(n) * h->out;
+    mse_kernel<<<h->loss_blocks, 256, 0, st>>>(h->Y, t, h->dY, cnt, 1.0f / static_cast<float>(cnt), h->partial);
+    CF_CHECK_LAUNCH("mse_kernel");
+    // layer 3
+    CF_TRY(gemm_bf16(h->A2, h->hid, 1, h->dY, h->out, 0, h->gW3, h->out, h->hid, h->out, n, nullptr, nullptr,
+                     kEpiStore, st));
+    colsum_kernel<<<(h->out + 127) / 128, 128, 0, st>>>(h->dY, n, h->out, h->gb3);
+    CF_CHECK_LAUNCH("colsum_kernel");
+    CF_TRY(gemm_bf16(h->dY, h->out, 0, h->W3, h->out, 1, h->dZ2, h->hid, n, h->hid, h->out, nullptr, h->A2,
+                     kEpiReluMask, st));
+    // layer 2
+    CF_TRY(gemm_bf16(h->A1, h->hid, 1, h->dZ2, h->hid, 0, h->gW2, h->hid, h->hid, h->hid, n, nullptr, nullptr,
+                     kEpiStore, st));
+    colsum_kernel<<<(h->hid + 127) / 128, 128, 0, st>>>(h->dZ2, n, h->hid, h->gb2);
+    CF_CHECK_LAUNCH("colsum_kernel");
+    CF_TRY(gemm_bf16(h->dZ2, h->hid, 0, h->W2, h->hid, 1, h->dZ1, h->hid, n, h->hid, h->hid, nullptr, h->A1,
+                     kEpiReluMask, st));
+    // layer 1
+    CF_TRY(gemm_bf16(x, h->in, 1, h->dZ1, h->hid, 0, h->gW1, h->hid, h->in, h->hid, n, nullptr, nullptr, kEpiStore,
+                     st));
+    colsum_kernel<<<(h->hid + 127) / 128, 128, 0, st>>>(h->dZ1, n, h->hid, h->gb1);
+    CF_CHECK_LAUNCH("colsum_kernel");
+    if (loss) {
+        std::vector<double> part(h->loss_blocks);
+        CF_CUDA(cudaMemcpyAsync(part.data(), h->partial, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st));
+        CF_CUDA(cudaStreamSynchronize(st));
+        double s = 0.0;
+        for (double v : part) s += v;
+        *loss = s / static_cast<double>(cnt);
+    }
+    return CF_OK;
+}
+
+}  // namespace
+
+extern "C" int cf_mlp_create(int in_dim, int hidden, int out_dim, int max_batch, unsigned long long seed, int device,
+                             cf_mlp **out) {
+    clear_error();
+    CF_REQUIRE(out, "cf_mlp_create: null handle pointer");
+    *out = nullptr;
+    CF_REQUIRE(in_dim > 0 && hidden > 0 && out_dim > 0 && max_batch > 0 && in_dim <= 4096 && hidden <= 4096 &&
+                   out_dim <= 4096,
+               "cf_mlp_create: bad sizes (%d, %d, %d, batch %d)", in_dim, hidden, out_dim, max_batch);
+    CF_CUDA(cudaSetDevice(device));
+    cf_mlp *h = new (std::nothrow) cf_mlp();
+    if (!h) return set_error(CF_ENOMEM, "cf_mlp_create: host allocation failed");
+    h->in = in_dim;
+    h->hid = hidden;
+    h->out = out_dim;
+    h->max_batch = max_batch;
+    h->device = device;
+    h->nparam = static_cast<long long>(in_dim) * hidden + hidden + static_cast<long long>(hidden) * hidden + hidden +
+                static_cast<long long>(hidden) * out_dim + out_dim;
+    int rc = CF_OK;
+    do {
+        if ((rc = cuda_status(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate",
+                              __FILE__, __LINE__)))
+            break;
+        const size_t np = h->nparam, act = static_cast<size_t>(max_batch) * hidden;
+        if ((rc = mlp_alloc(h, &h->params, np)) || (rc = mlp_alloc(h, &h->grads, np)) ||
+            (rc = mlp_alloc(h, &h->adam_m, np)) || (rc = mlp_alloc(h, &h->adam_v, np)) ||
+            (rc = mlp_alloc(h, &h->A1, act)) || (rc = mlp_alloc(h, &h->A2, act)) || (rc = mlp_alloc(h, &h->dZ1, act)) ||
+            (rc = mlp_alloc(h, &h->dZ2, act)) || (rc = mlp_alloc(h, &h->Y, static_cast<size_t>(max_batch) * out_dim)) ||
+            (rc = mlp_alloc(h, &h->dY, static_cast<size_t>(max_batch) * out_dim)) ||
+            (rc = mlp_alloc(h, &h->partial, h->loss_blocks)))
+            break;
+        set_views(h);
+        // He-uniform weights from the seed, zero biases
+        std::vector<float> p(np, 0.0f);
+        std::mt19937_64 rng(seed);
+        auto fill = [&](long long off, int fan_in, long long count) {
+            std::uniform_real_distribution<float> u(-std::sqrt(6.0f / fan_in), std::sqrt(6.0f / fan_in));
+            for (long long i = 0; i < count; ++i) p[off + i] = u(rng);
+        };
+        fill(h->W1 - h->params, in_dim, static_cast<long long>(in_dim) * hidden);
+        fill(h->W2 - h->params, hidden, static_cast<long long>(hidden) * hidden);
+        fill(h->W3 - h->params, hidden, static_cast<long long>(hidden) * out_dim);
+        if ((rc = cuda_status(cudaMemcpy(h->params, p.data(), np * sizeof(float), cudaMemcpyHostToDevice),
+                              "cudaMemcpy", __FILE__, __LINE__)) ||
+            (rc = cuda_status(cudaMemset(h->adam_m, 0, np * sizeof(float)), "cudaMemset", __FILE__, __LINE__)) ||
+            (rc = cuda_status(cudaMemset(h->adam_v, 0, np * sizeof(float)), "cudaMemset", __FILE__, __LINE__)))
+            break;
+    } while (0);
+    if (rc != CF_OK) {
+        std::string msg = cf_last_error();
+        for (void *q : h->allocations) cudaFree(q);
+        if (h->stream) cudaStreamDestroy(h->stream);
+        delete h;
+        return set_error(rc, "%s", msg.c_str());
+    }
+    *out = h;
+    return CF_OK;
+}
+
+extern "C" int cf_mlp_destroy(cf_mlp *h) {
+    if (!h) return CF_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void *q : h->allocations) cudaFree(q);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return CF_OK;
+}
+
+extern "C" long long cf_mlp_num_params(cf_mlp *h) { return h ? h->nparam : -1; }
+
+extern "C" int cf_mlp_forward(cf_mlp *h, const float *x, int n, float *y, void *stream) {
+    clear_error();
+    CF_REQUIRE(h && x && y, "cf_mlp_forward: null argument");
+    CF_REQUIRE(n >= 0 && n <= h->max_batch, "cf_mlp_forward: batch %d outside [0, %d]", n, h->max_batch);
+    CF_CUDA(cudaSetDevice(h->device));
+    return forward(h, x, n, y, stream ? static_cast<cudaStream_t>(stream) : h->stream);
+}
+
+extern "C" int cf_mlp_gradients(cf_mlp *h, const float *x, const float *t, int n, float *grads, double *loss) {
+    clear_error();
+    CF_REQUIRE(h && x && t, "cf_mlp_gradients: null argument");
+    CF_REQUIRE(n > 0 && n <= h->max_batch, "cf_mlp_gradients: batch %d outside [1, %d]", n, h->max_batch);
+    CF_CUDA(cudaSetDevice(h->device));
+    double l = 0.0;
+    CF_TRY(backward(h, x, t, n, &l));
+    if (loss) *loss = l;
+    if (grads) {
+        CF_CUDA(cudaMemcpyAsync(grads, h->grads, sizeof(float) * h->nparam, cudaMemcpyDeviceToHost, h->stream));
+        CF_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return CF_OK;
+}
+
+extern "C" int cf_mlp_train_step(cf_mlp *h, const float *x, const float *t, int n, float lr, double *loss) {
+    clear_error();
+    CF_REQUIRE(h && x && t, "cf_mlp_train_step: null argument");
+    CF_REQUIRE(n > 0 && n <= h->max_batch, "cf_mlp_train_step: batch %d outside [1, %d]", n, h->max_batch);
+    CF_REQUIRE(lr > 0.0f, "cf_mlp_train_step: learning rate must be positive");
+    CF_CUDA(cudaSetDevice(h->device));
+    CF_TRY(backward(h, x, t, n, loss));
+    h->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, static_cast<float>(h->step));
+    const float c2 = 1.0f - std::pow(b2, static_cast<float>(h->step));
+    adam_kernel<<<256, 256, 0, h->stream>>>(h->params, h->grads, h->adam_m, h->adam_v, h->nparam, lr, b1, b2, c1, c2,
+                                            1e-8f);
+    CF_CHECK_LAUNCH("adam_kernel");
+    return CF_OK;
+}
+
+extern "C" int cf_mlp_get_params(cf_mlp *h, float *params) {
+    clear_error();
+    CF_REQUIRE(h && params, "cf_mlp_get_params: null argument");
+    CF_CUDA(cudaSetDevice(h->device));
+    CF_CUDA(cudaStreamSynchronize(h->stream));
+    CF_CUDA(cudaMemcpy(params, h->params, sizeof(float) * h->nparam, cudaMemcpyDeviceToHost));
+    return CF_OK;
+}
+
+extern "C" int cf_mlp_set_params(cf_mlp *h, const float *params) {
+    clear_error();
+    CF_REQUIRE(h && params, "cf_mlp_set_params: null argument");
+    CF_CUDA(cudaSetDevice(h->device));
+    CF_CUDA(cudaStreamSynchronize(h->stream));
+    CF_CUDA(cudaMemcpy(h->params, params, sizeof(float) * h->nparam, cudaMemcpyHostToDevice));
+    return CF_OK;
+}
+
+extern "C" int cf_mlp_stream(cf_mlp *h, void **stream) {
+    clear_error();
+    CF_REQUIRE(h && stream, "null argument");
+    *stream = static_cast<void *>(h->stream);
+    return CF_OK;
+}

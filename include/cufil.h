@@ -293,6 +293,31 @@ CF_API int cf_sim_set_tuning(cf_sim *s, const int *choice);
 CF_API int cf_sim_get_tuning(cf_sim *s, int *choice);
 
 /* ------------------------------------------------------------------------
+ * cf_mlp: the per-filament network of the learned preconditioner
+ * (CF_PRECOND_LEARNED).  No counterpart in the reference.  A fully connected
+ * network in -> hidden -> hidden -> out with ReLU, FP32 master weights, BF16
+ * tensor-core GEMMs with FP32 accumulation, trained by the library's own
+ * backward and Adam kernels on the mean squared error.  Tensors are device
+ * pointers to row-major FP32 [n x in] / [n x out]; n <= max_batch.
+ * Parameters, flat: W1 [in x H], b1 [H], W2 [H x H], b2 [H], W3 [H x out], b3 [out].
+ * ------------------------------------------------------------------------ */
+typedef struct cf_mlp cf_mlp;
+
+CF_API int cf_mlp_create(int in_dim, int hidden, int out_dim, int max_batch, unsigned long long seed, int device,
+                         cf_mlp **out);
+CF_API int cf_mlp_destroy(cf_mlp *h);
+CF_API long long cf_mlp_num_params(cf_mlp *h);
+/* y = net(x) on `stream` (NULL: the network's own stream). */
+CF_API int cf_mlp_forward(cf_mlp *h, const float *x, int n, float *y, void *stream);
+/* Loss and flat gradient (host, num_params floats; either may be NULL) of one batch. */
+CF_API int cf_mlp_gradients(cf_mlp *h, const float *x, const float *t, int n, float *grads, double *loss);
+/* One Adam step (beta 0.9 / 0.999) on one batch; loss may be NULL (then no synchronisation). */
+CF_API int cf_mlp_train_step(cf_mlp *h, const float *x, const float *t, int n, float lr, double *loss);
+CF_API int cf_mlp_get_params(cf_mlp *h, float *params);
+CF_API int cf_mlp_set_params(cf_mlp *h, const float *params);
+CF_API int cf_mlp_stream(cf_mlp *h, void **stream);
+
+/* ------------------------------------------------------------------------
  * Batches of independent arrays (periodic-orbit / bisection sweeps): many
  * wall arrays of uneven size stepped together, one graph launch per step for
  * the whole batch.  Each array is described by its own cf_sim_config; every
