@@ -275,6 +275,20 @@ int backward(cf_mlp *h, const float *x, const float *t, int n, double *loss) {
 
 }  // namespace
 
+namespace cufil {
+// Forward pass on a caller's stream for the implicit step (checked sizes).
+int mlp_forward_dev(cf_mlp *h, const float *x, int n, float *y, cudaStream_t st) {
+    if (n > h->max_batch) return set_error(CF_EINVAL, "network batch %d above its capacity %d", n, h->max_batch);
+    return forward(h, x, n, y, st);
+}
+int mlp_dims(const cf_mlp *h, int *in, int *out, int *max_batch) {
+    *in = h->in;
+    *out = h->out;
+    *max_batch = h->max_batch;
+    return CF_OK;
+}
+}  // namespace cufil
+
 extern "C" int cf_mlp_create(int in_dim, int hidden, int out_dim, int max_batch, unsigned long long seed, int device,
                              cf_mlp **out) {
     clear_error();

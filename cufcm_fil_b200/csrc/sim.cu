@@ -20,6 +20,7 @@
 #include "rpy_kernels.cuh"
 #include "sim_kernels.cuh"
 #include "patch_kernels.cuh"
+#include "learned_kernels.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -31,6 +32,11 @@
 #include <vector>
 
 using namespace cufil;
+
+namespace cufil {
+int mlp_forward_dev(cf_mlp *h, const float *x, int n, float *y, cudaStream_t st);
+int mlp_dims(const cf_mlp *h, int *in, int *out, int *max_batch);
+}  // namespace cufil
 
 namespace {
 constexpr int kIterLogCap = 4096;  // steps remembered by the iteration log (per array)
@@ -77,6 +83,12 @@ struct Engine {
     size_t apply_smem = 0;
     cudaGraph_t rgraph = nullptr;
     cudaGraphExec_t rexec = nullptr;
+    // learned correction
+    bool learned = false;
+    cf_mlp *net = nullptr;
+    // training-pair collection (host-driven steps only)
+    float *cx = nullptr, *ct = nullptr;
+    int c_max = 0, c_pairs = 0;
     std::vector<void *> allocations;
 };
 
@@ -293,12 +305,33 @@ int launch_prologue(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
 int launch_body(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
     arnoldi_precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, h);
     CF_CHECK_LAUNCH("arnoldi_precond_kernel");
+    if (e->learned) {  // z = P_bd(q) + s * net(features(q)), then the rows arnoldi_precond left to us
+        learned_features_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.t, e->d.lx, e->d.lscale);
+        CF_CHECK_LAUNCH("learned_features_kernel");
+        CF_TRY(mlp_forward_dev(e->net, e->d.lx, e->d.F, e->d.ly, st));
+        learned_correct_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.ly, e->d.lscale);
+        CF_CHECK_LAUNCH("learned_correct_kernel");
+        pack_rows_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.z, e->d.w);
+        CF_CHECK_LAUNCH("pack_rows_kernel");
+    }
     if (e->line) {  // z = P^-1 Q_k from the copy in t, then the rows arnoldi_precond leaves to us
         CF_TRY(launch_patch_apply(e, e->d.t, e->d.z, 1, st));
         pack_rows_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.z, e->d.w);
         CF_CHECK_LAUNCH("pack_rows_kernel");
     }
     CF_TRY(launch_matvec_tail(e, e->d.z, e->d.w, st));
+    if (e->cx && e->c_pairs < e->c_max) {  // one training pair (w = A z, z) of the plain solver
+        const size_t F = e->d.F;
+        learned_features_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.w,
+                                                                   e->cx + e->c_pairs * F * e->d.lin, e->d.lscale);
+        CF_CHECK_LAUNCH("learned_features_kernel");
+        precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, e->d.w, e->d.t);
+        CF_CHECK_LAUNCH("precond_kernel");
+        learned_target_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.z, e->d.t, e->d.lscale,
+                                                                 e->ct + e->c_pairs * F * e->d.lout);
+        CF_CHECK_LAUNCH("learned_target_kernel");
+        e->c_pairs += 1;
+    }
     dots_kernel<<<e->dots_grid, 256, 0, st>>>(e->d, e->d.h1);
     CF_CHECK_LAUNCH("dots_kernel");
     CF_TRY(launch_update(e, e->d.h1, 0, h, st, e->tune.update_rows, e->update_grid));
@@ -427,11 +460,12 @@ int batch_status(const std::vector<GmresCtl> &c) {
 }
 
 int run_step(Engine *e, int nt) {
+    CF_REQUIRE(!e->learned || e->net, "CF_PRECOND_LEARNED: no network attached (cf_sim_set_network)");
     CF_TRY(launch_step_begin(e, nt, e->stream));
     CF_TRY(launch_kinematics(e, e->stream));
     CF_TRY(maybe_refresh(e, nt));
     e->stepped = true;
-    if (e->use_graph) {
+    if (e->use_graph && !e->cx) {
         if (!e->exec) {
             int rc = build_graph(e);
             if (rc != CF_OK) {
@@ -469,7 +503,7 @@ int validate(const cf_sim_config *cfg, const char *who) {
     CF_REQUIRE(cfg->beat == CF_BEAT_FULFORD_BLAKE || cfg->beat == CF_BEAT_FULFORD_BLAKE_ORIGINAL,
                "%s: unknown beat %d", who, cfg->beat);
     CF_REQUIRE(cfg->precond == CF_PRECOND_NONE || cfg->precond == CF_PRECOND_BLOCK_DIAG ||
-                   cfg->precond == CF_PRECOND_LINE,
+                   cfg->precond == CF_PRECOND_LINE || cfg->precond == CF_PRECOND_LEARNED,
                "%s: preconditioner %d not available in this entry point", who, cfg->precond);
     CF_REQUIRE(cfg->line_patch >= 0 && cfg->line_patch <= 32, "%s: line_patch must be 0..32 (got %d)", who,
                cfg->line_patch);
@@ -588,6 +622,31 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     return CF_OK;
 }
 
+// Neighbours of each filament along its lattice line (equal base x, consecutive
+// in y, the beat direction): [F][2], -1 where the line ends.
+int build_neighbours(Engine *e, const cf_sim_config *cfgs) {
+    std::vector<int> nbr(2 * static_cast<size_t>(e->d.F), -1);
+    for (int b = 0; b < e->B; ++b) {
+        const ArrayInfo &a = e->arr[b];
+        const double *bp = cfgs[b].base_pos;
+        std::vector<int> idx(a.F);
+        for (int q = 0; q < a.F; ++q) idx[q] = q;
+        std::sort(idx.begin(), idx.end(), [&](int u, int v) {
+            if (bp[3 * u] != bp[3 * v]) return bp[3 * u] < bp[3 * v];
+            return bp[3 * u + 1] < bp[3 * v + 1];
+        });
+        for (size_t q = 0; q < idx.size(); ++q) {
+            const double x0 = bp[3 * idx[q]];
+            const int g = a.fil0 + idx[q];
+            if (q > 0 && std::fabs(bp[3 * idx[q - 1]] - x0) <= 1e-6 * (1.0 + std::fabs(x0)))
+                nbr[2 * g] = a.fil0 + idx[q - 1];
+            if (q + 1 < idx.size() && std::fabs(bp[3 * idx[q + 1]] - x0) <= 1e-6 * (1.0 + std::fabs(x0)))
+                nbr[2 * g + 1] = a.fil0 + idx[q + 1];
+        }
+    }
+    return eng_upload(e, const_cast<int **>(&e->d.nbr), nbr.data(), nbr.size());
+}
+
 int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     const cf_sim_config &c0 = cfgs[0];
     e->common = c0;
@@ -649,10 +708,14 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     d.ldh = mi_max + 1;
     d.hstride = static_cast<long long>(mi_max + 2) * (mi_max + 1);
     d.sstride = mi_max + 2;
-    d.flexible = 0;
-    d.precond = (c0.precond == CF_PRECOND_BLOCK_DIAG || c0.precond == CF_PRECOND_LINE) ? 1 : 0;
+    d.precond = (c0.precond == CF_PRECOND_NONE) ? 0 : 1;
     d.line = c0.precond == CF_PRECOND_LINE ? 1 : 0;
     e->line = d.line != 0;
+    d.learned = c0.precond == CF_PRECOND_LEARNED ? 1 : 0;
+    e->learned = d.learned != 0;
+    d.flexible = d.learned;
+    d.lin = 9 * ns + 2;   // own force rows, 2 rate rows, neighbour-mean force rows, shape
+    d.lout = 3 * ns + 2;
     d.dyn_phase = dp;
     d.dyn_angle = da;
     d.dt = c0.dt;
@@ -707,6 +770,11 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     CF_TRY(eng_alloc(e, &d.t, nr));
     CF_TRY(eng_alloc(e, &d.Q, (mi + 1) * ldq));
     d.Z = nullptr;
+    if (d.flexible) CF_TRY(eng_alloc(e, &d.Z, (mi + 1) * ldq));
+    CF_TRY(eng_alloc(e, &d.lx, static_cast<size_t>(F) * d.lin));
+    CF_TRY(eng_alloc(e, &d.ly, static_cast<size_t>(F) * d.lout));
+    CF_TRY(eng_alloc(e, &d.lscale, F));
+    CF_TRY(build_neighbours(e, cfgs));
     const size_t sm = static_cast<size_t>(B) * d.sstride;
     CF_TRY(eng_alloc(e, &d.H, static_cast<size_t>(B) * d.hstride));
     CF_TRY(eng_alloc(e, &d.cs, sm));
@@ -1136,6 +1204,7 @@ namespace {
 int launches_for(const Engine *e, int iters) {
     int n = 1 + 5 + 7 * iters + 3;
     if (e && e->line) n += 2 * iters + 1 + (e->refreshed_last ? refresh_launches(e) : 0);
+    if (e && e->learned) n += 6 * iters;  // features, 3 GEMMs, correction, packing
     return n;
 }
 }  // namespace
@@ -1230,6 +1299,66 @@ extern "C" int cf_sim_precond_info(cf_sim *s, int *n_patches, int *max_n, double
     if (max_n) *max_n = s->line ? s->P.max_n : 0;
     if (refresh_flops) *refresh_flops = fl;
     if (apply_bytes) *apply_bytes = by;
+    return CF_OK;
+}
+
+extern "C" int cf_sim_learned_dims(cf_sim *s, int *n_in, int *n_out) {
+    clear_error();
+    CF_REQUIRE(s, "null handle");
+    if (n_in) *n_in = s->d.lin;
+    if (n_out) *n_out = s->d.lout;
+    return CF_OK;
+}
+
+extern "C" int cf_sim_set_network(cf_sim *s, cf_mlp *net) {
+    clear_error();
+    CF_REQUIRE(s && net, "null argument");
+    CF_REQUIRE(s->learned, "cf_sim_set_network: the handle does not use CF_PRECOND_LEARNED");
+    int in = 0, out = 0, mb = 0;
+    mlp_dims(net, &in, &out, &mb);
+    CF_REQUIRE(in == s->d.lin && out == s->d.lout && mb >= s->d.F,
+               "cf_sim_set_network: network %d -> %d (batch %d) does not fit %d -> %d for %d filaments", in, out, mb,
+               s->d.lin, s->d.lout, s->d.F);
+    CF_CUDA(cudaSetDevice(s->device));
+    CF_CUDA(cudaStreamSynchronize(s->stream));
+    s->net = net;
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->exec = nullptr;
+    s->graph = nullptr;
+    return CF_OK;
+}
+
+extern "C" int cf_sim_collect_pairs(cf_sim *s, int nt, int max_pairs, float *x, float *t, int *rows) {
+    clear_error();
+    CF_REQUIRE(s && x && t && max_pairs > 0, "cf_sim_collect_pairs: bad arguments");
+    CF_REQUIRE(!s->learned && !s->line && s->d.precond == 1,
+               "cf_sim_collect_pairs: pairs come from the block-diagonal solver (CF_PRECOND_BLOCK_DIAG)");
+    CF_REQUIRE(nt >= 0, "cf_sim_collect_pairs: nt must be >= 0");
+    CF_CUDA(cudaSetDevice(s->device));
+    s->cx = x;
+    s->ct = t;
+    s->c_max = max_pairs;
+    s->c_pairs = 0;
+    const int rc = run_step(s, nt);
+    const int pairs = s->c_pairs;
+    s->cx = s->ct = nullptr;
+    s->c_max = s->c_pairs = 0;
+    CF_TRY(rc);
+    CF_CUDA(cudaStreamSynchronize(s->stream));
+    if (rows) *rows = pairs * s->d.F;
+    return CF_OK;
+}
+
+extern "C" int cf_sim_features(cf_sim *s, const double *v, float *x) {
+    clear_error();
+    CF_REQUIRE(s && v && x, "null argument");
+    CF_CUDA(cudaSetDevice(s->device));
+    CF_CUDA(cudaMemcpyAsync(s->d.t, v, sizeof(double) * s->arr[0].n, cudaMemcpyHostToDevice, s->stream));
+    learned_features_kernel<<<s->d.F, s->fil_threads, 0, s->stream>>>(s->d, s->d.t, s->d.lx, s->d.lscale);
+    CF_CHECK_LAUNCH("learned_features_kernel");
+    CF_CUDA(cudaMemcpyAsync(x, s->d.lx, sizeof(float) * s->d.F * s->d.lin, cudaMemcpyDeviceToHost, s->stream));
+    CF_CUDA(cudaStreamSynchronize(s->stream));
     return CF_OK;
 }
 

@@ -103,6 +103,10 @@ struct SimDev {
     int flexible;             // keep Z = P^{-1} Q (nonlinear preconditioner)
     int precond;              // 0: none, 1: block-diagonal (also the fallback of the patch preconditioner)
     int line;                 // line-patch preconditioner (patch_kernels.cuh) applied between kernels
+    int learned;              // block-diagonal + network correction (learned_kernels.cuh), flexible GMRES
+    const int *nbr;           // [F][2] neighbours of each filament along its lattice line (-1: none)
+    float *lx, *ly, *lscale;  // network input [F][lin], output [F][lout], residual scale [F]
+    int lin, lout;            // feature and correction widths
     int dyn_phase, dyn_angle; // rate blocks present
     int s_rows, s_cols;       // arclength table (0 rows: bisection)
     int n_phase_refs, n_angle_refs;
@@ -588,17 +592,18 @@ __global__ void arnoldi_precond_kernel(SimDev d, cudaGraphConditionalHandle h) {
         if (fr.pr >= 0) q[fr.pr] = src[fr.pr] * sc;
         if (fr.ar >= 0) q[fr.ar] = src[fr.ar] * sc;
     }
-    if (d.line) {  // the patch preconditioner runs next, from a fixed copy of Q_k
+    if (d.line || d.learned) {  // the next kernels read a fixed copy of Q_k
         for (int j = threadIdx.x; j < nb; j += blockDim.x) d.t[fr.lam + j] = q[fr.lam + j];
         if (threadIdx.x == 0) {
             if (fr.pr >= 0) d.t[fr.pr] = q[fr.pr];
             if (fr.ar >= 0) d.t[fr.ar] = q[fr.ar];
         }
-        return;
+        if (d.line) return;
     }
     __syncthreads();
     double *zout = d.flexible ? d.Z + static_cast<size_t>(k) * d.ldq : d.z;
     precond_block(d, m, fr, q, zout, smp, sm32);
+    if (d.learned) return;  // the network's correction and the packing follow
     for (int kk = threadIdx.x; kk < d.nseg; kk += blockDim.x) {
         const long long r = fr.lam + 3 * kk;
         d.f4[m * d.nseg + kk] = make_float4(static_cast<float>(zout[r]), static_cast<float>(zout[r + 1]),

@@ -158,6 +158,38 @@ class WallCiliaSimulation:
     def launches_per_step(self, iters: int) -> int:
         return _lib.load().cf_sim_launches_per_step(self._h, int(iters))
 
+    # -- learned preconditioner (CF_PRECOND_LEARNED) -------------------------
+    def learned_dims(self):
+        """(feature width, correction width) of the per-filament network."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _lib.call("cf_sim_learned_dims", self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def set_network(self, net):
+        """Attaches a FilamentMLP (kept alive by this object) as the learned correction."""
+        _lib.call("cf_sim_set_network", self._h, net.handle)
+        self._net = net
+
+    def collect_pairs(self, nt: int, max_pairs: int):
+        """Runs step nt (block-diagonal handle) and returns the training pairs of its first
+        `max_pairs` Arnoldi products as torch CUDA tensors (features [rows, in], targets [rows, out])."""
+        import torch
+        n_in, n_out = self.learned_dims()
+        x = torch.empty((max_pairs * self.n_fil, n_in), dtype=torch.float32, device="cuda")
+        t = torch.empty((max_pairs * self.n_fil, n_out), dtype=torch.float32, device="cuda")
+        rows = ctypes.c_int()
+        _lib.call("cf_sim_collect_pairs", self._h, int(nt), int(max_pairs), ctypes.c_void_p(x.data_ptr()),
+                  ctypes.c_void_p(t.data_ptr()), ctypes.byref(rows))
+        return x[:rows.value], t[:rows.value]
+
+    def features(self, v) -> np.ndarray:
+        """Network features [n_fil, in] of a host vector of the system size."""
+        v = np.ascontiguousarray(v, np.float64)
+        n_in, _ = self.learned_dims()
+        out = np.zeros((self.n_fil, n_in), np.float32)
+        _lib.call("cf_sim_features", self._h, _p(v), _p(out))
+        return out
+
     def refresh_preconditioner(self):
         """CF_PRECOND_LINE: rebuilds the patch inverses for the current kinematics (asynchronous)."""
         _lib.call("cf_sim_refresh_preconditioner", self._h)

@@ -317,6 +317,27 @@ CF_API int cf_mlp_get_params(cf_mlp *h, float *params);
 CF_API int cf_mlp_set_params(cf_mlp *h, const float *params);
 CF_API int cf_mlp_stream(cf_mlp *h, void **stream);
 
+/* Learned preconditioner (CF_PRECOND_LEARNED, flexible GMRES): the
+ * block-diagonal preconditioner plus a per-filament network correction
+ * z_m = P_bd(r)_m + s_m net(features_m(r)); no counterpart in the reference.
+ * Features per filament, scaled by s_m = |(r_m, rbar_m)|: its 3*nseg force
+ * rows and 2 rate rows, the mean force rows of its neighbours along the
+ * lattice line (rbar_m), then its segment positions relative to its base over
+ * the filament length (unscaled): 9*nseg + 2 values; the correction has
+ * 3*nseg + 2.  cf_sim_learned_dims gives both widths.
+ * cf_sim_set_network attaches a cf_mlp of those widths (batch >= n_fil); the
+ * handle keeps the pointer, the caller keeps ownership.
+ * cf_sim_collect_pairs runs step nt of a CF_PRECOND_BLOCK_DIAG handle and,
+ * after each of its first max_pairs Arnoldi products w = A z, writes the
+ * features of w and the target (z_m - P_bd(w)_m) / s_m of every filament into
+ * the device arrays x [max_pairs*n_fil][in] and t [max_pairs*n_fil][out];
+ * rows = the number written.  cf_sim_features: features of a host vector
+ * (system size) into host x [n_fil][in]. */
+CF_API int cf_sim_learned_dims(cf_sim *s, int *n_in, int *n_out);
+CF_API int cf_sim_set_network(cf_sim *s, cf_mlp *net);
+CF_API int cf_sim_collect_pairs(cf_sim *s, int nt, int max_pairs, float *x, float *t, int *rows);
+CF_API int cf_sim_features(cf_sim *s, const double *v, float *x);
+
 /* ------------------------------------------------------------------------
  * Batches of independent arrays (periodic-orbit / bisection sweeps): many
  * wall arrays of uneven size stepped together, one graph launch per step for

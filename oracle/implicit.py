@@ -218,6 +218,31 @@ class WallCilia:
             out[rows] = np.linalg.solve(self.patch_block(fils), v[rows])
         return out
 
+    def learned_features(self, v):
+        """Features of the learned preconditioner's network for vector v (not a reference routine):
+        [own force rows | 2 rate rows | neighbour-mean force rows] / s, then the shape relative to the
+        base over the filament length; returns (X [F, 9*nseg+2], s [F])."""
+        ns, F = self.nseg, self.nfil
+        n3, po, ao = self._offsets()
+        v = np.asarray(v, float)
+        lam = v[:n3].reshape(F, 3 * ns)
+        rates = np.zeros((F, 2))
+        if po is not None:
+            rates[:, 0] = v[po:po + F]
+        if ao is not None:
+            rates[:, 1] = v[ao:ao + F]
+        nbr = line_neighbours(self.bases)
+        mean = np.zeros_like(lam)
+        for m in range(F):
+            ids = [k for k in nbr[m] if k >= 0]
+            if ids:
+                mean[m] = lam[ids].mean(0)
+        s = np.sqrt((lam ** 2).sum(1) + (rates ** 2).sum(1) + (mean ** 2).sum(1))
+        si = np.where(s > 0, 1.0 / np.where(s > 0, s, 1.0), 0.0)
+        shape = (self.x.reshape(F, ns, 3) - self.bases[:, None, :]).reshape(F, 3 * ns) / self.fil_length
+        X = np.concatenate([lam * si[:, None], rates * si[:, None], mean * si[:, None], shape], 1)
+        return X, s
+
     # -- mobility product (Mss_mult, wall, 3x3) -----------------------------
     def mobility(self, lam):
         f = np.asarray(lam, float).reshape(-1, 3)
@@ -345,6 +370,20 @@ class WallCilia:
 
     def tips(self):
         return self.x.reshape(self.nfil, self.nseg, 3)[:, -1, :].copy()
+
+
+def line_neighbours(bases):
+    """[F, 2] previous / next filament along each lattice line (equal base x, sorted by y), -1 at the ends."""
+    b = np.asarray(bases, float).reshape(-1, 3)
+    order = sorted(range(b.shape[0]), key=lambda i: (b[i, 0], b[i, 1]))
+    nbr = -np.ones((b.shape[0], 2), int)
+    for q, i in enumerate(order):
+        x0 = b[i, 0]
+        if q > 0 and abs(b[order[q - 1], 0] - x0) <= 1e-6 * (1.0 + abs(x0)):
+            nbr[i, 0] = order[q - 1]
+        if q + 1 < len(order) and abs(b[order[q + 1], 0] - x0) <= 1e-6 * (1.0 + abs(x0)):
+            nbr[i, 1] = order[q + 1]
+    return nbr
 
 
 def line_patches(bases, line_patch=32):
