@@ -122,6 +122,7 @@ SIGNATURES = {
     "cf_sim_refresh_preconditioner": [_vp],
     "cf_sim_learned_dims": [_vp, _vp, _vp],
     "cf_sim_set_network": [_vp, _vp],
+    "cf_sim_set_network_weight": [_vp, ctypes.c_double],
     "cf_sim_collect_pairs": [_vp, _i, _i, _vp, _vp, _vp],
     "cf_sim_features": [_vp, _vp, _vp],
     "cf_sim_precond_info": [_vp, _vp, _vp, _vp, _vp],

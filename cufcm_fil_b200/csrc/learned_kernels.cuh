@@ -77,7 +77,7 @@ __global__ void learned_correct_kernel(SimDev d, const float *Y, const float *sc
     if (k >= d.arr[fr.b].max_iter) return;
     double *zk = d.Z + static_cast<size_t>(k) * d.ldq;
     const int nl = 3 * d.nseg;
-    const double s = scale[m];
+    const double s = d.lalpha * scale[m];
     const float *y = Y + static_cast<size_t>(m) * d.lout;
     for (int j = threadIdx.x; j < nl; j += blockDim.x) {
         const double val = zk[fr.lam + j] + s * y[j];

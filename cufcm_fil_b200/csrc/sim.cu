@@ -715,6 +715,7 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     e->learned = d.learned != 0;
     d.flexible = d.learned;
     d.lin = 9 * ns + 2;   // own force rows, 2 rate rows, neighbour-mean force rows, shape
+    d.lalpha = 1.0;
     d.lout = 3 * ns + 2;
     d.dyn_phase = dp;
     d.dyn_angle = da;
@@ -1322,6 +1323,20 @@ extern "C" int cf_sim_set_network(cf_sim *s, cf_mlp *net) {
     CF_CUDA(cudaSetDevice(s->device));
     CF_CUDA(cudaStreamSynchronize(s->stream));
     s->net = net;
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->exec = nullptr;
+    s->graph = nullptr;
+    return CF_OK;
+}
+
+extern "C" int cf_sim_set_network_weight(cf_sim *s, double alpha) {
+    clear_error();
+    CF_REQUIRE(s, "null handle");
+    CF_REQUIRE(alpha >= 0.0 && alpha <= 4.0, "cf_sim_set_network_weight: weight %g outside [0, 4]", alpha);
+    CF_CUDA(cudaSetDevice(s->device));
+    CF_CUDA(cudaStreamSynchronize(s->stream));
+    s->d.lalpha = alpha;
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
     s->exec = nullptr;

@@ -107,6 +107,7 @@ struct SimDev {
     const int *nbr;           // [F][2] neighbours of each filament along its lattice line (-1: none)
     float *lx, *ly, *lscale;  // network input [F][lin], output [F][lout], residual scale [F]
     int lin, lout;            // feature and correction widths
+    double lalpha;            // weight of the network correction (chosen by validation; 1 by default)
     int dyn_phase, dyn_angle; // rate blocks present
     int s_rows, s_cols;       // arclength table (0 rows: bisection)
     int n_phase_refs, n_angle_refs;

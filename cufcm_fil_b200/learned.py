@@ -56,6 +56,8 @@ class Comparison:
     block_diagonal_status: int
     learned_iterations: int
     learned_status: int
+    weight: float = 1.0
+    by_weight: dict = None
 
     @property
     def gain(self) -> float:
@@ -67,11 +69,18 @@ class Comparison:
         return self.learned_status == _lib.CF_OK and self.learned_iterations < self.block_diagonal_iterations
 
 
-def compare(make_sim, seed, net: FilamentMLP, nt=0) -> Comparison:
-    """Step nt of the same state with the block-diagonal preconditioner and with the network."""
+def compare(make_sim, seed, net: FilamentMLP, nt=0, weights=(1.0, 0.5, 0.25)) -> Comparison:
+    """Step nt of the same state with the block-diagonal preconditioner and with the network at each
+    correction weight; the weight with the fewest converged iterations is reported."""
     with make_sim(seed, _lib.CF_PRECOND_BLOCK_DIAG) as sim:
         rb = sim.step(nt)
-    with make_sim(seed, _lib.CF_PRECOND_LEARNED) as sim:
-        sim.set_network(net)
-        rl = sim.step(nt)
-    return Comparison(rb.iterations, rb.status, rl.iterations, rl.status)
+    by_weight = {}
+    for w in weights:
+        with make_sim(seed, _lib.CF_PRECOND_LEARNED) as sim:
+            sim.set_network(net)
+            sim.set_network_weight(w)
+            r = sim.step(nt)
+            by_weight[w] = (r.iterations, r.status)
+    ok = [w for w in weights if by_weight[w][1] == _lib.CF_OK]
+    best = min(ok, key=lambda w: by_weight[w][0]) if ok else weights[0]
+    return Comparison(rb.iterations, rb.status, by_weight[best][0], by_weight[best][1], best, by_weight)

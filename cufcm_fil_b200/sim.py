@@ -170,6 +170,10 @@ class WallCiliaSimulation:
         _lib.call("cf_sim_set_network", self._h, net.handle)
         self._net = net
 
+    def set_network_weight(self, alpha: float):
+        """Weight of the network correction (0: the block-diagonal preconditioner alone)."""
+        _lib.call("cf_sim_set_network_weight", self._h, ctypes.c_double(alpha))
+
     def collect_pairs(self, nt: int, max_pairs: int):
         """Runs step nt (block-diagonal handle) and returns the training pairs of its first
         `max_pairs` Arnoldi products as torch CUDA tensors (features [rows, in], targets [rows, out])."""

@@ -335,6 +335,8 @@ CF_API int cf_mlp_stream(cf_mlp *h, void **stream);
  * (system size) into host x [n_fil][in]. */
 CF_API int cf_sim_learned_dims(cf_sim *s, int *n_in, int *n_out);
 CF_API int cf_sim_set_network(cf_sim *s, cf_mlp *net);
+/* Weight of the network correction, z_m = P_bd(r)_m + alpha s_m net(...), in [0, 4] (default 1). */
+CF_API int cf_sim_set_network_weight(cf_sim *s, double alpha);
 CF_API int cf_sim_collect_pairs(cf_sim *s, int nt, int max_pairs, float *x, float *t, int *rows);
 CF_API int cf_sim_features(cf_sim *s, const double *v, float *x);
 

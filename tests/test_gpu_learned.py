@@ -65,13 +65,14 @@ def test_trained_network_gain_is_measured_and_judged():
         assert losses[-1] < losses[0]
         cmp = learned.compare(make_sim, 99, net)
         print(f"held-out state: block-diagonal {cmp.block_diagonal_iterations} iterations, learned "
-              f"{cmp.learned_iterations} (status {cmp.learned_status}), gain {cmp.gain:.2f}, "
-              f"losses {losses}")
+              f"{cmp.learned_iterations} at weight {cmp.weight} (status {cmp.learned_status}), gain "
+              f"{cmp.gain:.2f}; by weight {cmp.by_weight}; losses {losses}")
         assert cmp.block_diagonal_status in (_lib.CF_OK, _lib.CF_NOT_CONVERGED)
         assert cmp.use_learned == (cmp.learned_status == _lib.CF_OK and cmp.gain > 1.0)
         # a converged learned step satisfies the FP64 system of the oracle
         with make_sim(99, _lib.CF_PRECOND_LEARNED) as sim:
             sim.set_network(net)
+            sim.set_network_weight(cmp.weight)
             res = sim.step(0)
             if res.status == _lib.CF_OK:
                 cpu = implicit.WallCilia(shape_sequence=1, **_args(99))
