@@ -295,6 +295,27 @@ def run_batched(local, inp):
                       "per step on 64 streams (concurrent) or with a wait after each (sequential)"}
 
 
+def run_large(local, inp, flush, steps=4):
+    """1024 cilia (32 x 32 lattice, 20 480 segments): whole-line patches against the block-diagonal preconditioner."""
+    import torch
+    from cufcm_fil_b200 import _lib
+    from cufcm_fil_b200.sim import lattice_simulation
+    out = {"workload": "1024 cilia x 20 segments, 32x32 lattice spacing 20a, phases U(0,2pi), GMRES tol 1e-6"}
+    for name, code in (("line_patches", _lib.CF_PRECOND_LINE), ("block_diagonal", _lib.CF_PRECOND_BLOCK_DIAG)):
+        sim = lattice_simulation(32, spacing=SPACING, nseg=NSEG, seg_sep=SEG_SEP, s_table=inp["s_table"],
+                                 gmres_tol=GMRES_TOL, device=local, precond=code)
+        stream = torch.cuda.ExternalStream(sim.stream_handle())
+        sim.step(0)
+        ms = time_steps(sim, stream, flush, 1, steps)
+        res = sim.last_solve()
+        its = sim.iteration_log(1 + steps)[1:1 + steps]
+        out[name] = {"timesteps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
+                     "gmres_iters_per_step": float(np.mean(its)), "converged": bool(res.status == _lib.CF_OK)}
+        sim.close()
+    out["speedup"] = out["line_patches"]["timesteps_per_s"] / out["block_diagonal"]["timesteps_per_s"]
+    return out
+
+
 def run_ours(args):
     import torch
     from cufcm_fil_b200 import RpyMobilitySolver, _lib
@@ -399,6 +420,7 @@ def run_ours(args):
     plain_value = plain_steps / (plain_ms / 1e3)
 
     batched = run_batched(local, inp) if (world == 1 and not args.no_batched) else None
+    large = run_large(local, inp, flush) if (world == 1 and not args.no_batched) else None
 
     if rank == 0:
         cs = clocks.summary()
@@ -433,10 +455,14 @@ def run_ours(args):
             "rpy_pairs_per_s": pairs / (apply_us * 1e-6), "rpy_apply_us": apply_us,
             "patch_refresh_ms": refresh_ms, "tuning": tuning,
             "roofline": dominant, "roofline_other": other,
+            "traffic_note": "ncu (profiles/gj_update_16x16_patches.md): one gj_update launch, the refresh's top "
+                            "kernel, moves 77.4 MB of DRAM (the 63 MB of patch matrices stay L2-resident between "
+                            "rounds); the pair kernel 0.18 MB (profiles/rpy_wall_sym_batch_16x16_step.md)",
             "e2e": {"value": e2e_value, "unit": "timesteps/s", "h2d_bytes_per_step": 4 * F * 8,
                     "d2h_bytes_per_step": 4 * F * 8 + 3 * N * 8 + 3 * N * 8 + 16},
             "gpu_launches": launches, "clocks": cs,
             "batched": batched,
+            "lattice_32x32": large,
             "cpu_baseline": cpu_baseline(inp) if (world == 1 and not args.no_cpu_baseline) else None,
         }
         print(json.dumps(line), flush=True)
