@@ -102,9 +102,32 @@ __global__ void cell_bounds_kernel(Params p, const int *__restrict__ keys, int *
 
 // Per-warp tables of the particle's 1-D kernels (ngd <= 32).
 struct WarpTables {
-    float g[3][32];  // Gaussian factors along x, y, z
-    float d[3][32];  // grid point minus particle position along x, y, z
-    int ind[3][32];  // periodic grid indices
+    float g[3][32];   // Gaussian factors along x, y, z
+    float d2[3][32];  // squared distance of the grid point to the particle along x, y, z
+    int ind[3][32];   // periodic grid offsets: i, j*nx, k*nx*ny
+};
+
+// Walks the ngd^3 points of a particle's support, lane L taking the flattened
+// points L, L+32, ...: (ii, jj, kk) advance by the fixed strides of 32 with one
+// carry each instead of being divided out of the flat index.
+struct SupportWalk {
+    int ii, jj, kk, di, dj, dk, ngd;
+    __device__ __forceinline__ SupportWalk(int lane, int n) : ngd(n) {
+        const int n2 = n * n;
+        kk = lane / n2;
+        jj = (lane - kk * n2) / n;
+        ii = lane - kk * n2 - jj * n;
+        dk = 32 / n2;
+        dj = (32 - dk * n2) / n;
+        di = 32 - dk * n2 - dj * n;
+    }
+    __device__ __forceinline__ void next() {
+        ii += di;
+        jj += dj;
+        kk += dk;
+        if (ii >= ngd) { ii -= ngd; ++jj; }
+        if (jj >= ngd) { jj -= ngd; ++kk; }
+    }
 };
 
 __device__ __forceinline__ void build_tables(const Params &p, float4 y, WarpTables &t, int lane) {
@@ -118,8 +141,9 @@ __device__ __forceinline__ void build_tables(const Params &p, float4 y, WarpTabl
             const float xg = rintf(pos[c] / p.dx) - ngdh + lane;
             const float xx = xg * p.dx - pos[c];
             t.g[c][lane] = anorm * expf(-xx * xx * inv2s2);
-            t.d[c][lane] = xx;
-            t.ind[c][lane] = static_cast<int>(xg - n[c] * floorf(xg / n[c]));
+            t.d2[c][lane] = xx * xx;
+            const int stride = c == 0 ? 1 : (c == 1 ? p.nx : p.nx * p.ny);
+            t.ind[c][lane] = static_cast<int>(xg - n[c] * floorf(xg / n[c])) * stride;
         }
     }
     __syncwarp();
@@ -141,14 +165,12 @@ __global__ void __launch_bounds__(128) spread_kernel(Params p, const float4 *__r
     const float c_0 = 1.0f - 1.5f * p.pdmag / S2;
     const int ngd = p.ngd, ngd2 = ngd * ngd;
     float *gx = grid, *gy = grid + p.grid_size, *gz = grid + 2 * p.grid_size;
-    for (int tt = lane; tt < ngd2 * ngd; tt += 32) {
-        const int kk = tt / ngd2;
-        const int jj = (tt - kk * ngd2) / ngd;
-        const int ii = tt - kk * ngd2 - jj * ngd;
-        const float r2 = t.d[0][ii] * t.d[0][ii] + t.d[1][jj] * t.d[1][jj] + t.d[2][kk] * t.d[2][kk];
+    SupportWalk sw(lane, ngd);
+    for (int tt = lane; tt < ngd2 * ngd; tt += 32, sw.next()) {
+        const int ii = sw.ii, jj = sw.jj, kk = sw.kk;
+        const float r2 = t.d2[0][ii] + t.d2[1][jj] + t.d2[2][kk];
         const float wgt = t.g[0][ii] * t.g[1][jj] * t.g[2][kk] * (c_0 + c_r2 * r2);
-        const size_t ind = t.ind[0][ii] + static_cast<size_t>(t.ind[1][jj]) * p.nx +
-                           static_cast<size_t>(t.ind[2][kk]) * p.nx * p.ny;
+        const int ind = t.ind[0][ii] + t.ind[1][jj] + t.ind[2][kk];
         atomicAdd(gx + ind, f.x * wgt);
         atomicAdd(gy + ind, f.y * wgt);
         atomicAdd(gz + ind, f.z * wgt);
@@ -200,14 +222,12 @@ __global__ void __launch_bounds__(128) gather_kernel(Params p, const float4 *__r
     const int ngd = p.ngd, ngd2 = ngd * ngd;
     const float *gx = grid, *gy = grid + p.grid_size, *gz = grid + 2 * p.grid_size;
     float vx = 0.0f, vy = 0.0f, vz = 0.0f;
-    for (int tt = lane; tt < ngd2 * ngd; tt += 32) {
-        const int kk = tt / ngd2;
-        const int jj = (tt - kk * ngd2) / ngd;
-        const int ii = tt - kk * ngd2 - jj * ngd;
-        const float r2 = t.d[0][ii] * t.d[0][ii] + t.d[1][jj] * t.d[1][jj] + t.d[2][kk] * t.d[2][kk];
+    SupportWalk sw(lane, ngd);
+    for (int tt = lane; tt < ngd2 * ngd; tt += 32, sw.next()) {
+        const int ii = sw.ii, jj = sw.jj, kk = sw.kk;
+        const float r2 = t.d2[0][ii] + t.d2[1][jj] + t.d2[2][kk];
         const float wgt = t.g[0][ii] * t.g[1][jj] * t.g[2][kk] * (c_0 + c_r2 * r2) * vol;
-        const size_t ind = t.ind[0][ii] + static_cast<size_t>(t.ind[1][jj]) * p.nx +
-                           static_cast<size_t>(t.ind[2][kk]) * p.nx * p.ny;
+        const int ind = t.ind[0][ii] + t.ind[1][jj] + t.ind[2][kk];
         vx += __ldg(gx + ind) * wgt;
         vy += __ldg(gy + ind) * wgt;
         vz += __ldg(gz + ind) * wgt;
@@ -402,7 +422,8 @@ extern "C" int cf_fcm_create(const cf_fcm_config *cfg, cf_fcm **out) {
                "cf_fcm_create: parameters must be positive");
     const int ngd = static_cast<int>(std::lround(cfg->alpha * cfg->beta));
     CF_REQUIRE(ngd >= 1 && ngd <= 32, "cf_fcm_create: kernel support round(alpha*beta) = %d must lie in [1, 32]", ngd);
-    CF_REQUIRE(static_cast<double>(cfg->nx) * cfg->ny * cfg->nz < 4.0e9, "cf_fcm_create: grid too large");
+    CF_REQUIRE(static_cast<double>(cfg->nx) * cfg->ny * cfg->nz < 2147483647.0,
+               "cf_fcm_create: grid too large (at most 2^31 - 1 points: the kernels index it with 32-bit offsets)");
     CF_CUDA(cudaSetDevice(cfg->device));
     cf_fcm *h = new (std::nothrow) cf_fcm();
     if (!h) return set_error(CF_ENOMEM, "cf_fcm_create: host allocation failed");
