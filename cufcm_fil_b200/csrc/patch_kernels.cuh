@@ -115,50 +115,53 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
 // clears the patch's ok flag.
 __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     static_assert(kGjBlock * 4 == 256, "one row per 4 threads");
-    __shared__ float D[kGjBlock][kGjBlock + 1];
+    constexpr int Q = kGjBlock / 4;  // entries of a row held by each of its 4 threads
+    __shared__ float rowbuf[2][kGjBlock];
     const int p = blockIdx.x;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
     if (k0 >= n) return;
     const int b = min(kGjBlock, n - k0);
     const float *A = P.A + P.moff[p];
-    const int r = threadIdx.x >> 2, cq = threadIdx.x & 3;  // row r, columns cq + 4q
+    const int r = threadIdx.x >> 2, cq = threadIdx.x & 3;  // row r, columns cq + 4q (registers)
+    const int lane = threadIdx.x & 31;
     if (K == 0 && threadIdx.x == 0) P.ok[p] = 1;
+    float reg[Q];
 #pragma unroll
-    for (int q = 0; q < kGjBlock / 4; ++q) {
+    for (int q = 0; q < Q; ++q) {
         const int c = cq + 4 * q;
-        D[r][c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : 0.0f;
+        reg[q] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : 0.0f;
     }
-    __syncthreads();
     for (int t = 0; t < b; ++t) {
-        const float colr = D[r][t];
-        const float piv = D[t][t];
-        const float ip = 1.0f / piv;
-        if (threadIdx.x == 0 && (!(fabsf(piv) > 0.0f) || !isfinite(piv))) P.ok[p] = 0;
-        __syncthreads();
-        if (r == t) {
+        // the row's entry in column t, from the one of its 4 threads that holds it
+        float own = 0.0f;
 #pragma unroll
-            for (int q = 0; q < kGjBlock / 4; ++q) {
+        for (int q = 0; q < Q; ++q)
+            if (q == (t >> 2)) own = reg[q];
+        const float colr = __shfl_sync(0xffffffffu, own, (lane & ~3) | (t & 3));
+        float *rb = rowbuf[t & 1];
+        if (r == t) {  // scale the pivot row and publish it
+            const float ip = 1.0f / colr;  // colr is the pivot here
+            if (cq == (t & 3) && (!(fabsf(colr) > 0.0f) || !isfinite(colr))) P.ok[p] = 0;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
                 const int c = cq + 4 * q;
-                D[t][c] = (c == t) ? ip : D[t][c] * ip;
+                reg[q] = (c == t) ? ip : reg[q] * ip;
+                rb[c] = reg[q];
             }
         }
         __syncthreads();
-        if (r != t && r < b) {
+        if (r != t && r < b) {  // eliminate column t from the other rows
 #pragma unroll
-            for (int q = 0; q < kGjBlock / 4; ++q) {
+            for (int q = 0; q < Q; ++q) {
                 const int c = cq + 4 * q;
-                D[r][c] = (c == t) ? -colr * ip : D[r][c] - colr * D[t][c];
+                reg[q] = ((c == t) ? 0.0f : reg[q]) - colr * rb[c];
             }
         }
-        __syncthreads();
     }
     float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
 #pragma unroll
-    for (int q = 0; q < kGjBlock / 4; ++q) {
-        const int c = cq + 4 * q;
-        dv[r * kGjBlock + c] = D[r][c];
-    }
+    for (int q = 0; q < Q; ++q) dv[r * kGjBlock + cq + 4 * q] = (r < b) ? reg[q] : 0.0f;
 }
 
 // Round K, part (b), one thread per column j (and per row i = j) of a patch:
@@ -167,14 +170,15 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
 //   cbuf[i][s] = A[i, k0 + s]        for rows i outside the pivot rows (old values).
 // grid = (ceil(max_n / 256), patches).
 __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
-    __shared__ float Dv[kGjBlock][kGjBlock + 1];
-    const int p = blockIdx.y;
+    constexpr int G = 4, RG = kGjBlock / G;  // output-row groups (blockIdx.z) and rows per group
+    __shared__ float Dv[RG][kGjBlock + 1];
+    const int p = blockIdx.y, grp = blockIdx.z;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
     if (k0 >= n) return;
     const int b = min(kGjBlock, n - k0);
-    const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
-    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) Dv[e / kGjBlock][e % kGjBlock] = dv[e];
+    const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock + grp * RG * kGjBlock;
+    for (int e = threadIdx.x; e < RG * kGjBlock; e += blockDim.x) Dv[e / kGjBlock][e % kGjBlock] = dv[e];
     __syncthreads();
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -185,23 +189,22 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     float a[kGjBlock];
 #pragma unroll
     for (int s = 0; s < kGjBlock; ++s) a[s] = (!in_block && s < b) ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
-    for (int r0 = 0; r0 < kGjBlock; r0 += 16) {
 #pragma unroll
-        for (int r = r0; r < r0 + 16; ++r) {
-            float acc = 0.0f;
-            if (in_block) {
-                acc = Dv[r][j - k0];
-            } else {
+    for (int rr = 0; rr < RG; ++rr) {
+        float acc = 0.0f;
+        if (in_block) {
+            acc = Dv[rr][j - k0];
+        } else {
 #pragma unroll
-                for (int s = 0; s < kGjBlock; ++s) acc += Dv[r][s] * a[s];
-            }
-            rb[static_cast<size_t>(r) * n + j] = acc;  // rows r >= b hold zeros (D^-1 is zero-padded)
+            for (int s = 0; s < kGjBlock; ++s) acc += Dv[rr][s] * a[s];
         }
+        rb[static_cast<size_t>(grp * RG + rr) * n + j] = acc;  // rows >= b hold zeros (D^-1 is zero-padded)
     }
-    const int i = j;  // the same thread copies the old pivot columns of row i
+    // this group copies its quarter of the old pivot columns of row i = j
+    const int i = j;
     const bool pivot_row = i >= k0 && i < k0 + b;
-#pragma unroll 8
-    for (int s = 0; s < kGjBlock; ++s)
+#pragma unroll
+    for (int s = grp * RG; s < grp * RG + RG; ++s)
         cb[static_cast<size_t>(i) * kGjBlock + s] = (!pivot_row && s < b) ? A[static_cast<size_t>(i) * n + k0 + s] : 0.0f;
 }
 

@@ -249,7 +249,7 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     for (int K = 0; K < e->gj_rounds; ++K) {
         gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_pivot_kernel");
-        gj_prep_kernel<<<dim3(cols, P.np), 256, 0, st>>>(P, K);
+        gj_prep_kernel<<<dim3(cols, P.np, 4), 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_prep_kernel");
         gj_update_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_update_kernel");
