@@ -11,7 +11,9 @@
 // blocked Gauss-Jordan elimination without pivoting, in per-filament order
 // ([3*nseg lambda | phase rate | angle rate] per filament): every 62-unknown
 // filament block is eliminated lambda-first, so the rate pivots are Schur
-// complements -k^T M^-1 k and stay away from zero.  The preconditioner is
+// complements -k^T M^-1 k and stay away from zero.  The elimination is the
+// symmetric sweep (every intermediate matrix stays symmetric), so only the upper
+// block triangle is updated and the result is -A_pp^-1.  The preconditioner is
 // P^-1 r = blockdiag(A_pp^-1) r; it replaces apply_preconditioner_new
 // (mobility_solver.cpp:1102-1243), whose block-diagonal form (6 pi a on the
 // forces, a 2x2 Schur solve for the rates) remains the fallback of any patch
@@ -164,11 +166,14 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     for (int q = 0; q < Q; ++q) dv[r * kGjBlock + cq + 4 * q] = (r < b) ? reg[q] : 0.0f;
 }
 
-// Round K, part (b), one thread per column j (and per row i = j) of a patch:
-//   rbuf[s][j] = (D^-1 A[K, j])_s   for j outside the pivot columns,
-//   rbuf[s][j] = D^-1[s][j - k0]     for j inside them (the new pivot block),
-//   cbuf[i][s] = A[i, k0 + s]        for rows i outside the pivot rows (old values).
-// grid = (ceil(max_n / 256), patches).
+// Round K, part (b), one thread per column j of a patch (and one group of 16
+// of the 64 output rows per blockIdx.z).  The matrix is kept symmetric and only
+// its upper block triangle is maintained, so the pivot rows' entries are
+//   U[s][j] = A[k0 + s][j] for j >= k0,   A[j][k0 + s] for j < k0  (by symmetry),
+// and the pass writes
+//   rbuf[s][j] = (D^-1 U)[s][j] outside the pivot columns, -D^-1[s][j - k0] inside,
+//   cbuf[j][s] = U[s][j]         for j outside the pivot rows (zero inside).
+// grid = (ceil(max_n / 256), patches, 4).
 __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     constexpr int G = 4, RG = kGjBlock / G;  // output-row groups (blockIdx.z) and rows per group
     __shared__ float Dv[RG][kGjBlock + 1];
@@ -187,32 +192,36 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
     const bool in_block = j >= k0 && j < k0 + b;
     float a[kGjBlock];
+    if (j >= k0) {
 #pragma unroll
-    for (int s = 0; s < kGjBlock; ++s) a[s] = (!in_block && s < b) ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
+        for (int s = 0; s < kGjBlock; ++s) a[s] = (!in_block && s < b) ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
+    } else {
+#pragma unroll
+        for (int s = 0; s < kGjBlock; ++s) a[s] = (s < b) ? A[static_cast<size_t>(j) * n + k0 + s] : 0.0f;
+    }
 #pragma unroll
     for (int rr = 0; rr < RG; ++rr) {
         float acc = 0.0f;
         if (in_block) {
-            acc = Dv[rr][j - k0];
+            acc = -Dv[rr][j - k0];
         } else {
 #pragma unroll
             for (int s = 0; s < kGjBlock; ++s) acc += Dv[rr][s] * a[s];
         }
         rb[static_cast<size_t>(grp * RG + rr) * n + j] = acc;  // rows >= b hold zeros (D^-1 is zero-padded)
     }
-    // this group copies its quarter of the old pivot columns of row i = j
-    const int i = j;
-    const bool pivot_row = i >= k0 && i < k0 + b;
+    // this group's quarter of the pivot-row entries of column j, transposed: row j of cbuf
 #pragma unroll
-    for (int s = grp * RG; s < grp * RG + RG; ++s)
-        cb[static_cast<size_t>(i) * kGjBlock + s] = (!pivot_row && s < b) ? A[static_cast<size_t>(i) * n + k0 + s] : 0.0f;
+    for (int s = 0; s < RG; ++s)
+        cb[static_cast<size_t>(j) * kGjBlock + grp * RG + s] = in_block ? 0.0f : a[grp * RG + s];
 }
 
-// Round K, part (c), 64x64 tiles of the whole matrix:
-//   pivot rows       A[i, j] = rbuf[i - k0][j]
+// Round K, part (c), the 64x64 tiles of the upper block triangle:
+//   pivot rows       A[i, j] = rbuf[i - k0][j]      (-D^-1 in the pivot block)
 //   other rows       A[i, j] -= C_i . rbuf[:, j]   (j outside the pivot columns)
-//                    A[i, j]  = -C_i . rbuf[:, j]  (pivot columns: -C_i D^-1)
-// with C_i = cbuf[i][:].  Each thread owns 4 rows x 4 columns of the tile
+//                    A[i, j]  = -C_i . rbuf[:, j]  (pivot columns: C_i D^-1)
+// with C_i = cbuf[i][:] -- the symmetric sweep, which leaves -A^-1 after the
+// last round.  Each thread owns 4 rows x 4 columns of the tile
 // (columns interleaved by 16, so every load and store of a half-warp is one
 // contiguous run) and loads each of its rows of A in one batch.
 // grid = (tiles, patches).
@@ -227,6 +236,7 @@ __global__ void __launch_bounds__(256, 5) gj_update_kernel(PatchDev P, int K) {
     const int T = (n + kGjTile - 1) / kGjTile;
     if (static_cast<int>(blockIdx.x) >= T * T) return;
     const int ti = blockIdx.x / T, tj = blockIdx.x - ti * T;
+    if (ti > tj) return;  // the lower block triangle is filled in once, after the last round
     const int row0 = ti * kGjTile, col0 = tj * kGjTile;
     float *__restrict__ A = P.A + P.moff[p];
     const float *__restrict__ cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
@@ -282,6 +292,30 @@ __global__ void __launch_bounds__(256, 5) gj_update_kernel(PatchDev P, int K) {
     }
 }
 
+// After the last round: fills the lower block triangle from the upper one
+// (tile (ti, tj), ti > tj, from the transpose of tile (tj, ti)); the matrix is
+// then -A_pp^-1 in full.  grid = (tiles, patches).
+__global__ void __launch_bounds__(256) gj_mirror_kernel(PatchDev P) {
+    __shared__ float tile[kGjTile][kGjTile + 1];
+    const int p = blockIdx.y;
+    const int n = P.nf[p] * P.nbf;
+    const int T = (n + kGjTile - 1) / kGjTile;
+    if (static_cast<int>(blockIdx.x) >= T * T) return;
+    const int ti = blockIdx.x / T, tj = blockIdx.x - ti * T;
+    if (ti <= tj) return;
+    float *A = P.A + P.moff[p];
+    const int r0 = tj * kGjTile, c0 = ti * kGjTile;  // the source tile, upper triangle
+    for (int e = threadIdx.x; e < kGjTile * kGjTile; e += blockDim.x) {
+        const int r = e / kGjTile, c = e - r * kGjTile;
+        tile[r][c] = (r0 + r < n && c0 + c < n) ? A[static_cast<size_t>(r0 + r) * n + c0 + c] : 0.0f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kGjTile * kGjTile; e += blockDim.x) {
+        const int r = e / kGjTile, c = e - r * kGjTile;  // destination (c0 + r, r0 + c)
+        if (c0 + r < n && r0 + c < n) A[static_cast<size_t>(c0 + r) * n + r0 + c] = tile[c][r];
+    }
+}
+
 // Clears a patch's ok flag if its inverse holds a non-finite entry.
 __global__ void patch_check_kernel(PatchDev P) {
     const int p = blockIdx.y;
@@ -332,7 +366,7 @@ __global__ void __launch_bounds__(256) patch_apply_kernel(SimDev d, PatchDev P, 
         double acc = 0.0;
         for (int c = lane; c < n; c += 32) acc += static_cast<double>(__ldg(ar + c)) * xs[c];
         acc = warp_sum(acc);
-        if (lane == 0) out[rows[r]] = acc;
+        if (lane == 0) out[rows[r]] = -acc;  // the refresh leaves -A_pp^-1
     }
 }
 
