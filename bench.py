@@ -364,16 +364,13 @@ def run_ours(args):
     torch.cuda.synchronize()
     e_events = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     e_events[0].record(stream)
+    h_x = torch.empty(3 * N, dtype=torch.float32).pin_memory()
+    h_f = torch.empty(6 * N, dtype=torch.float32).pin_memory()
     for k in range(args.steps):
-        sim.set_state(h_phase, h_angle, h_pd, h_ad)   # H2D 4*F doubles
-        sim.step(nt)                                    # D2H: solver status
+        # H2D 4*F doubles of state; D2H 4*F doubles of state, 3N + 6N floats of positions and forces, status
+        state = (h_phase, h_angle, h_pd, h_ad)
+        sim.step_io(nt, state_in=state, state_out=state, x_segs=h_x, f_segs=h_f)
         nt += 1
-        out = sim.state()                               # D2H 4*F doubles
-        x_segs, f_segs = sim.segments()                 # D2H 3N doubles (positions) + 3N doubles (forces)
-        h_phase.copy_(torch.from_numpy(out["phase"]))
-        h_angle.copy_(torch.from_numpy(out["angle"]))
-        h_pd.copy_(torch.from_numpy(out["phase_dot"]))
-        h_ad.copy_(torch.from_numpy(out["angle_dot"]))
     e_events[1].record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(world, e_events[0].elapsed_time(e_events[1]))
@@ -464,7 +461,9 @@ def run_ours(args):
                             "kernel, moves 77.4 MB of DRAM (the 63 MB of patch matrices stay L2-resident between "
                             "rounds); the pair kernel 0.18 MB (profiles/rpy_wall_sym_batch_16x16_step.md)",
             "e2e": {"value": e2e_value, "unit": "timesteps/s", "h2d_bytes_per_step": 4 * F * 8,
-                    "d2h_bytes_per_step": 4 * F * 8 + 3 * N * 8 + 3 * N * 8 + 16, "gmres_iters_per_step": e2e_iters,
+                    "d2h_bytes_per_step": 4 * F * 8 + 3 * N * 4 + 6 * N * 4 + 40, "gmres_iters_per_step": e2e_iters,
+                    "call": "WallCiliaSimulation.step_io (cf_sim_step_io): state up, step, state + positions + "
+                            "forces down, one synchronisation",
                     "steps": "the timed steps replayed from the state after the warm-up"},
             "gpu_launches": launches, "clocks": cs,
             "batched": batched,

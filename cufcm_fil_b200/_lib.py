@@ -108,6 +108,7 @@ SIGNATURES = {
     "cf_sim_get_state": [_vp, _vp, _vp, _vp, _vp],
     "cf_sim_get_segments": [_vp, _vp, _vp],
     "cf_sim_get_directions": [_vp, _vp, _vp],
+    "cf_sim_step_io": [_vp, _i] + [_vp] * 12,
     "cf_sim_get_arclengths": [_vp, _vp],
     "cf_sim_system_size": [_vp],
     "cf_sim_stream": [_vp, ctypes.POINTER(_vp)],

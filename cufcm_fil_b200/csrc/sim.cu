@@ -86,6 +86,7 @@ struct Engine {
     // learned correction
     bool learned = false;
     cf_mlp *net = nullptr;
+    float *seg_out = nullptr;  // staging of cf_sim_step_io's segment outputs [9N]
     // training-pair collection (host-driven steps only)
     float *cx = nullptr, *ct = nullptr;
     int c_max = 0, c_pairs = 0;
@@ -1153,6 +1154,39 @@ extern "C" int cf_sim_get_segments(cf_sim *s, float *x_segs, float *f_segs) {
             for (int c = 0; c < 6; ++c) f_segs[6 * i + c] = c < 3 ? static_cast<float>(buf[3 * i + c]) : 0.0f;
     }
     return CF_OK;
+}
+
+extern "C" int cf_sim_step_io(cf_sim *s, int nt, const double *phase_in, const double *angle_in,
+                              const double *phase_dot_in, const double *angle_dot_in, double *phase_out,
+                              double *angle_out, double *phase_dot_out, double *angle_dot_out, float *x_segs,
+                              float *f_segs, int *iters, double *relres) {
+    clear_error();
+    CF_REQUIRE(s, "null handle");
+    CF_REQUIRE(nt >= 0, "cf_sim_step_io: nt must be >= 0");
+    CF_CUDA(cudaSetDevice(s->device));
+    const int N = s->d.N;
+    if ((x_segs || f_segs) && !s->seg_out) CF_TRY(eng_alloc(s, &s->seg_out, 9 * static_cast<size_t>(N)));
+    CF_TRY(copy_state_in(s, phase_in, angle_in, phase_dot_in, angle_dot_in));
+    CF_TRY(run_step(s, nt));
+    const size_t fb = sizeof(double) * s->d.F;
+    cudaStream_t st = s->stream;
+    if (phase_out) CF_CUDA(cudaMemcpyAsync(phase_out, s->d.phase, fb, cudaMemcpyDeviceToHost, st));
+    if (angle_out) CF_CUDA(cudaMemcpyAsync(angle_out, s->d.angle, fb, cudaMemcpyDeviceToHost, st));
+    if (phase_dot_out) CF_CUDA(cudaMemcpyAsync(phase_dot_out, s->d.phase_dot, fb, cudaMemcpyDeviceToHost, st));
+    if (angle_dot_out) CF_CUDA(cudaMemcpyAsync(angle_dot_out, s->d.angle_dot, fb, cudaMemcpyDeviceToHost, st));
+    if (x_segs || f_segs) {
+        segments_out_kernel<<<(N + 255) / 256, 256, 0, st>>>(s->d, s->seg_out, s->seg_out + 3 * static_cast<size_t>(N));
+        CF_CHECK_LAUNCH("segments_out_kernel");
+        if (x_segs) CF_CUDA(cudaMemcpyAsync(x_segs, s->seg_out, sizeof(float) * 3 * N, cudaMemcpyDeviceToHost, st));
+        if (f_segs)
+            CF_CUDA(cudaMemcpyAsync(f_segs, s->seg_out + 3 * static_cast<size_t>(N), sizeof(float) * 6 * N,
+                                    cudaMemcpyDeviceToHost, st));
+    }
+    std::vector<GmresCtl> c;
+    CF_TRY(read_ctls(s, c));  // the one synchronisation
+    if (iters) *iters = iters_of(c[0]);
+    if (relres) *relres = c[0].relres;
+    return status_of(c[0], 0, 1);
 }
 
 extern "C" int cf_sim_get_directions(cf_sim *s, double *k_phase, double *k_angle) {

@@ -1090,6 +1090,21 @@ __global__ void finish_kernel(SimDev d) {
     }
 }
 
+// Segment positions and constraint forces of the batch's first array in the
+// reference's host layouts (x_segs [3N], f_segs [6N] with zero torques), FP32.
+__global__ void segments_out_kernel(SimDev d, float *x, float *f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const ArrayInfo &a = d.arr[0];
+    if (i >= a.N) return;
+    const int g = a.seg0 + i;
+    const long long row = a.voff + 3LL * i;
+    for (int c = 0; c < 3; ++c) {
+        x[3 * i + c] = static_cast<float>(d.xd[3 * g + c]);
+        f[6 * i + c] = static_cast<float>(d.sol[row + c]);
+        f[6 * i + 3 + c] = 0.0f;
+    }
+}
+
 // f4 = float(force rows of v) for the pair kernel, one thread per segment.
 __global__ void pack_forces_kernel(SimDev d, const double *v) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -105,6 +105,21 @@ class WallCiliaSimulation:
                        ok=(_lib.CF_OK, _lib.CF_NOT_CONVERGED))
         return GmresResult(it.value, rel.value, rc)
 
+    def step_io(self, nt: int, state_in=None, state_out=None, x_segs=None, f_segs=None) -> GmresResult:
+        """One step with its host traffic in one call: `state_in` / `state_out` are (phase, angle, phase_dot,
+        angle_dot) float64 host arrays (numpy or pinned torch; None skips), x_segs [3N] / f_segs [6N] float32."""
+        def q(a):
+            if a is None:
+                return None
+            return ctypes.c_void_p(a.ctypes.data if hasattr(a, "ctypes") else a.data_ptr())
+        si = list(state_in) if state_in is not None else [None] * 4
+        so = list(state_out) if state_out is not None else [None] * 4
+        it = ctypes.c_int()
+        rel = ctypes.c_double()
+        rc = _lib.call("cf_sim_step_io", self._h, int(nt), *(q(a) for a in si), *(q(a) for a in so), q(x_segs),
+                       q(f_segs), ctypes.byref(it), ctypes.byref(rel), ok=(_lib.CF_OK, _lib.CF_NOT_CONVERGED))
+        return GmresResult(it.value, rel.value, rc)
+
     def step_async(self, nt: int):
         """Enqueues step nt (one graph launch); read the solve with :meth:`last_solve`."""
         _lib.call("cf_sim_step_async", self._h, int(nt))

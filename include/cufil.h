@@ -250,6 +250,15 @@ CF_API int cf_sim_get_state(cf_sim *s, double *phase, double *angle, double *pha
 /* Segment positions [3*N_s] and constraint forces [6*N_s] in the reference's
  * host layouts (x_segs_host / f_segs_host). */
 CF_API int cf_sim_get_segments(cf_sim *s, float *x_segs, float *f_segs);
+/* One step with its host traffic in a single call: uploads the filament state
+ * (any *_in may be NULL: keep the device state), runs step nt, and returns the
+ * new state [n_fil] each, the segment positions x_segs [3*N_s] and constraint
+ * forces f_segs [6*N_s] (reference layouts), iterations and residual (any
+ * output may be NULL), with one synchronisation.  Same status as cf_sim_step. */
+CF_API int cf_sim_step_io(cf_sim *s, int nt, const double *phase_in, const double *angle_in,
+                          const double *phase_dot_in, const double *angle_dot_in, double *phase_out,
+                          double *angle_out, double *phase_dot_out, double *angle_dot_out, float *x_segs,
+                          float *f_segs, int *iters, double *relres);
 /* Velocity directions K_phase, K_angle [3*N_s] each (vel_dir_phase/angle). */
 CF_API int cf_sim_get_directions(cf_sim *s, double *k_phase, double *k_angle);
 /* Arclength parameters of the current kinematics [n_fil*n_seg] (s_to_use). */

@@ -151,3 +151,23 @@ def test_zero_rhs_gives_zero_solution():
         res = gpu.step(0)
         _, fs = gpu.segments()
         assert res.iterations == 0 and np.all(fs == 0.0)
+
+
+def test_step_io_equals_separate_calls(s_table):
+    gpu_a, _ = make_pair(3, 40.0, s_table, seed=8)
+    gpu_b, _ = make_pair(3, 40.0, s_table, seed=8)
+    with gpu_a, gpu_b:
+        st = gpu_a.state()
+        state = tuple(np.array(st[k]) for k in ("phase", "angle", "phase_dot", "angle_dot"))
+        x = np.zeros(3 * gpu_a.n_seg_total, np.float32)
+        f = np.zeros(6 * gpu_a.n_seg_total, np.float32)
+        for nt in range(3):
+            ra = gpu_a.step_io(nt, state_in=state, state_out=state, x_segs=x, f_segs=f)
+            rb = gpu_b.step(nt)
+            assert ra.iterations == rb.iterations and ra.status == rb.status
+        sb = gpu_b.state()
+        for arr, key in zip(state, ("phase", "angle", "phase_dot", "angle_dot")):
+            np.testing.assert_array_equal(arr, sb[key])
+        xb, fb = gpu_b.segments()
+        np.testing.assert_array_equal(x, xb)
+        np.testing.assert_array_equal(f, fb)
