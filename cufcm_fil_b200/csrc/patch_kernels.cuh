@@ -111,23 +111,22 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
     }
 }
 
-// Round K of the blocked Gauss-Jordan inversion, part (a), one block per
-// patch: inverts the pivot block D = A[K, K] (b <= 64) in shared memory and
-// stores D^-1 (zero-padded to 64 x 64) in dinv.  A non-finite or zero pivot
-// clears the patch's ok flag.
-__global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
+// Part (a) of a round: inverts pivot block K of patch p (rows and columns [64K, 64K + b)) in
+// place of dinv; called by all 256 threads of a block.  Each thread keeps 16
+// entries of the 64x64 block in registers (row tid/4, columns tid%4 + 4q); per
+// elimination step the pivot row is published through a double-buffered
+// shared row (one barrier per step) and each row's pivot-column entry comes
+// from a shuffle among the row's 4 threads.  A non-finite or zero pivot clears
+// the patch's ok flag.
+// A: the patch matrix (n x n), dv: its dinv block, ok: its flag.
+__device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int *ok, int K, float (*rowbuf)[kGjBlock]) {
     static_assert(kGjBlock * 4 == 256, "one row per 4 threads");
-    constexpr int Q = kGjBlock / 4;  // entries of a row held by each of its 4 threads
-    __shared__ float rowbuf[2][kGjBlock];
-    const int p = blockIdx.x;
-    const int n = P.nf[p] * P.nbf;
+    constexpr int Q = kGjBlock / 4;
     const int k0 = K * kGjBlock;
-    if (k0 >= n) return;
     const int b = min(kGjBlock, n - k0);
-    const float *A = P.A + P.moff[p];
-    const int r = threadIdx.x >> 2, cq = threadIdx.x & 3;  // row r, columns cq + 4q (registers)
+    const int r = threadIdx.x >> 2, cq = threadIdx.x & 3;
     const int lane = threadIdx.x & 31;
-    if (K == 0 && threadIdx.x == 0) P.ok[p] = 1;
+    if (K == 0 && threadIdx.x == 0) *ok = 1;
     float reg[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -135,7 +134,6 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
         reg[q] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : 0.0f;
     }
     for (int t = 0; t < b; ++t) {
-        // the row's entry in column t, from the one of its 4 threads that holds it
         float own = 0.0f;
 #pragma unroll
         for (int q = 0; q < Q; ++q)
@@ -144,7 +142,7 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
         float *rb = rowbuf[t & 1];
         if (r == t) {  // scale the pivot row and publish it
             const float ip = 1.0f / colr;  // colr is the pivot here
-            if (cq == (t & 3) && (!(fabsf(colr) > 0.0f) || !isfinite(colr))) P.ok[p] = 0;
+            if (cq == (t & 3) && (!(fabsf(colr) > 0.0f) || !isfinite(colr))) *ok = 0;
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 const int c = cq + 4 * q;
@@ -161,9 +159,23 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
             }
         }
     }
-    float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
 #pragma unroll
     for (int q = 0; q < Q; ++q) dv[r * kGjBlock + cq + 4 * q] = (r < b) ? reg[q] : 0.0f;
+}
+
+__device__ __forceinline__ void pivot_invert_patch(const PatchDev &P, int p, int K, float (*rowbuf)[kGjBlock]) {
+    pivot_invert(P.A + P.moff[p], P.nf[p] * P.nbf, P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock, P.ok + p, K,
+                 rowbuf);
+}
+
+// Round 0, part (a): the first pivot block of every patch (later pivot blocks
+// are inverted by the previous round's update, see gj_update_kernel).
+__global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
+    __shared__ float rowbuf[2][kGjBlock];
+    const int p = blockIdx.x;
+    const int n = P.nf[p] * P.nbf;
+    if (K * kGjBlock >= n) return;
+    pivot_invert_patch(P, p, K, rowbuf);
 }
 
 // Round K, part (b), one thread per column j of a patch (and one group of 16
@@ -225,7 +237,7 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
 // (columns interleaved by 16, so every load and store of a half-warp is one
 // contiguous run) and loads each of its rows of A in one batch.
 // grid = (tiles, patches).
-__global__ void __launch_bounds__(256, 5) gj_update_kernel(PatchDev P, int K) {
+__global__ void __launch_bounds__(256, 4) gj_update_kernel(PatchDev P, int K) {
     __shared__ float Cs[kGjTile][kGjBlock + 1];
     __shared__ float Rs[kGjBlock][kGjTile + 1];
     const int p = blockIdx.y;
@@ -235,7 +247,12 @@ __global__ void __launch_bounds__(256, 5) gj_update_kernel(PatchDev P, int K) {
     const int b = min(kGjBlock, n - k0);
     const int T = (n + kGjTile - 1) / kGjTile;
     if (static_cast<int>(blockIdx.x) >= T * T) return;
-    const int ti = blockIdx.x / T, tj = blockIdx.x - ti * T;
+    // Block 0 takes the next round's diagonal tile, so that it starts first and, after its update,
+    // inverts that pivot block for the next round while the other blocks finish theirs.
+    const int diag = (K + 1 < T) ? (K + 1) * T + (K + 1) : -1;
+    int tile = blockIdx.x;
+    if (diag >= 0) tile = (blockIdx.x == 0) ? diag : (static_cast<int>(blockIdx.x) <= diag ? blockIdx.x - 1 : blockIdx.x);
+    const int ti = tile / T, tj = tile - ti * T;
     if (ti > tj) return;  // the lower block triangle is filled in once, after the last round
     const int row0 = ti * kGjTile, col0 = tj * kGjTile;
     float *__restrict__ A = P.A + P.moff[p];
@@ -289,6 +306,11 @@ __global__ void __launch_bounds__(256, 5) gj_update_kernel(PatchDev P, int K) {
             ar[j] = pivot_row ? Rs[i - k0][v * 16 + tx]
                               : ((j >= k0 && j < k0 + b) ? -acc[u][v] : old[v] - acc[u][v]);
         }
+    }
+    if (tile == diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
+        __shared__ float rowbuf[2][kGjBlock];
+        __syncthreads();
+        pivot_invert_patch(P, p, K + 1, rowbuf);
     }
 }
 

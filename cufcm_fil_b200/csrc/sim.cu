@@ -247,9 +247,9 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     patch_rates_kernel<<<P.np, 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_rates_kernel");
     const int cols = (P.max_n + 255) / 256;
+    gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, 0);  // later pivot blocks: inverted inside the previous update
+    CF_CHECK_LAUNCH("gj_pivot_kernel");
     for (int K = 0; K < e->gj_rounds; ++K) {
-        gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, K);
-        CF_CHECK_LAUNCH("gj_pivot_kernel");
         gj_prep_kernel<<<dim3(cols, P.np, 4), 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_prep_kernel");
         gj_update_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P, K);
@@ -262,7 +262,7 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     return CF_OK;
 }
 
-int refresh_launches(const Engine *e) { return e->line ? 4 + 3 * e->gj_rounds : 0; }
+int refresh_launches(const Engine *e) { return e->line ? 5 + 2 * e->gj_rounds : 0; }
 
 int launch_patch_apply(Engine *e, const double *in, double *out, int masked, cudaStream_t st) {
     patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), 256, e->apply_smem, st>>>(e->d, e->P, in, out, masked);
