@@ -236,22 +236,24 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
 // last round.  Each thread owns 4 rows x 4 columns of the tile
 // (columns interleaved by 16, so every load and store of a half-warp is one
 // contiguous run) and loads each of its rows of A in one batch.
-// grid = (tiles, patches).
+// grid = (patches, tiles): patches run fastest, so every patch's first block
+// (the diagonal tile below) is issued in the first wave.
 __global__ void __launch_bounds__(256, 4) gj_update_kernel(PatchDev P, int K) {
     __shared__ float Cs[kGjTile][kGjBlock + 1];
     __shared__ float Rs[kGjBlock][kGjTile + 1];
-    const int p = blockIdx.y;
+    const int p = blockIdx.x;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
     if (k0 >= n) return;
     const int b = min(kGjBlock, n - k0);
     const int T = (n + kGjTile - 1) / kGjTile;
-    if (static_cast<int>(blockIdx.x) >= T * T) return;
+    const int bid = blockIdx.y;
+    if (bid >= T * T) return;
     // Block 0 takes the next round's diagonal tile, so that it starts first and, after its update,
     // inverts that pivot block for the next round while the other blocks finish theirs.
     const int diag = (K + 1 < T) ? (K + 1) * T + (K + 1) : -1;
-    int tile = blockIdx.x;
-    if (diag >= 0) tile = (blockIdx.x == 0) ? diag : (static_cast<int>(blockIdx.x) <= diag ? blockIdx.x - 1 : blockIdx.x);
+    int tile = bid;
+    if (diag >= 0) tile = (bid == 0) ? diag : (bid <= diag ? bid - 1 : bid);
     const int ti = tile / T, tj = tile - ti * T;
     if (ti > tj) return;  // the lower block triangle is filled in once, after the last round
     const int row0 = ti * kGjTile, col0 = tj * kGjTile;

@@ -252,7 +252,7 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     for (int K = 0; K < e->gj_rounds; ++K) {
         gj_prep_kernel<<<dim3(cols, P.np, 4), 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_prep_kernel");
-        gj_update_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P, K);
+        gj_update_kernel<<<dim3(P.np, e->gj_tiles), 256, 0, st>>>(P, K);  // patches fastest: diagonals first
         CF_CHECK_LAUNCH("gj_update_kernel");
     }
     gj_mirror_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P);
