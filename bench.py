@@ -342,7 +342,7 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     first_nt = nt
-    snapshot = sim.state()  # the end-to-end leg replays the timed steps from here
+    snapshot = sim.checkpoint()  # the end-to-end leg replays the timed steps from here
     barrier(world)
     with ClockSampler(local) as clocks:
         total_ms = time_steps(sim, stream, flush, nt, args.steps)
@@ -359,6 +359,7 @@ def run_ours(args):
     #      the trajectory would need a different number of GMRES iterations)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64)).pin_memory()
     st = snapshot
+    sim.restore(st)  # the warm start too: the first replayed step then starts exactly as the first timed one
     h_phase, h_angle, h_pd, h_ad = (pin(st[k]) for k in ("phase", "angle", "phase_dot", "angle_dot"))
     nt = first_nt
     F = NX * NX

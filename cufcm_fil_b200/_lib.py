@@ -113,6 +113,8 @@ SIGNATURES = {
     "cf_sim_system_size": [_vp],
     "cf_sim_stream": [_vp, ctypes.POINTER(_vp)],
     "cf_sim_set_state": [_vp, _vp, _vp, _vp, _vp],
+    "cf_sim_get_solution": [_vp, _vp],
+    "cf_sim_set_solution": [_vp, _vp],
     "cf_sim_iteration_log": [_vp, _vp, _i],
     "cf_sim_launches_per_step": [_vp, _i],
     "cf_sim_initial_guess": [_vp, _i],

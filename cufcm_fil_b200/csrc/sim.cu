@@ -1226,6 +1226,29 @@ extern "C" int cf_sim_set_state(cf_sim *s, const double *phase, const double *an
     return copy_state_in(s, phase, angle, phase_dot, angle_dot);
 }
 
+extern "C" int cf_sim_get_solution(cf_sim *s, double *sol) {
+    clear_error();
+    CF_REQUIRE(s && sol, "cf_sim_get_solution: bad arguments");
+    CF_CUDA(cudaSetDevice(s->device));
+    CF_CUDA(cudaMemcpyAsync(sol, s->d.sol, sizeof(double) * s->arr[0].n, cudaMemcpyDeviceToHost, s->stream));
+    CF_CUDA(cudaStreamSynchronize(s->stream));
+    return CF_OK;
+}
+
+extern "C" int cf_sim_set_solution(cf_sim *s, const double *sol) {
+    clear_error();
+    CF_REQUIRE(s && sol, "cf_sim_set_solution: bad arguments");
+    CF_CUDA(cudaSetDevice(s->device));
+    const ArrayInfo &a = s->arr[0];
+    CF_CUDA(cudaMemcpyAsync(s->d.sol, sol, sizeof(double) * a.n, cudaMemcpyHostToDevice, s->stream));
+    // the rate rows are the filament rates too
+    const size_t fb = sizeof(double) * a.F;
+    if (a.po >= 0) CF_CUDA(cudaMemcpyAsync(s->d.phase_dot, s->d.sol + a.po, fb, cudaMemcpyDeviceToDevice, s->stream));
+    if (a.ao >= 0) CF_CUDA(cudaMemcpyAsync(s->d.angle_dot, s->d.sol + a.ao, fb, cudaMemcpyDeviceToDevice, s->stream));
+    CF_CUDA(cudaStreamSynchronize(s->stream));  // the host buffer may be reused on return
+    return CF_OK;
+}
+
 extern "C" int cf_sim_iteration_log(cf_sim *s, int *iters, int n) {
     clear_error();
     CF_REQUIRE(s && iters && n >= 0 && n <= kIterLogCap, "cf_sim_iteration_log: bad arguments");

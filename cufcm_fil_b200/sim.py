@@ -241,6 +241,31 @@ class WallCiliaSimulation:
         _lib.call("cf_sim_get_state", self._h, _p(ph), _p(an), _p(pd), _p(ad))
         return dict(phase=ph, angle=an, phase_dot=pd, angle_dot=ad)
 
+    def solution(self) -> np.ndarray:
+        """The saddle-point solution of the last step [system size]: constraint forces, then rates; it is the
+        next step's GMRES warm start."""
+        out = np.zeros(self.size)
+        _lib.call("cf_sim_get_solution", self._h, _p(out))
+        return out
+
+    def set_solution(self, sol):
+        """Replaces the warm start (and the filament rates, from its rate rows); synchronous."""
+        sol = np.ascontiguousarray(sol, np.float64)
+        if sol.shape != (self.size,):
+            raise ValueError(f"solution must have shape ({self.size},)")
+        _lib.call("cf_sim_set_solution", self._h, _p(sol))
+
+    def checkpoint(self) -> dict:
+        """Everything the next step depends on: filament state and the warm start."""
+        ck = self.state()
+        ck["solution"] = self.solution()
+        return ck
+
+    def restore(self, ck: dict):
+        """Puts back a checkpoint(); the following steps repeat the checkpointed trajectory exactly."""
+        self.set_solution(ck["solution"])
+        self.set_state(phase=ck["phase"], angle=ck["angle"])
+
     def segments(self):
         """(x_segs [3N], f_segs [6N]) in the reference's host layouts."""
         x = np.zeros(3 * self.n_seg_total, np.float32)

@@ -269,6 +269,12 @@ CF_API int cf_sim_stream(cf_sim *s, void **stream);
  * be NULL); the rates are also the GMRES warm start.  Asynchronous. */
 CF_API int cf_sim_set_state(cf_sim *s, const double *phase, const double *angle, const double *phase_dot,
                             const double *angle_dot);
+/* The saddle-point solution [system size]: constraint forces and rates of the
+ * last step, which seed the next step's GMRES (mobility_solver.cpp:2298-2388).
+ * Saved with cf_sim_get_state it checkpoints the whole trajectory state;
+ * cf_sim_set_solution also sets the filament rates from its rate rows. */
+CF_API int cf_sim_get_solution(cf_sim *s, double *sol);
+CF_API int cf_sim_set_solution(cf_sim *s, const double *sol);
 /* GMRES iterations of step nt are kept at index nt % 4096; copies the first n. */
 CF_API int cf_sim_iteration_log(cf_sim *s, int *iters, int n);
 /* Kernels launched by one step that ran `iters` GMRES iterations. */
