@@ -178,54 +178,79 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     pivot_invert_patch(P, p, K, rowbuf);
 }
 
-// Round K, part (b), one thread per column j of a patch (and one group of 16
-// of the 64 output rows per blockIdx.z).  The matrix is kept symmetric and only
-// its upper block triangle is maintained, so the pivot rows' entries are
-//   U[s][j] = A[k0 + s][j] for j >= k0,   A[j][k0 + s] for j < k0  (by symmetry),
-// and the pass writes
+// Round K, part (b), one 64-column tile [j0, j0 + 64) of a patch per block.
+// The matrix is kept symmetric and only its upper block triangle is
+// maintained, so the pivot rows' entries are
+//   U[s][j] = A[k0 + s][j] for j >= k0,   A[j][k0 + s] for j < k0  (by symmetry);
+// both are read as 64 contiguous floats per row of A and staged in shared
+// memory as U[s][c].  The pass writes
 //   rbuf[s][j] = (D^-1 U)[s][j] outside the pivot columns, -D^-1[s][j - k0] inside,
 //   cbuf[j][s] = U[s][j]         for j outside the pivot rows (zero inside).
-// grid = (ceil(max_n / 256), patches, 4).
+// Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
+// block's or disjoint from it.  Each thread owns 4 rows x 4 columns of
+// D^-1 U (rows ty + 16u, columns tx + 16v).  grid = (tiles, patches).
 __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
-    constexpr int G = 4, RG = kGjBlock / G;  // output-row groups (blockIdx.z) and rows per group
-    __shared__ float Dv[RG][kGjBlock + 1];
-    const int p = blockIdx.y, grp = blockIdx.z;
+    static_assert(kGjTile == kGjBlock, "column tiles are pivot-block wide");
+    __shared__ float Dv[kGjBlock][kGjBlock + 1];
+    __shared__ float Us[kGjBlock][kGjTile + 1];
+    const int p = blockIdx.y;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
-    if (k0 >= n) return;
+    const int j0 = blockIdx.x * kGjTile;
+    if (k0 >= n || j0 >= n) return;
     const int b = min(kGjBlock, n - k0);
-    const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock + grp * RG * kGjBlock;
-    for (int e = threadIdx.x; e < RG * kGjBlock; e += blockDim.x) Dv[e / kGjBlock][e % kGjBlock] = dv[e];
-    __syncthreads();
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
+    const int w = min(kGjTile, n - j0);  // columns in this tile
     const float *A = P.A + P.moff[p];
     float *rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
     float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
-    const bool in_block = j >= k0 && j < k0 + b;
-    float a[kGjBlock];
-    if (j >= k0) {
-#pragma unroll
-        for (int s = 0; s < kGjBlock; ++s) a[s] = (!in_block && s < b) ? A[static_cast<size_t>(k0 + s) * n + j] : 0.0f;
-    } else {
-#pragma unroll
-        for (int s = 0; s < kGjBlock; ++s) a[s] = (s < b) ? A[static_cast<size_t>(j) * n + k0 + s] : 0.0f;
-    }
-#pragma unroll
-    for (int rr = 0; rr < RG; ++rr) {
-        float acc = 0.0f;
-        if (in_block) {
-            acc = -Dv[rr][j - k0];
-        } else {
-#pragma unroll
-            for (int s = 0; s < kGjBlock; ++s) acc += Dv[rr][s] * a[s];
+    const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
+    if (j0 == k0) {  // the pivot columns: -D^-1, and no pivot-row copies
+        for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
+            const int r = e / kGjTile, c = e - r * kGjTile;
+            if (c < w) rb[static_cast<size_t>(r) * n + j0 + c] = -dv[r * kGjBlock + c];  // zero-padded rows
         }
-        rb[static_cast<size_t>(grp * RG + rr) * n + j] = acc;  // rows >= b hold zeros (D^-1 is zero-padded)
+        for (int e = threadIdx.x; e < w * kGjBlock; e += blockDim.x) cb[static_cast<size_t>(j0) * kGjBlock + e] = 0.0f;
+        return;
     }
-    // this group's quarter of the pivot-row entries of column j, transposed: row j of cbuf
+    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) Dv[e / kGjBlock][e % kGjBlock] = dv[e];
+    if (j0 > k0) {  // U[s][c] = A[k0 + s][j0 + c]
+        for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
+            const int s_ = e / kGjTile, c = e - s_ * kGjTile;
+            Us[s_][c] = (s_ < b && c < w) ? A[static_cast<size_t>(k0 + s_) * n + j0 + c] : 0.0f;
+        }
+    } else {  // j0 + 64 <= k0: U[s][c] = A[j0 + c][k0 + s], rows of A read contiguously
+        for (int e = threadIdx.x; e < kGjTile * kGjBlock; e += blockDim.x) {
+            const int c = e / kGjBlock, s_ = e - c * kGjBlock;
+            Us[s_][c] = (s_ < b) ? A[static_cast<size_t>(j0 + c) * n + k0 + s_] : 0.0f;
+        }
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[4][4] = {};
+#pragma unroll 8
+    for (int s_ = 0; s_ < kGjBlock; ++s_) {
+        float dr[4], uc[4];
 #pragma unroll
-    for (int s = 0; s < RG; ++s)
-        cb[static_cast<size_t>(j) * kGjBlock + grp * RG + s] = in_block ? 0.0f : a[grp * RG + s];
+        for (int u = 0; u < 4; ++u) dr[u] = Dv[ty + 16 * u][s_];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) uc[v] = Us[s_][tx + 16 * v];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(dr[u], uc[v], acc[u][v]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int c = tx + 16 * v;
+            if (c < w) rb[static_cast<size_t>(ty + 16 * u) * n + j0 + c] = acc[u][v];  // rows >= b: zeros
+        }
+    // the pivot-row entries of the tile's columns, transposed: rows j0 .. j0 + w of cbuf
+    for (int e = threadIdx.x; e < w * kGjBlock; e += blockDim.x) {
+        const int c = e / kGjBlock, s_ = e - c * kGjBlock;
+        cb[static_cast<size_t>(j0 + c) * kGjBlock + s_] = Us[s_][c];
+    }
 }
 
 // Round K, part (c), the 64x64 tiles of the upper block triangle:

@@ -78,7 +78,8 @@ struct Engine {
     bool line = false;
     PatchDev P{};
     long long patch_floats = 0;
-    int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_tiles = 1, apply_chunks = 1;
+    int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_cols = 1, gj_tiles = 1;
+    int apply_chunks = 1;
     bool refreshed_last = false;
     size_t apply_smem = 0;
     cudaGraph_t rgraph = nullptr;
@@ -246,11 +247,10 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     CF_CHECK_LAUNCH("patch_mobility_kernel");
     patch_rates_kernel<<<P.np, 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_rates_kernel");
-    const int cols = (P.max_n + 255) / 256;
     gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, 0);  // later pivot blocks: inverted inside the previous update
     CF_CHECK_LAUNCH("gj_pivot_kernel");
     for (int K = 0; K < e->gj_rounds; ++K) {
-        gj_prep_kernel<<<dim3(cols, P.np, 4), 256, 0, st>>>(P, K);
+        gj_prep_kernel<<<dim3(e->gj_cols, P.np), 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_prep_kernel");
         gj_update_kernel<<<dim3(P.np, e->gj_tiles), 256, 0, st>>>(P, K);  // patches fastest: diagonals first
         CF_CHECK_LAUNCH("gj_update_kernel");
@@ -618,6 +618,7 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     e->mob_grid = static_cast<int>((ns * ns + 255) / 256);
     e->gj_rounds = (max_n + kGjBlock - 1) / kGjBlock;
     const int T = (max_n + kGjTile - 1) / kGjTile;
+    e->gj_cols = T;
     e->gj_tiles = T * T;
     e->apply_chunks = (max_n + 63) / 64;
     e->apply_smem = sizeof(double) * std::max(max_n, 3 * d.nseg);

@@ -495,9 +495,10 @@ __global__ void rhs_kernel(SimDev d) {
     filament_rows(d, fr, d.sol, d.w, sm32);  // filament rows of A x0 for the initial residual
     const ArrayInfo &a = d.arr[fr.b];
     if (arrive_last(&d.ctl[fr.b].counter, a.F, &last)) {
+        double acc = 0.0;  // the filaments' partials, summed by the whole block in a fixed order
+        for (int q = threadIdx.x; q < a.F; q += blockDim.x) acc += __ldcg(&d.norm_partial[a.fil0 + q]);
+        acc = block_sum(acc, sm32);
         if (threadIdx.x == 0) {
-            double acc = 0.0;
-            for (int q = 0; q < a.F; ++q) acc += __ldcg(&d.norm_partial[a.fil0 + q]);
             d.ctl[fr.b].norm_rhs = sqrt(acc);
             d.ctl[fr.b].counter = 0;
         }
@@ -728,10 +729,11 @@ __global__ void residual_decide_kernel(SimDev d, cudaGraphConditionalHandle h) {
     if (threadIdx.x == 0) d.norm_partial[m] = ss;
     const ArrayInfo &a = d.arr[fr.b];
     if (!arrive_last(&d.ctl[fr.b].counter, a.F, &last)) return;
+    double acc = 0.0;  // the filaments' partials, summed by the whole block in a fixed order
+    for (int q = threadIdx.x; q < a.F; q += blockDim.x) acc += __ldcg(&d.norm_partial[a.fil0 + q]);
+    acc = block_sum(acc, sm32);
     if (threadIdx.x == 0) {
         GmresCtl *ctl = d.ctl + fr.b;
-        double acc = 0.0;
-        for (int q = 0; q < a.F; ++q) acc += __ldcg(&d.norm_partial[a.fil0 + q]);
         ctl->counter = 0;
         const double nr = ctl->norm_rhs;
         double b0 = sqrt(acc);
@@ -931,10 +933,11 @@ __global__ void __launch_bounds__(256) update_kernel(SimDev d, const double *h, 
                 const double tot = block_sum(ss, sm32);
                 if (threadIdx.x == 0) d.norm_partial[max(lo, t0)] = tot;
                 if (arrive_last(&d.ctl[cur].counter, ranges_meeting(t0, t1, per), &last)) {
+                    double acc = 0.0;  // the blocks' partials, summed by the whole block in a fixed order
+                    for (long long c = t0 / per + threadIdx.x; c <= (t1 - 1) / per; c += blockDim.x)
+                        acc += __ldcg(&d.norm_partial[max(c * per, t0)]);
+                    acc = block_sum(acc, sm32);
                     if (threadIdx.x == 0) {
-                        double acc = 0.0;
-                        for (long long c = t0 / per; c <= (t1 - 1) / per; ++c)
-                            acc += __ldcg(&d.norm_partial[max(c * per, t0)]);
                         d.ctl[cur].counter = 0;
                         qn = sqrt(acc);
                     }

@@ -114,12 +114,16 @@ def test_step_solution_satisfies_system_and_matches_oracle(s_table):
         assert abs(res.iterations - it_cpu) <= max(3, 0.2 * it_cpu)
 
 
-@pytest.mark.parametrize("spacing,steps,tip_tol", [(60.0, 300, 1e-3), (20.0, 10, 2e-3)])
+@pytest.mark.parametrize("spacing,steps,tip_tol", [(60.0, 90, 1e-3), (20.0, 10, 2e-3)])
 def test_tip_trajectories_match_oracle(s_table, spacing, steps, tip_tol):
     # 16 cilia x 20 segments; tips after `steps` implicit steps at GMRES tolerance 1e-6.
     # At spacing 20 neighbouring cilia overlap and the dynamics are chaotic: the FP64 oracle run
     # with FP32 pair sums departs from the same run in FP64 by ~4e-4 L after 10 steps and by O(L)
     # after 40, so the dense case is compared over 10 steps only.
+    # At spacing 60 the first 90 steps are well conditioned (a 1e-7 change of the initial phases
+    # moves the oracle's tips by 2.5e-6 L by step 89); between steps ~90 and ~105 the saddle
+    # system of this array is nearly singular and the same change grows to 1e-3 L (1e-2 L by
+    # step 300), so later steps are fixed by the rounding of the sums, not by the physics.
     gpu, cpu = make_pair(4, spacing, s_table, seed=5)
     L = 2.6 * 19
     with gpu:
