@@ -46,7 +46,7 @@ struct PatchDev {
     const long long *roff;   // first entry of each patch in `rows` [np]
     const long long *rows;   // batch-vector row of each local unknown
     float *A;                // patch matrices, then their inverses (row-major n x n)
-    float *cbuf;             // pivot-column copies, [np][max_n][kGjBlock]
+    float *cbuf;             // pivot-row copies U, [np][kGjBlock][max_n] (row stride n)
     float *rbuf;             // scaled pivot rows, [np][kGjBlock][max_n]
     float *dinv;             // inverted pivot blocks, [np][kGjBlock][kGjBlock]
     int *ok;                 // [np] 1 when the inverse is finite
@@ -111,71 +111,174 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
     }
 }
 
-// Part (a) of a round: inverts pivot block K of patch p (rows and columns [64K, 64K + b)) in
-// place of dinv; called by all 256 threads of a block.  Each thread keeps 16
-// entries of the 64x64 block in registers (row tid/4, columns tid%4 + 4q); per
-// elimination step the pivot row is published through a double-buffered
-// shared row (one barrier per step) and each row's pivot-column entry comes
-// from a shuffle among the row's 4 threads.  A non-finite or zero pivot clears
-// the patch's ok flag.
-// A: the patch matrix (n x n), dv: its dinv block, ok: its flag.
-__device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int *ok, int K, float (*rowbuf)[kGjBlock]) {
-    static_assert(kGjBlock * 4 == 256, "one row per 4 threads");
-    constexpr int Q = kGjBlock / 4;
-    const int k0 = K * kGjBlock;
-    const int b = min(kGjBlock, n - k0);
-    const int r = threadIdx.x >> 2, cq = threadIdx.x & 3;
+// Gauss-Jordan inversion without pivoting of a 32x32 block held by one warp,
+// lane r holding row r in a[]; returns true (in every lane) if a pivot was
+// zero or not finite.  The row is kept rotated: at step t, a[j] holds column
+// (t + j) mod 32, so the pivot column is always a[0] and every register index
+// is static while the step loop stays rolled (a small loop body, no
+// instruction-cache misses); after 32 steps the order is the original one.
+// The scaled pivot row reaches the other lanes by shuffles.
+__device__ __forceinline__ bool warp_invert32(float (&a)[32]) {
     const int lane = threadIdx.x & 31;
-    if (K == 0 && threadIdx.x == 0) *ok = 1;
-    float reg[Q];
+    bool bad = false;
+#pragma unroll 1
+    for (int t = 0; t < 32; ++t) {
+        const float f = a[0];  // this row's entry in column t
+        const float piv = __shfl_sync(0xffffffffu, f, t);
+        bad |= !(fabsf(piv) > 0.0f) || !isfinite(piv);
+        const float ip = 1.0f / piv;
+        const bool own = lane == t;
+        const float col_t = own ? ip : -f * ip;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const int c = cq + 4 * q;
-        reg[q] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : 0.0f;
-    }
-    for (int t = 0; t < b; ++t) {
-        float own = 0.0f;
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-            if (q == (t >> 2)) own = reg[q];
-        const float colr = __shfl_sync(0xffffffffu, own, (lane & ~3) | (t & 3));
-        float *rb = rowbuf[t & 1];
-        if (r == t) {  // scale the pivot row and publish it
-            const float ip = 1.0f / colr;  // colr is the pivot here
-            if (cq == (t & 3) && (!(fabsf(colr) > 0.0f) || !isfinite(colr))) *ok = 0;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int c = cq + 4 * q;
-                reg[q] = (c == t) ? ip : reg[q] * ip;
-                rb[c] = reg[q];
-            }
+        for (int j = 1; j < 32; ++j) {
+            const float pr = __shfl_sync(0xffffffffu, a[j], t) * ip;  // scaled pivot row, column (t + j) mod 32
+            a[j - 1] = own ? pr : fmaf(-f, pr, a[j]);
         }
-        __syncthreads();
-        if (r != t && r < b) {  // eliminate column t from the other rows
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int c = cq + 4 * q;
-                reg[q] = ((c == t) ? 0.0f : reg[q]) - colr * rb[c];
-            }
-        }
+        a[31] = col_t;
     }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) dv[r * kGjBlock + cq + 4 * q] = (r < b) ? reg[q] : 0.0f;
+    return bad;
 }
 
-__device__ __forceinline__ void pivot_invert_patch(const PatchDev &P, int p, int K, float (*rowbuf)[kGjBlock]) {
+// O[i][j] (+)= sign * sum_k L[i][k] R[k][j] for 32x32 blocks in shared memory
+// (leading dimensions ldl, ldr, ldo); all 256 threads, 4 entries each.
+__device__ __forceinline__ void block_gemm32(const float *L, int ldl, const float *R, int ldr, float *O, int ldo,
+                                             const float *Add, int lda, float sign) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int o = threadIdx.x + 256 * m, i = o >> 5, j = o & 31;
+        float acc = 0.0f;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) acc = fmaf(L[i * ldl + k], R[k * ldr + j], acc);
+        O[i * ldo + j] = (Add ? Add[i * lda + j] : 0.0f) + sign * acc;
+    }
+}
+
+// acc = L R for 64x64 blocks in shared memory (leading dimension kInvLd); each
+// of the 256 threads owns rows 4*(tid/16) + u and columns tid%16 + 16v.
+constexpr int kInvLd = kGjBlock + 1, kInvLq = 33;
+__device__ __forceinline__ void block_gemm64(const float *L, const float *R, float (&acc)[4][4]) {
+    const int r0 = 4 * (threadIdx.x >> 4), c0 = threadIdx.x & 15;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0f;
+#pragma unroll 8
+    for (int k = 0; k < kGjBlock; ++k) {
+        float l[4], r[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) l[u] = L[(r0 + u) * kInvLd + k];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) r[v] = R[k * kInvLd + c0 + 16 * v];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(l[u], r[v], acc[u][v]);
+    }
+}
+
+// The pivot block D (rows and columns [k0, k0 + b) of A, padded with the identity to 64 x 64) into M.
+__device__ __forceinline__ void load_pivot_block(const float *A, int n, int k0, int b, float *M) {
+    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) {
+        const int r = e >> 6, c = e & 63;
+        M[r * kInvLd + c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : (r == c ? 1.0f : 0.0f);
+    }
+}
+
+// Part (a) of a round: inverts pivot block K of patch p (rows and columns
+// [64K, 64K + b)) into its dinv block, zero-padded to 64 x 64; called by all
+// 256 threads of a block.  The 64x64 block D = [[P, B], [C, E]] (32x32
+// quarters, padded with the identity beyond b) is inverted through the Schur
+// complement S = E - C P^-1 B:
+//   D^-1 = [[P^-1 + P^-1 B S^-1 C P^-1, -P^-1 B S^-1], [-S^-1 C P^-1, S^-1]],
+// the two 32x32 inversions by one warp each (warp_invert32), the products by
+// the whole block.  Forming P^-1 explicitly loses accuracy when P is ill
+// conditioned, so the result X is refined by one Newton step,
+// X <- X + X (I - D X), which squares its residual.  A zero or non-finite
+// pivot clears the patch's ok flag.
+// A: the patch matrix (n x n), dv: its dinv block, ok: its flag, ws: shared
+// memory of at least kInvWs floats.
+constexpr int kInvWs = 2 * kGjBlock * kInvLd;
+__device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int *ok, int K, float *ws) {
+    static_assert(kGjBlock == 64, "two 32x32 quarters");
+    static_assert(2 * 32 * kInvLq <= kGjBlock * kInvLd, "X and Y fit in the second buffer");
+    const int k0 = K * kGjBlock;
+    const int b = min(kGjBlock, n - k0);
+    float *D = ws, *W = ws + kGjBlock * kInvLd;  // D: the block, then its inverse; W: scratch
+    float *X = W, *Y = W + 32 * kInvLq;
+    load_pivot_block(A, n, k0, b, D);
+    __syncthreads();
+    float *Pq = D, *Bq = D + 32, *Cq = D + 32 * kInvLd, *Eq = Cq + 32;
+    const int lane = threadIdx.x & 31;
+    __shared__ int bad;
+    if (threadIdx.x < 32) {  // P^-1 in place
+        float a[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) a[c] = Pq[lane * kInvLd + c];
+        const bool bd = warp_invert32(a);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Pq[lane * kInvLd + c] = a[c];
+        if (lane == 0) bad = bd ? 1 : 0;
+    }
+    __syncthreads();
+    block_gemm32(Pq, kInvLd, Bq, kInvLd, X, kInvLq, nullptr, 0, 1.0f);  // X = P^-1 B
+    block_gemm32(Cq, kInvLd, Pq, kInvLd, Y, kInvLq, nullptr, 0, 1.0f);  // Y = C P^-1
+    __syncthreads();
+    block_gemm32(Cq, kInvLd, X, kInvLq, Eq, kInvLd, Eq, kInvLd, -1.0f);  // S = E - C X, in place of E
+    __syncthreads();
+    if (threadIdx.x < 32) {  // S^-1 in place
+        float a[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) a[c] = Eq[lane * kInvLd + c];
+        const bool bd = warp_invert32(a);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Eq[lane * kInvLd + c] = a[c];
+        if (lane == 0 && bd) bad = 1;
+    }
+    __syncthreads();
+    block_gemm32(X, kInvLq, Eq, kInvLd, Bq, kInvLd, nullptr, 0, -1.0f);  // top right  -X S^-1, in place of B
+    block_gemm32(Eq, kInvLd, Y, kInvLq, Cq, kInvLd, nullptr, 0, -1.0f);  // bottom left -S^-1 Y, in place of C
+    __syncthreads();
+    block_gemm32(Bq, kInvLd, Y, kInvLq, Pq, kInvLd, Pq, kInvLd, -1.0f);  // top left P^-1 - (-X S^-1) Y
+    __syncthreads();
+    // Newton step: W = D again, then W = I - D X, then X + X W straight to dv
+    load_pivot_block(A, n, k0, b, W);
+    __syncthreads();
+    float acc[4][4];
+    block_gemm64(W, D, acc);
+    __syncthreads();
+    const int r0 = 4 * (threadIdx.x >> 4), c0 = threadIdx.x & 15;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) W[(r0 + u) * kInvLd + c0 + 16 * v] = (r0 + u == c0 + 16 * v ? 1.0f : 0.0f) - acc[u][v];
+    __syncthreads();
+    block_gemm64(D, W, acc);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int r = r0 + u, c = c0 + 16 * v;
+            dv[r * kGjBlock + c] = (r < b && c < b) ? D[r * kInvLd + c] + acc[u][v] : 0.0f;
+        }
+    if (threadIdx.x == 0) {
+        if (bad) *ok = 0;
+        else if (K == 0) *ok = 1;
+    }
+}
+
+__device__ __forceinline__ void pivot_invert_patch(const PatchDev &P, int p, int K, float *ws) {
     pivot_invert(P.A + P.moff[p], P.nf[p] * P.nbf, P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock, P.ok + p, K,
-                 rowbuf);
+                 ws);
 }
 
 // Round 0, part (a): the first pivot block of every patch (later pivot blocks
 // are inverted by the previous round's update, see gj_update_kernel).
 __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
-    __shared__ float rowbuf[2][kGjBlock];
+    __shared__ float ws[kInvWs];
     const int p = blockIdx.x;
     const int n = P.nf[p] * P.nbf;
     if (K * kGjBlock >= n) return;
-    pivot_invert_patch(P, p, K, rowbuf);
+    pivot_invert_patch(P, p, K, ws);
 }
 
 // Round K, part (b), one 64-column tile [j0, j0 + 64) of a patch per block.
@@ -185,8 +288,8 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
 // both are read as 64 contiguous floats per row of A and staged in shared
 // memory as U[s][c].  The pass writes
 //   rbuf[s][j] = (D^-1 U)[s][j] outside the pivot columns, -D^-1[s][j - k0] inside,
-//   cbuf[j][s] = U[s][j]         for j outside the pivot rows (zero inside).
-// Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
+//   cbuf[s][j] = U[s][j]         for j outside the pivot rows (zero inside),
+// both [64][n] with row stride n.  Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
 // block's or disjoint from it.  Each thread owns 4 rows x 4 columns of
 // D^-1 U (rows ty + 16u, columns tx + 16v).  grid = (tiles, patches).
 __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
@@ -207,9 +310,11 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     if (j0 == k0) {  // the pivot columns: -D^-1, and no pivot-row copies
         for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
             const int r = e / kGjTile, c = e - r * kGjTile;
-            if (c < w) rb[static_cast<size_t>(r) * n + j0 + c] = -dv[r * kGjBlock + c];  // zero-padded rows
+            if (c < w) {
+                rb[static_cast<size_t>(r) * n + j0 + c] = -dv[r * kGjBlock + c];  // zero-padded rows
+                cb[static_cast<size_t>(r) * n + j0 + c] = 0.0f;
+            }
         }
-        for (int e = threadIdx.x; e < w * kGjBlock; e += blockDim.x) cb[static_cast<size_t>(j0) * kGjBlock + e] = 0.0f;
         return;
     }
     for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) Dv[e / kGjBlock][e % kGjBlock] = dv[e];
@@ -246,10 +351,10 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
             const int c = tx + 16 * v;
             if (c < w) rb[static_cast<size_t>(ty + 16 * u) * n + j0 + c] = acc[u][v];  // rows >= b: zeros
         }
-    // the pivot-row entries of the tile's columns, transposed: rows j0 .. j0 + w of cbuf
-    for (int e = threadIdx.x; e < w * kGjBlock; e += blockDim.x) {
-        const int c = e / kGjBlock, s_ = e - c * kGjBlock;
-        cb[static_cast<size_t>(j0 + c) * kGjBlock + s_] = Us[s_][c];
+    // the pivot-row entries of the tile's columns
+    for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
+        const int s_ = e / kGjTile, c = e - s_ * kGjTile;
+        if (c < w) cb[static_cast<size_t>(s_) * n + j0 + c] = Us[s_][c];
     }
 }
 
@@ -257,20 +362,26 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
 //   pivot rows       A[i, j] = rbuf[i - k0][j]      (-D^-1 in the pivot block)
 //   other rows       A[i, j] -= C_i . rbuf[:, j]   (j outside the pivot columns)
 //                    A[i, j]  = -C_i . rbuf[:, j]  (pivot columns: C_i D^-1)
-// with C_i = cbuf[i][:] -- the symmetric sweep, which leaves -A^-1 after the
-// last round.  Each thread owns 4 rows x 4 columns of the tile
-// (columns interleaved by 16, so every load and store of a half-warp is one
-// contiguous run) and loads each of its rows of A in one batch.
+// with C_i = cbuf[:][i] -- the symmetric sweep, which leaves -A^-1 after the
+// last round.  Tiles and pivot blocks are both 64 wide, so a tile lies in the
+// pivot rows (ti == K, a copy), in the pivot columns (tj == K) or in neither.
+// The product: each thread owns 4 consecutive rows x 4 consecutive columns and
+// reads both operands as float4 from shared memory (row pitch 68 floats);
+// the result is staged in shared memory so that the tile's old values are
+// read and written back in coalesced rows.
 // grid = (patches, tiles): patches run fastest, so every patch's first block
 // (the diagonal tile below) is issued in the first wave.
 __global__ void __launch_bounds__(256, 4) gj_update_kernel(PatchDev P, int K) {
-    __shared__ float Cs[kGjTile][kGjBlock + 1];
-    __shared__ float Rs[kGjBlock][kGjTile + 1];
+    constexpr int LD = kGjTile + 4;
+    static_assert(kGjTile == 64 && kGjBlock == 64, "256 threads: 4x4 per thread, 4 rows per pass");
+    static_assert(2 * kGjBlock * LD >= kInvWs, "the diagonal block's inversion reuses the tiles' shared memory");
+    __shared__ __align__(16) float sm[2][kGjBlock][LD];
+    float(*Cs)[LD] = sm[0];  // Cs[s][r] = C[row0 + r][s]; later the product
+    float(*Rs)[LD] = sm[1];  // Rs[s][c] = rbuf[s][col0 + c]
     const int p = blockIdx.x;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
     if (k0 >= n) return;
-    const int b = min(kGjBlock, n - k0);
     const int T = (n + kGjTile - 1) / kGjTile;
     const int bid = blockIdx.y;
     if (bid >= T * T) return;
@@ -281,63 +392,60 @@ __global__ void __launch_bounds__(256, 4) gj_update_kernel(PatchDev P, int K) {
     if (diag >= 0) tile = (bid == 0) ? diag : (bid <= diag ? bid - 1 : bid);
     const int ti = tile / T, tj = tile - ti * T;
     if (ti > tj) return;  // the lower block triangle is filled in once, after the last round
+    const bool prow = ti == K, pcol = tj == K;
     const int row0 = ti * kGjTile, col0 = tj * kGjTile;
     float *__restrict__ A = P.A + P.moff[p];
-    const float *__restrict__ cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    const float *__restrict__ cb = P.cbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
     const float *__restrict__ rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    for (int e = threadIdx.x; e < kGjTile * kGjBlock; e += blockDim.x) {
-        const int r = e / kGjBlock, s = e - r * kGjBlock;
-        const int i = row0 + r;
-        Cs[r][s] = (i < n) ? cb[static_cast<size_t>(i) * kGjBlock + s] : 0.0f;
-    }
-    for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
-        const int s = e / kGjTile, c = e - s * kGjTile;
-        const int j = col0 + c;
-        Rs[s][c] = (j < n) ? rb[static_cast<size_t>(s) * n + j] : 0.0f;
+    // coalesced element passes: column cc, rows r0 + 4m
+    const int cc = threadIdx.x & 63, r0 = threadIdx.x >> 6;
+    const int j = col0 + cc;
+    const size_t step = 4 * static_cast<size_t>(n);  // 4 rows
+    {
+        const float *rp = rb + static_cast<size_t>(r0) * n + j, *cp = cb + static_cast<size_t>(r0) * n + row0 + cc;
+        const bool rok = j < n, cok = !prow && row0 + cc < n;
+#pragma unroll 4
+        for (int m = 0; m < 16; ++m, rp += step, cp += step) {
+            Rs[r0 + 4 * m][cc] = rok ? *rp : 0.0f;
+            if (!prow) Cs[r0 + 4 * m][cc] = cok ? *cp : 0.0f;
+        }
     }
     __syncthreads();
-    float acc[4][4];
+    // this thread's column j of the tile, rows row0 + r0 + 4m
+    float *__restrict__ Ac = A + static_cast<size_t>(row0 + r0) * n + j;
+    const int mrows = j < n ? min(16, (n - row0 - r0 + 3) / 4) : 0;  // rows i < n
+    if (prow) {  // the pivot rows: rbuf itself (row0 == k0)
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+        for (int m = 0; m < 16; ++m)
+            if (m < mrows) Ac[m * step] = Rs[r0 + 4 * m][cc];
+    } else {
+        const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+        float acc[4][4] = {};
+#pragma unroll 4
+        for (int s_ = 0; s_ < kGjBlock; ++s_) {
+            const float4 c4 = *reinterpret_cast<const float4 *>(&Cs[s_][4 * ty]);
+            const float4 r4 = *reinterpret_cast<const float4 *>(&Rs[s_][4 * tx]);
+            const float cr[4] = {c4.x, c4.y, c4.z, c4.w}, rr[4] = {r4.x, r4.y, r4.z, r4.w};
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0f;
-#pragma unroll 8
-    for (int s = 0; s < kGjBlock; ++s) {
-        float cr[4], rr[4];
+            for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) cr[u] = Cs[ty * 4 + u][s];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) rr[v] = Rs[s][v * 16 + tx];
+                for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(cr[u], rr[v], acc[u][v]);
+        }
+        __syncthreads();  // every thread is done with Cs: it now holds the product
 #pragma unroll
         for (int u = 0; u < 4; ++u)
+            *reinterpret_cast<float4 *>(&Cs[4 * ty + u][4 * tx]) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+        __syncthreads();
+        float old[16];  // all loads first, then all stores
 #pragma unroll
-            for (int v = 0; v < 4; ++v) acc[u][v] += cr[u] * rr[v];
-    }
+        for (int m = 0; m < 16; ++m) old[m] = (!pcol && m < mrows) ? Ac[m * step] : 0.0f;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int i = row0 + ty * 4 + u;
-        if (i >= n) continue;
-        const bool pivot_row = i >= k0 && i < k0 + b;
-        float *__restrict__ ar = A + static_cast<size_t>(i) * n;
-        float old[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int j = col0 + v * 16 + tx;
-            old[v] = (!pivot_row && j < n) ? ar[j] : 0.0f;
-        }
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int j = col0 + v * 16 + tx;
-            if (j >= n) continue;
-            ar[j] = pivot_row ? Rs[i - k0][v * 16 + tx]
-                              : ((j >= k0 && j < k0 + b) ? -acc[u][v] : old[v] - acc[u][v]);
-        }
+        for (int m = 0; m < 16; ++m)
+            if (m < mrows) Ac[m * step] = old[m] - Cs[r0 + 4 * m][cc];
     }
     if (tile == diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
-        __shared__ float rowbuf[2][kGjBlock];
         __syncthreads();
-        pivot_invert_patch(P, p, K + 1, rowbuf);
+        pivot_invert_patch(P, p, K + 1, &sm[0][0][0]);
     }
 }
 

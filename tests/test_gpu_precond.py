@@ -46,22 +46,26 @@ def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
+@pytest.mark.parametrize("geom", [(24, 4, 4), (32, 2, 16)])
 @pytest.mark.parametrize("dyn", [(True, True), (True, False), (False, False)])
-def test_patch_preconditioner_matches_oracle(s_table, dyn):
-    # 4 x 6 lattice: lines of 6 filaments along y cut into patches of 3
-    gpu, cpu = make(24, 4, s_table, dynamic_phase=dyn[0], dynamic_angle=dyn[1])
+def test_patch_preconditioner_matches_oracle(s_table, dyn, geom):
+    # (24, 4, 4): 4 x 6 lattice, lines of 6 filaments along y cut into patches of 3 (186 unknowns,
+    # three pivot blocks, the last one partial); (32, 2, 16): two lines of 16 filaments, one patch
+    # each (992 unknowns with both rates: 16 pivot blocks, the last 32 wide)
+    n_fil, nx, lp = geom
+    gpu, cpu = make(n_fil, nx, s_table, dynamic_phase=dyn[0], dynamic_angle=dyn[1], line_patch=lp)
     with gpu:
         gpu.initial_guess(0)
         cpu.initial_guess(0)
         v = np.random.default_rng(5).standard_normal(gpu.size)
         out = gpu.apply_preconditioner_new(v)
-        ref = cpu.line_patch_precond(v, line_patch=4)
+        ref = cpu.line_patch_precond(v, line_patch=lp)
         assert rel(out, ref) < 1e-3, rel(out, ref)
         # a patch inverse applied to its own block reproduces the input
         back = cpu.matvec(ref)
-        fils = implicit.line_patches(cpu.bases, 4)[0]
+        fils = implicit.line_patches(cpu.bases, lp)[0]
         rows = cpu.patch_rows(fils)
-        np.testing.assert_allclose(cpu.patch_block(fils) @ ref[rows], v[rows], rtol=1e-9, atol=1e-9)
+        np.testing.assert_allclose(cpu.patch_block(fils) @ ref[rows], v[rows], rtol=1e-8, atol=1e-8)
         assert np.all(np.isfinite(back))
 
 
