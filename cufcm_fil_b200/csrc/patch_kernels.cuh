@@ -39,18 +39,24 @@ struct PatchDev {
     int np;                  // patches
     int nbf;                 // unknowns per filament (3*nseg + rate rows)
     int max_n;               // largest patch system
+    int max_ld;              // patch_ld(max_n): row stride of the rbuf / cbuf slots
     const int *fil0;         // first entry of each patch in `fils` [np]
     const int *nf;           // filaments per patch [np]
     const int *fils;         // filament ids (batch numbering), patch by patch
     const long long *moff;   // first float of each patch matrix [np]
     const long long *roff;   // first entry of each patch in `rows` [np]
     const long long *rows;   // batch-vector row of each local unknown
-    float *A;                // patch matrices, then their inverses (row-major n x n)
-    float *cbuf;             // pivot-row copies U, [np][kGjBlock][max_n] (row stride n)
-    float *rbuf;             // scaled pivot rows, [np][kGjBlock][max_n]
+    float *A;                // patch matrices, then their inverses (row-major n x n, row stride patch_ld(n))
+    float *cbuf;             // pivot-row copies U, [np][kGjBlock][max_ld] (row stride patch_ld(n))
+    float *rbuf;             // scaled pivot rows, [np][kGjBlock][max_ld] (row stride patch_ld(n))
     float *dinv;             // inverted pivot blocks, [np][kGjBlock][kGjBlock]
     int *ok;                 // [np] 1 when the inverse is finite
+    int *counter;            // per-round tile counters of the update [rounds]
 };
+
+// Row stride of a patch system of n unknowns: rows start on 16 bytes, so tiles
+// move in 16-byte copies.  The padding columns [n, ld) are never part of a result.
+__host__ __device__ __forceinline__ int patch_ld(int n) { return (n + 3) & ~3; }
 
 // Mobility entries: one thread per (target segment, source segment) pair of a
 // patch; writes the 3x3 block into the lambda rows / columns.
@@ -65,7 +71,7 @@ __global__ void patch_mobility_kernel(SimDev d, PatchDev P) {
     const int aj = sj / d.nseg, kj = sj - aj * d.nseg;
     const int gi = P.fils[P.fil0[p] + ai] * d.nseg + ki;
     const int gj = P.fils[P.fil0[p] + aj] * d.nseg + kj;
-    const int n = nfp * P.nbf;
+    const int ld = patch_ld(nfp * P.nbf);
     float *A = P.A + P.moff[p];
     const long long r0 = static_cast<long long>(ai) * P.nbf + 3 * ki;
     const long long c0 = static_cast<long long>(aj) * P.nbf + 3 * kj;
@@ -81,7 +87,7 @@ __global__ void patch_mobility_kernel(SimDev d, PatchDev P) {
             const float dz = static_cast<float>(d.xd[3 * gi + 2] - d.xd[3 * gj + 2]);
             wall_pair_f32<3, 3>(dx, dy, dz, zi, static_cast<float>(d.xd[3 * gj + 2]), f, v);
         }
-        for (int q = 0; q < 3; ++q) A[(r0 + q) * n + c0 + c] = v[q];
+        for (int q = 0; q < 3; ++q) A[(r0 + q) * ld + c0 + c] = v[q];
     }
 }
 
@@ -89,7 +95,7 @@ __global__ void patch_mobility_kernel(SimDev d, PatchDev P) {
 __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
     const int p = blockIdx.x;
     const int nfp = P.nf[p];
-    const int n = nfp * P.nbf;
+    const int ld = patch_ld(nfp * P.nbf);
     const int nl = 3 * d.nseg;
     float *A = P.A + P.moff[p];
     for (int e = threadIdx.x; e < nfp * nl; e += blockDim.x) {
@@ -99,14 +105,14 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
         long long c = static_cast<long long>(a) * P.nbf + nl;
         if (d.dyn_phase) {
             const float v = -static_cast<float>(d.kp[g3]);
-            A[r * n + c] = v;
-            A[c * n + r] = v;
+            A[r * ld + c] = v;
+            A[c * ld + r] = v;
             ++c;
         }
         if (d.dyn_angle) {
             const float v = -static_cast<float>(d.ka[g3]);
-            A[r * n + c] = v;
-            A[c * n + r] = v;
+            A[r * ld + c] = v;
+            A[c * ld + r] = v;
         }
     }
 }
@@ -180,7 +186,7 @@ __device__ __forceinline__ void block_gemm64(const float *L, const float *R, flo
 __device__ __forceinline__ void load_pivot_block(const float *A, int n, int k0, int b, float *M) {
     for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) {
         const int r = e >> 6, c = e & 63;
-        M[r * kInvLd + c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * n + k0 + c] : (r == c ? 1.0f : 0.0f);
+        M[r * kInvLd + c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * patch_ld(n) + k0 + c] : (r == c ? 1.0f : 0.0f);
     }
 }
 
@@ -303,16 +309,17 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     if (k0 >= n || j0 >= n) return;
     const int b = min(kGjBlock, n - k0);
     const int w = min(kGjTile, n - j0);  // columns in this tile
+    const size_t ld = patch_ld(n);
     const float *A = P.A + P.moff[p];
-    float *rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
-    float *cb = P.cbuf + static_cast<size_t>(p) * P.max_n * kGjBlock;
+    float *rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_ld;
+    float *cb = P.cbuf + static_cast<size_t>(p) * kGjBlock * P.max_ld;
     const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
     if (j0 == k0) {  // the pivot columns: -D^-1, and no pivot-row copies
         for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
             const int r = e / kGjTile, c = e - r * kGjTile;
             if (c < w) {
-                rb[static_cast<size_t>(r) * n + j0 + c] = -dv[r * kGjBlock + c];  // zero-padded rows
-                cb[static_cast<size_t>(r) * n + j0 + c] = 0.0f;
+                rb[static_cast<size_t>(r) * ld + j0 + c] = -dv[r * kGjBlock + c];  // zero-padded rows
+                cb[static_cast<size_t>(r) * ld + j0 + c] = 0.0f;
             }
         }
         return;
@@ -321,12 +328,12 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     if (j0 > k0) {  // U[s][c] = A[k0 + s][j0 + c]
         for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
             const int s_ = e / kGjTile, c = e - s_ * kGjTile;
-            Us[s_][c] = (s_ < b && c < w) ? A[static_cast<size_t>(k0 + s_) * n + j0 + c] : 0.0f;
+            Us[s_][c] = (s_ < b && c < w) ? A[(k0 + s_) * ld + j0 + c] : 0.0f;
         }
     } else {  // j0 + 64 <= k0: U[s][c] = A[j0 + c][k0 + s], rows of A read contiguously
         for (int e = threadIdx.x; e < kGjTile * kGjBlock; e += blockDim.x) {
             const int c = e / kGjBlock, s_ = e - c * kGjBlock;
-            Us[s_][c] = (s_ < b) ? A[static_cast<size_t>(j0 + c) * n + k0 + s_] : 0.0f;
+            Us[s_][c] = (s_ < b) ? A[(j0 + c) * ld + k0 + s_] : 0.0f;
         }
     }
     __syncthreads();
@@ -349,12 +356,92 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             const int c = tx + 16 * v;
-            if (c < w) rb[static_cast<size_t>(ty + 16 * u) * n + j0 + c] = acc[u][v];  // rows >= b: zeros
+            if (c < w) rb[(ty + 16 * u) * ld + j0 + c] = acc[u][v];  // rows >= b: zeros
         }
     // the pivot-row entries of the tile's columns
     for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
         const int s_ = e / kGjTile, c = e - s_ * kGjTile;
-        if (c < w) cb[static_cast<size_t>(s_) * n + j0 + c] = Us[s_][c];
+        if (c < w) cb[s_ * ld + j0 + c] = Us[s_][c];
+    }
+}
+
+// 16-byte asynchronous copy global -> shared (zero-filled when !valid; src is
+// then not read but must still be a mapped address).  Both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(float *dst, const float *src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// One tile of round K's update: which tile of which patch, and its kind.
+struct GjTile {
+    int p, n, row0, col0;
+    bool valid, prow, pcol, diag;
+};
+
+// Work item -> tile.  Items run patch-fastest over a triangle enumeration of
+// the upper block triangle (T = the largest patch's tiles per side) in which
+// index 0 is the next round's diagonal tile (K + 1, K + 1), so the first np
+// items are the patches' diagonal tiles and are taken first.
+__device__ __forceinline__ GjTile gj_tile(const PatchDev &P, int K, int T, int item) {
+    GjTile t{};
+    t.p = item % P.np;
+    int q = item / P.np;
+    t.n = P.nf[t.p] * P.nbf;
+    const int Tp = (t.n + kGjTile - 1) / kGjTile;
+    const int d = K + 1;
+    if (d < T) {
+        const int qd = d * T - d * (d - 1) / 2;  // triangle index of (d, d)
+        q = (q == 0) ? qd : (q <= qd ? q - 1 : q);
+    }
+    int ti = 0;
+    while (ti < T && q >= T - ti) {
+        q -= T - ti;
+        ++ti;
+    }
+    const int tj = ti + q;
+    t.valid = K * kGjBlock < t.n && ti < Tp && tj < Tp;
+    t.row0 = ti * kGjTile;
+    t.col0 = tj * kGjTile;
+    t.prow = ti == K;
+    t.pcol = tj == K;
+    t.diag = ti == d && tj == d;
+    return t;
+}
+
+// Stage of the update pipeline: the tile's C (Cs[s][r] = cbuf[s][row0 + r]),
+// R (Rs[s][c] = rbuf[s][col0 + c]) and old values (Ao[r][c]), rows of 68
+// floats (16-byte aligned, and rows 4 apart fall on different banks).
+constexpr int kUpLd = kGjTile + 4;
+constexpr int kUpStage = 3 * kGjBlock * kUpLd;
+constexpr size_t kUpdateSmem = 2 * kUpStage * sizeof(float);
+
+// Issues the 16-byte copies of a tile into `stage`: 16 chunks of 4 floats per
+// row; chunks at or beyond the row stride are zero-filled (within it, the
+// padding columns hold values that only reach padding outputs).
+__device__ __forceinline__ void gj_issue_tile(const PatchDev &P, const GjTile &t, float *stage) {
+    float *Cs = stage, *Rs = stage + kGjBlock * kUpLd, *Ao = stage + 2 * kGjBlock * kUpLd;
+    const float *A = P.A + P.moff[t.p];
+    const float *cb = P.cbuf + static_cast<size_t>(t.p) * kGjBlock * P.max_ld;
+    const float *rb = P.rbuf + static_cast<size_t>(t.p) * kGjBlock * P.max_ld;
+    const int n = t.n, ld = patch_ld(n);
+    const int ch = threadIdx.x & 15, r0 = threadIdx.x >> 4;  // chunk of a row, first row (rows r0 + 16m)
+    const int j = t.col0 + 4 * ch, ir = t.row0 + 4 * ch;
+    const bool jok = j < ld, iok = ir < ld;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int s_ = r0 + 16 * m;
+        cp_async16(&Rs[s_ * kUpLd + 4 * ch], jok ? rb + s_ * ld + j : rb, jok);
+        if (!t.prow) cp_async16(&Cs[s_ * kUpLd + 4 * ch], iok ? cb + s_ * ld + ir : cb, iok);
+        if (!t.prow && !t.pcol) {
+            const int i = t.row0 + s_;
+            const bool ok = i < n && jok;
+            cp_async16(&Ao[s_ * kUpLd + 4 * ch], ok ? A + static_cast<size_t>(i) * ld + j : A, ok);
+        }
     }
 }
 
@@ -365,88 +452,102 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
 // with C_i = cbuf[:][i] -- the symmetric sweep, which leaves -A^-1 after the
 // last round.  Tiles and pivot blocks are both 64 wide, so a tile lies in the
 // pivot rows (ti == K, a copy), in the pivot columns (tj == K) or in neither.
-// The product: each thread owns 4 consecutive rows x 4 consecutive columns and
-// reads both operands as float4 from shared memory (row pitch 68 floats);
-// the result is staged in shared memory so that the tile's old values are
-// read and written back in coalesced rows.
-// grid = (patches, tiles): patches run fastest, so every patch's first block
-// (the diagonal tile below) is issued in the first wave.
-__global__ void __launch_bounds__(256, 4) gj_update_kernel(PatchDev P, int K) {
-    constexpr int LD = kGjTile + 4;
-    static_assert(kGjTile == 64 && kGjBlock == 64, "256 threads: 4x4 per thread, 4 rows per pass");
-    static_assert(2 * kGjBlock * LD >= kInvWs, "the diagonal block's inversion reuses the tiles' shared memory");
-    __shared__ __align__(16) float sm[2][kGjBlock][LD];
-    float(*Cs)[LD] = sm[0];  // Cs[s][r] = C[row0 + r][s]; later the product
-    float(*Rs)[LD] = sm[1];  // Rs[s][c] = rbuf[s][col0 + c]
-    const int p = blockIdx.x;
-    const int n = P.nf[p] * P.nbf;
-    const int k0 = K * kGjBlock;
-    if (k0 >= n) return;
-    const int T = (n + kGjTile - 1) / kGjTile;
-    const int bid = blockIdx.y;
-    if (bid >= T * T) return;
-    // Block 0 takes the next round's diagonal tile, so that it starts first and, after its update,
-    // inverts that pivot block for the next round while the other blocks finish theirs.
-    const int diag = (K + 1 < T) ? (K + 1) * T + (K + 1) : -1;
-    int tile = bid;
-    if (diag >= 0) tile = (bid == 0) ? diag : (bid <= diag ? bid - 1 : bid);
-    const int ti = tile / T, tj = tile - ti * T;
-    if (ti > tj) return;  // the lower block triangle is filled in once, after the last round
-    const bool prow = ti == K, pcol = tj == K;
-    const int row0 = ti * kGjTile, col0 = tj * kGjTile;
-    float *__restrict__ A = P.A + P.moff[p];
-    const float *__restrict__ cb = P.cbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
-    const float *__restrict__ rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_n;
-    // coalesced element passes: column cc, rows r0 + 4m
-    const int cc = threadIdx.x & 63, r0 = threadIdx.x >> 6;
-    const int j = col0 + cc;
-    const size_t step = 4 * static_cast<size_t>(n);  // 4 rows
-    {
-        const float *rp = rb + static_cast<size_t>(r0) * n + j, *cp = cb + static_cast<size_t>(r0) * n + row0 + cc;
-        const bool rok = j < n, cok = !prow && row0 + cc < n;
-#pragma unroll 4
-        for (int m = 0; m < 16; ++m, rp += step, cp += step) {
-            Rs[r0 + 4 * m][cc] = rok ? *rp : 0.0f;
-            if (!prow) Cs[r0 + 4 * m][cc] = cok ? *cp : 0.0f;
-        }
-    }
+// Persistent blocks take tiles from a per-round counter and copy the next
+// tile's operands and old values into the other shared-memory stage
+// (cp.async) while they update the current one.  Each thread owns rows
+// 4ty + u and columns 4tx + v (one float4 of each operand per step, float4
+// stores).  The block that takes a patch's diagonal tile (K + 1, K + 1)
+// inverts it for the next round right after its update, while the other
+// blocks go on with the rest.  Dynamic shared memory: kUpdateSmem bytes.
+__global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, int T, int *counter) {
+    static_assert(kGjTile == 64 && kGjBlock == 64, "256 threads: 4x4 per thread");
+    static_assert(kUpStage >= kInvWs, "the inversion reuses a stage");
+    extern __shared__ __align__(16) float usm[];
+    __shared__ int next_item;
+    const int total = P.np * (T * (T + 1) / 2);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
     __syncthreads();
-    // this thread's column j of the tile, rows row0 + r0 + 4m
-    float *__restrict__ Ac = A + static_cast<size_t>(row0 + r0) * n + j;
-    const int mrows = j < n ? min(16, (n - row0 - r0 + 3) / 4) : 0;  // rows i < n
-    if (prow) {  // the pivot rows: rbuf itself (row0 == k0)
-#pragma unroll
-        for (int m = 0; m < 16; ++m)
-            if (m < mrows) Ac[m * step] = Rs[r0 + 4 * m][cc];
-    } else {
-        const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-        float acc[4][4] = {};
-#pragma unroll 4
-        for (int s_ = 0; s_ < kGjBlock; ++s_) {
-            const float4 c4 = *reinterpret_cast<const float4 *>(&Cs[s_][4 * ty]);
-            const float4 r4 = *reinterpret_cast<const float4 *>(&Rs[s_][4 * tx]);
-            const float cr[4] = {c4.x, c4.y, c4.z, c4.w}, rr[4] = {r4.x, r4.y, r4.z, r4.w};
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(cr[u], rr[v], acc[u][v]);
+    const int first = next_item;
+    if (first >= total) return;
+    GjTile cur = gj_tile(P, K, T, first);
+    int stage = 0;
+    if (cur.valid) gj_issue_tile(P, cur, usm);
+    cp_async_commit();
+    while (true) {
+        __syncthreads();  // every thread has read next_item and finished with the other stage
+        if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int nitem = next_item;
+        GjTile nxt{};
+        nxt.valid = false;
+        if (nitem < total) {
+            nxt = gj_tile(P, K, T, nitem);
+            if (nxt.valid) gj_issue_tile(P, nxt, usm + (stage ^ 1) * kUpStage);
         }
-        __syncthreads();  // every thread is done with Cs: it now holds the product
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-            *reinterpret_cast<float4 *>(&Cs[4 * ty + u][4 * tx]) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+        cp_async_commit();
+        cp_async_wait<1>();  // the current stage has landed
         __syncthreads();
-        float old[16];  // all loads first, then all stores
+        if (cur.valid) {
+            float *st = usm + stage * kUpStage;
+            const float *Cs = st, *Rs = st + kGjBlock * kUpLd, *Ao = st + 2 * kGjBlock * kUpLd;
+            const int n = cur.n, ld = patch_ld(n);
+            const int j = cur.col0 + 4 * tx;
+            float *Ar = P.A + P.moff[cur.p] + static_cast<size_t>(cur.row0 + 4 * ty) * ld + j;
+            float4 res[4];
+            if (cur.prow) {  // the pivot rows: rbuf itself (row0 == k0)
 #pragma unroll
-        for (int m = 0; m < 16; ++m) old[m] = (!pcol && m < mrows) ? Ac[m * step] : 0.0f;
+                for (int u = 0; u < 4; ++u) res[u] = *reinterpret_cast<const float4 *>(&Rs[(4 * ty + u) * kUpLd + 4 * tx]);
+            } else {
+                float acc[4][4] = {};
+#pragma unroll 8
+                for (int s_ = 0; s_ < kGjBlock; ++s_) {
+                    const float4 c4 = *reinterpret_cast<const float4 *>(&Cs[s_ * kUpLd + 4 * ty]);
+                    const float4 r4 = *reinterpret_cast<const float4 *>(&Rs[s_ * kUpLd + 4 * tx]);
+                    const float cr[4] = {c4.x, c4.y, c4.z, c4.w}, rr[4] = {r4.x, r4.y, r4.z, r4.w};
 #pragma unroll
-        for (int m = 0; m < 16; ++m)
-            if (m < mrows) Ac[m * step] = old[m] - Cs[r0 + 4 * m][cc];
+                    for (int u = 0; u < 4; ++u)
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(cr[u], rr[v], acc[u][v]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    if (!cur.pcol) o = *reinterpret_cast<const float4 *>(&Ao[(4 * ty + u) * kUpLd + 4 * tx]);
+                    res[u] = make_float4(o.x - acc[u][0], o.y - acc[u][1], o.z - acc[u][2], o.w - acc[u][3]);
+                }
+            }
+            // the patch's last round writes its final values: a non-finite one marks the inverse unusable
+            const bool last = (K + 1) * kGjBlock >= n;
+            bool bad = false;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = cur.row0 + 4 * ty + u;
+                if (i >= n || j >= n) continue;
+                if (last) {
+                    bad |= !isfinite(res[u].x) || (j + 1 < n && !isfinite(res[u].y)) ||
+                           (j + 2 < n && !isfinite(res[u].z)) || (j + 3 < n && !isfinite(res[u].w));
+                }
+                float *dst = Ar + static_cast<size_t>(u) * ld;
+                if (j + 3 < n) {
+                    *reinterpret_cast<float4 *>(dst) = res[u];
+                } else {  // the row's last, partial chunk: nothing beyond column n - 1
+                    dst[0] = res[u].x;
+                    if (j + 1 < n) dst[1] = res[u].y;
+                    if (j + 2 < n) dst[2] = res[u].z;
+                }
+            }
+            if (bad) P.ok[cur.p] = 0;
+            if (cur.diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
+                __syncthreads();
+                pivot_invert_patch(P, cur.p, K + 1, st);
+            }
+        }
+        if (nitem >= total) break;
+        cur = nxt;
+        stage ^= 1;
     }
-    if (tile == diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
-        __syncthreads();
-        pivot_invert_patch(P, p, K + 1, &sm[0][0][0]);
-    }
+    cp_async_wait<0>();
 }
 
 // After the last round: fills the lower block triangle from the upper one
@@ -464,26 +565,13 @@ __global__ void __launch_bounds__(256) gj_mirror_kernel(PatchDev P) {
     const int r0 = tj * kGjTile, c0 = ti * kGjTile;  // the source tile, upper triangle
     for (int e = threadIdx.x; e < kGjTile * kGjTile; e += blockDim.x) {
         const int r = e / kGjTile, c = e - r * kGjTile;
-        tile[r][c] = (r0 + r < n && c0 + c < n) ? A[static_cast<size_t>(r0 + r) * n + c0 + c] : 0.0f;
+        tile[r][c] = (r0 + r < n && c0 + c < n) ? A[static_cast<size_t>(r0 + r) * patch_ld(n) + c0 + c] : 0.0f;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < kGjTile * kGjTile; e += blockDim.x) {
         const int r = e / kGjTile, c = e - r * kGjTile;  // destination (c0 + r, r0 + c)
-        if (c0 + r < n && r0 + c < n) A[static_cast<size_t>(c0 + r) * n + r0 + c] = tile[c][r];
+        if (c0 + r < n && r0 + c < n) A[static_cast<size_t>(c0 + r) * patch_ld(n) + r0 + c] = tile[c][r];
     }
-}
-
-// Clears a patch's ok flag if its inverse holds a non-finite entry.
-__global__ void patch_check_kernel(PatchDev P) {
-    const int p = blockIdx.y;
-    const int n = P.nf[p] * P.nbf;
-    const long long nn = static_cast<long long>(n) * n;
-    const float *A = P.A + P.moff[p];
-    bool bad = false;
-    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < nn;
-         e += static_cast<long long>(gridDim.x) * blockDim.x)
-        bad |= !isfinite(A[e]);
-    if (__syncthreads_or(bad) && threadIdx.x == 0) P.ok[p] = 0;
 }
 
 // out = blockdiag(A_pp^-1) in over the patches (in and out must differ).
@@ -491,11 +579,11 @@ __global__ void patch_check_kernel(PatchDev P) {
 // `in` into shared memory, each warp forms 8 output rows with the lanes
 // striding the (coalesced) matrix row.  A patch without a finite inverse uses
 // the block-diagonal preconditioner instead (first row chunk only).
-// Dynamic shared memory: max(max_n, 3*nseg) doubles.
+// Dynamic shared memory: max(patch_ld(max_n), 3*nseg) doubles.
 // With `masked`, patches of arrays whose GMRES stopped are skipped.
 __global__ void __launch_bounds__(256) patch_apply_kernel(SimDev d, PatchDev P, const double *in, double *out,
                                                           int masked) {
-    extern __shared__ double xs[];
+    extern __shared__ __align__(16) double xs[];
     __shared__ double sm32[32];
     const int p = blockIdx.y;
     const int n = P.nf[p] * P.nbf;
@@ -512,18 +600,38 @@ __global__ void __launch_bounds__(256) patch_apply_kernel(SimDev d, PatchDev P, 
         return;
     }
     const long long *rows = P.rows + P.roff[p];
-    for (int c = threadIdx.x; c < n; c += blockDim.x) xs[c] = in[rows[c]];
+    const int ld = patch_ld(n), n4 = ld >> 2;
+    for (int c = threadIdx.x; c < ld; c += blockDim.x) xs[c] = c < n ? in[rows[c]] : 0.0;  // padding: zeros
     __syncthreads();
     const float *A = P.A + P.moff[p];
+    const double2 *x2 = reinterpret_cast<const double2 *>(xs);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int rr = 0; rr < 8; ++rr) {
+    for (int rr = 0; rr < 8; rr += 2) {  // two rows at a time, 16-byte loads of the (padded) matrix rows
         const int r = r0 + warp * 8 + rr;
         if (r >= n) break;
-        const float *ar = A + static_cast<size_t>(r) * n;
-        double acc = 0.0;
-        for (int c = lane; c < n; c += 32) acc += static_cast<double>(__ldg(ar + c)) * xs[c];
-        acc = warp_sum(acc);
-        if (lane == 0) out[rows[r]] = -acc;  // the refresh leaves -A_pp^-1
+        const bool two = r + 1 < n;
+        const float4 *a0 = reinterpret_cast<const float4 *>(A + static_cast<size_t>(r) * ld);
+        const float4 *a1 = a0 + n4;
+        double s0 = 0.0, s1 = 0.0;
+        for (int c4 = lane; c4 < n4; c4 += 32) {
+            const float4 v0 = __ldg(a0 + c4);
+            const float4 v1 = two ? __ldg(a1 + c4) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const double2 xa = x2[2 * c4], xb = x2[2 * c4 + 1];
+            s0 = fma(static_cast<double>(v0.x), xa.x, s0);
+            s0 = fma(static_cast<double>(v0.y), xa.y, s0);
+            s0 = fma(static_cast<double>(v0.z), xb.x, s0);
+            s0 = fma(static_cast<double>(v0.w), xb.y, s0);
+            s1 = fma(static_cast<double>(v1.x), xa.x, s1);
+            s1 = fma(static_cast<double>(v1.y), xa.y, s1);
+            s1 = fma(static_cast<double>(v1.z), xb.x, s1);
+            s1 = fma(static_cast<double>(v1.w), xb.y, s1);
+        }
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+        if (lane == 0) {  // the refresh leaves -A_pp^-1
+            out[rows[r]] = -s0;
+            if (two) out[rows[r + 1]] = -s1;
+        }
     }
 }
 

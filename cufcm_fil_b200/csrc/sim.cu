@@ -79,7 +79,7 @@ struct Engine {
     PatchDev P{};
     long long patch_floats = 0;
     int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_cols = 1, gj_tiles = 1;
-    int apply_chunks = 1;
+    int apply_chunks = 1, gj_update_grid = 1;
     bool refreshed_last = false;
     size_t apply_smem = 0;
     cudaGraph_t rgraph = nullptr;
@@ -243,6 +243,7 @@ int launch_combine(Engine *e, cudaStream_t st) {
 int launch_refresh(Engine *e, cudaStream_t st) {
     const PatchDev &P = e->P;
     CF_CUDA(cudaMemsetAsync(P.A, 0, sizeof(float) * e->patch_floats, st));
+    CF_CUDA(cudaMemsetAsync(P.counter, 0, sizeof(int) * e->gj_rounds, st));
     patch_mobility_kernel<<<dim3(e->mob_grid, P.np), 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_mobility_kernel");
     patch_rates_kernel<<<P.np, 256, 0, st>>>(e->d, P);
@@ -252,17 +253,15 @@ int launch_refresh(Engine *e, cudaStream_t st) {
     for (int K = 0; K < e->gj_rounds; ++K) {
         gj_prep_kernel<<<dim3(e->gj_cols, P.np), 256, 0, st>>>(P, K);
         CF_CHECK_LAUNCH("gj_prep_kernel");
-        gj_update_kernel<<<dim3(P.np, e->gj_tiles), 256, 0, st>>>(P, K);  // patches fastest: diagonals first
+        gj_update_kernel<<<e->gj_update_grid, 256, kUpdateSmem, st>>>(P, K, e->gj_cols, P.counter + K);
         CF_CHECK_LAUNCH("gj_update_kernel");
     }
     gj_mirror_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P);
     CF_CHECK_LAUNCH("gj_mirror_kernel");
-    patch_check_kernel<<<dim3(32, P.np), 256, 0, st>>>(P);
-    CF_CHECK_LAUNCH("patch_check_kernel");
     return CF_OK;
 }
 
-int refresh_launches(const Engine *e) { return e->line ? 5 + 2 * e->gj_rounds : 0; }
+int refresh_launches(const Engine *e) { return e->line ? 4 + 2 * e->gj_rounds : 0; }
 
 int launch_patch_apply(Engine *e, const double *in, double *out, int masked, cudaStream_t st) {
     patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), 256, e->apply_smem, st>>>(e->d, e->P, in, out, masked);
@@ -581,7 +580,7 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
                 const int n = sz * nbf;
                 moff.push_back(mo);
                 roff.push_back(ro);
-                mo += static_cast<long long>(n) * n;
+                mo += static_cast<long long>(patch_ld(n)) * patch_ld(n);
                 ro += n;
                 max_n = std::max(max_n, n);
                 max_nf = std::max(max_nf, sz);
@@ -609,10 +608,15 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     CF_TRY(eng_upload(e, const_cast<long long **>(&P.roff), roff.data(), roff.size()));
     CF_TRY(eng_upload(e, const_cast<long long **>(&P.rows), rows.data(), rows.size()));
     CF_TRY(eng_alloc(e, &P.A, static_cast<size_t>(mo)));
-    CF_TRY(eng_alloc(e, &P.cbuf, static_cast<size_t>(P.np) * max_n * kGjBlock));
-    CF_TRY(eng_alloc(e, &P.rbuf, static_cast<size_t>(P.np) * max_n * kGjBlock));
+    P.max_ld = patch_ld(max_n);
+    CF_TRY(eng_alloc(e, &P.cbuf, static_cast<size_t>(P.np) * P.max_ld * kGjBlock));
+    CF_TRY(eng_alloc(e, &P.rbuf, static_cast<size_t>(P.np) * P.max_ld * kGjBlock));
+    // padding columns are read by whole 16-byte chunks: keep them finite
+    CF_CUDA(cudaMemset(P.cbuf, 0, sizeof(float) * P.np * P.max_ld * kGjBlock));
+    CF_CUDA(cudaMemset(P.rbuf, 0, sizeof(float) * P.np * P.max_ld * kGjBlock));
     CF_TRY(eng_alloc(e, &P.dinv, static_cast<size_t>(P.np) * kGjBlock * kGjBlock));
     CF_TRY(eng_alloc(e, &P.ok, P.np));
+    CF_TRY(eng_alloc(e, &P.counter, std::max(1, (max_n + kGjBlock - 1) / kGjBlock)));
     e->patch_floats = mo;
     const long long ns = static_cast<long long>(max_nf) * d.nseg;
     e->mob_grid = static_cast<int>((ns * ns + 255) / 256);
@@ -620,8 +624,11 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     const int T = (max_n + kGjTile - 1) / kGjTile;
     e->gj_cols = T;
     e->gj_tiles = T * T;
+    e->gj_update_grid = static_cast<int>(std::min<long long>(1LL * P.np * (T * (T + 1) / 2), 2LL * e->num_sms));
+    CF_CUDA(cudaFuncSetAttribute(gj_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kUpdateSmem)));
     e->apply_chunks = (max_n + 63) / 64;
-    e->apply_smem = sizeof(double) * std::max(max_n, 3 * d.nseg);
+    e->apply_smem = sizeof(double) * std::max(patch_ld(max_n), 3 * d.nseg);
     e->refresh_every = cfgs[0].precond_refresh > 0 ? cfgs[0].precond_refresh : 1;
     return CF_OK;
 }
