@@ -121,13 +121,13 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
 // lane r holding row r in a[]; returns true (in every lane) if a pivot was
 // zero or not finite.  The row is kept rotated: at step t, a[j] holds column
 // (t + j) mod 32, so the pivot column is always a[0] and every register index
-// is static while the step loop stays rolled (a small loop body, no
+// is static while the step loop stays short (unrolled 4 deep: no
 // instruction-cache misses); after 32 steps the order is the original one.
 // The scaled pivot row reaches the other lanes by shuffles.
 __device__ __forceinline__ bool warp_invert32(float (&a)[32]) {
     const int lane = threadIdx.x & 31;
     bool bad = false;
-#pragma unroll 1
+#pragma unroll 4
     for (int t = 0; t < 32; ++t) {
         const float f = a[0];  // this row's entry in column t
         const float piv = __shfl_sync(0xffffffffu, f, t);

@@ -867,7 +867,13 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
         CF_CUDA(cudaFuncSetAttribute(kinematics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(e->kin_smem)));
     if (e->line) CF_TRY(build_patches(e, cfgs));
-    CF_TRY(apply_tuning(e, Tuning{}));
+    // default dot-product chunk: about 16 chunks of the largest array, so that the (k + 1) x chunks
+    // items of the first iterations already cover the SMs (1024..4096 rows)
+    Tuning t0;
+    long long nmax = 1;
+    for (const ArrayInfo &a : e->arr) nmax = std::max<long long>(nmax, a.n);
+    t0.dots_chunk = static_cast<int>(std::min<long long>(4096, std::max<long long>(kMinDotsChunk, (nmax / 16 + 255) / 256 * 256)));
+    CF_TRY(apply_tuning(e, t0));
     const char *ng = std::getenv("CUFIL_NO_GRAPH");
     e->use_graph = !(ng && ng[0] == '1');
     return CF_OK;
