@@ -52,6 +52,9 @@ SPACING = 20.0
 GMRES_TOL = 1e-6
 F_PAIR = 154       # algorithmic flops of one 3x3 wall RPY pair (cuda_functions.cu:63-150)
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal SIMT FP32 peak at max SM clock
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture each):
+PAIR_KERNEL_DRAM_BYTES = 182_500            # rpy_wall_sym_batch_kernel, 5120 segments (profiles/rpy_wall_sym_batch_16x16_step.md)
+REFRESH_UPDATE_DRAM_BYTES = 37_500_000      # gj_update_kernel, 16 patches of 992 (profiles/gj_update_16x16_patches.md)
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -434,17 +437,20 @@ def run_ours(args):
         refresh_share = refresh_ms / step_ms
         pair_share = float(np.mean(iters) + 1) * apply_us * 1e-3 / step_ms
         roof_refresh = {"bound": "fp32", "achieved": refresh_tflops, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
-                        "frac": refresh_tflops / FP32_PEAK_TFLOPS, "traffic": None, "kernel": "patch refresh",
+                        "frac": refresh_tflops / FP32_PEAK_TFLOPS, "traffic": REFRESH_UPDATE_DRAM_BYTES,
+                        "kernel": "patch refresh",
                         "share_of_step": refresh_share,
                         "note": f"assembly + blocked Gauss-Jordan of {info['patches']} patch blocks of "
                                 f"{info['max_n']} unknowns, 2 n^3 flop each per rebuild, CUDA events around one "
                                 "rebuild; peak is the nominal FP32 SIMT rate (148 SMs x 128 lanes x 2 x 1.965 GHz), "
-                                "no FP32 peak is in the measured peaks"}
+                                "no FP32 peak is in the measured peaks; traffic: one gj_update launch (the refresh's "
+                                "top kernel; 16 per rebuild), ncu"}
         roof_pairs = {"bound": "fp32", "achieved": pair_tflops, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
-                      "frac": pair_tflops / FP32_PEAK_TFLOPS, "traffic": None, "kernel": "pair mobility product",
+                      "frac": pair_tflops / FP32_PEAK_TFLOPS, "traffic": PAIR_KERNEL_DRAM_BYTES,
+                      "kernel": "pair mobility product",
                       "share_of_step": pair_share,
                       "note": f"{F_PAIR} flop/pair x {N}^2 pairs per launch (tile kernel + reduce), CUDA events; "
-                              "nominal FP32 SIMT peak"}
+                              "nominal FP32 SIMT peak; traffic: the tile kernel's DRAM bytes per launch, ncu"}
         dominant, other = (roof_refresh, roof_pairs) if refresh_share >= pair_share else (roof_pairs, roof_refresh)
         line = {
             "metric": "timesteps/s, learned-precond vs plain GMRES at tol 1e-6; RPY pairs/s", "value": value,
@@ -462,8 +468,9 @@ def run_ours(args):
             "patch_refresh_ms": refresh_ms, "tuning": tuning,
             "roofline": dominant, "roofline_other": other,
             "traffic_note": "ncu (profiles/gj_update_16x16_patches.md): one gj_update launch, the refresh's top "
-                            "kernel, moves 77.4 MB of DRAM (the 63 MB of patch matrices stay L2-resident between "
-                            "rounds); the pair kernel 0.18 MB (profiles/rpy_wall_sym_batch_16x16_step.md)",
+                            "kernel, reads 37.4 MB of DRAM under ncu's cold cache (one read of the upper block "
+                            "triangle; the 63 MB of patch matrices stay L2-resident between rounds); the pair kernel "
+                            "0.18 MB (profiles/rpy_wall_sym_batch_16x16_step.md): both are compute-bound",
             "e2e": {"value": e2e_value, "unit": "timesteps/s", "h2d_bytes_per_step": 4 * F * 8,
                     "d2h_bytes_per_step": 4 * F * 8 + 3 * N * 4 + 6 * N * 4 + 40, "gmres_iters_per_step": e2e_iters,
                     "call": "WallCiliaSimulation.step_io (cf_sim_step_io): state up, step, state + positions + "
