@@ -117,30 +117,38 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
     }
 }
 
-// Gauss-Jordan inversion without pivoting of a 32x32 block held by one warp,
-// lane r holding row r in a[]; returns true (in every lane) if a pivot was
-// zero or not finite.  The row is kept rotated: at step t, a[j] holds column
-// (t + j) mod 32, so the pivot column is always a[0] and every register index
-// is static while the step loop stays short (unrolled 4 deep: no
-// instruction-cache misses); after 32 steps the order is the original one.
-// The scaled pivot row reaches the other lanes by shuffles.
-__device__ __forceinline__ bool warp_invert32(float (&a)[32]) {
-    const int lane = threadIdx.x & 31;
+// Gauss-Jordan inversion without pivoting of a 32x32 block by warps 0-3 of the
+// block: the thread (warp w, lane r) holds columns 8w .. 8w+7 of row r in v[].
+// Per step the warp that owns the pivot column publishes it in shared memory
+// (double-buffered, so one 128-thread named barrier per step); each warp
+// takes the pivot row's entries of its own columns from lane t by shuffles.
+// colbuf: 2 x 32 floats of shared memory.  Returns true if a pivot was zero or
+// not finite.  Warps 4-7 must not call it.
+__device__ __forceinline__ bool quad_invert32(float (&v)[8], float (*colbuf)[32]) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     bool bad = false;
-#pragma unroll 4
+#pragma unroll 2
     for (int t = 0; t < 32; ++t) {
-        const float f = a[0];  // this row's entry in column t
-        const float piv = __shfl_sync(0xffffffffu, f, t);
+        const int ow = t >> 3, oc = t & 7;  // owner warp and column slot of pivot column t
+        float *cb = colbuf[t & 1];
+        if (w == ow) {
+            float x = v[0];
+#pragma unroll
+            for (int c = 1; c < 8; ++c)
+                if (c == oc) x = v[c];
+            cb[lane] = x;
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        const float f = cb[lane], piv = cb[t];  // this row's entry in column t; the pivot
         bad |= !(fabsf(piv) > 0.0f) || !isfinite(piv);
         const float ip = 1.0f / piv;
         const bool own = lane == t;
-        const float col_t = own ? ip : -f * ip;
 #pragma unroll
-        for (int j = 1; j < 32; ++j) {
-            const float pr = __shfl_sync(0xffffffffu, a[j], t) * ip;  // scaled pivot row, column (t + j) mod 32
-            a[j - 1] = own ? pr : fmaf(-f, pr, a[j]);
+        for (int c = 0; c < 8; ++c) {
+            const float pr = __shfl_sync(0xffffffffu, v[c], t) * ip;  // scaled pivot row, this column
+            const bool pc = w == ow && c == oc;                        // this column is the pivot column
+            v[c] = pc ? (own ? ip : -f * ip) : (own ? pr : fmaf(-f, pr, v[c]));
         }
-        a[31] = col_t;
     }
     return bad;
 }
@@ -161,7 +169,7 @@ __device__ __forceinline__ void block_gemm32(const float *L, int ldl, const floa
 
 // acc = L R for 64x64 blocks in shared memory (leading dimension kInvLd); each
 // of the 256 threads owns rows 4*(tid/16) + u and columns tid%16 + 16v.
-constexpr int kInvLd = kGjBlock + 1, kInvLq = 33;
+constexpr int kInvLd = kGjBlock + 1;
 __device__ __forceinline__ void block_gemm64(const float *L, const float *R, float (&acc)[4][4]) {
     const int r0 = 4 * (threadIdx.x >> 4), c0 = threadIdx.x & 15;
 #pragma unroll
@@ -196,17 +204,20 @@ __device__ __forceinline__ void load_pivot_block(const float *A, int n, int k0, 
 // quarters, padded with the identity beyond b) is inverted through the Schur
 // complement S = E - C P^-1 B:
 //   D^-1 = [[P^-1 + P^-1 B S^-1 C P^-1, -P^-1 B S^-1], [-S^-1 C P^-1, S^-1]],
-// the two 32x32 inversions by one warp each (warp_invert32), the products by
+// the two 32x32 inversions by four warps each (quad_invert32), the products by
 // the whole block.  Forming P^-1 explicitly loses accuracy when P is ill
 // conditioned, so the result X is refined by one Newton step,
 // X <- X + X (I - D X), which squares its residual.  A zero or non-finite
 // pivot clears the patch's ok flag.
 // A: the patch matrix (n x n), dv: its dinv block, ok: its flag, ws: shared
 // memory of at least kInvWs floats.
+constexpr int kInvLq = 33;
 constexpr int kInvWs = 2 * kGjBlock * kInvLd;
 __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int *ok, int K, float *ws) {
     static_assert(kGjBlock == 64, "two 32x32 quarters");
     static_assert(2 * 32 * kInvLq <= kGjBlock * kInvLd, "X and Y fit in the second buffer");
+    __shared__ float colbuf[2][32];
+    __shared__ int bad;
     const int k0 = K * kGjBlock;
     const int b = min(kGjBlock, n - k0);
     float *D = ws, *W = ws + kGjBlock * kInvLd;  // D: the block, then its inverse; W: scratch
@@ -214,16 +225,15 @@ __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int 
     load_pivot_block(A, n, k0, b, D);
     __syncthreads();
     float *Pq = D, *Bq = D + 32, *Cq = D + 32 * kInvLd, *Eq = Cq + 32;
-    const int lane = threadIdx.x & 31;
-    __shared__ int bad;
-    if (threadIdx.x < 32) {  // P^-1 in place
-        float a[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (w < 4) {  // P^-1 in place
+        float v[8];
 #pragma unroll
-        for (int c = 0; c < 32; ++c) a[c] = Pq[lane * kInvLd + c];
-        const bool bd = warp_invert32(a);
+        for (int c = 0; c < 8; ++c) v[c] = Pq[lane * kInvLd + 8 * w + c];
+        const bool bd = quad_invert32(v, colbuf);
 #pragma unroll
-        for (int c = 0; c < 32; ++c) Pq[lane * kInvLd + c] = a[c];
-        if (lane == 0) bad = bd ? 1 : 0;
+        for (int c = 0; c < 8; ++c) Pq[lane * kInvLd + 8 * w + c] = v[c];
+        if (threadIdx.x == 0) bad = bd ? 1 : 0;
     }
     __syncthreads();
     block_gemm32(Pq, kInvLd, Bq, kInvLd, X, kInvLq, nullptr, 0, 1.0f);  // X = P^-1 B
@@ -231,14 +241,14 @@ __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int 
     __syncthreads();
     block_gemm32(Cq, kInvLd, X, kInvLq, Eq, kInvLd, Eq, kInvLd, -1.0f);  // S = E - C X, in place of E
     __syncthreads();
-    if (threadIdx.x < 32) {  // S^-1 in place
-        float a[32];
+    if (w < 4) {  // S^-1 in place
+        float v[8];
 #pragma unroll
-        for (int c = 0; c < 32; ++c) a[c] = Eq[lane * kInvLd + c];
-        const bool bd = warp_invert32(a);
+        for (int c = 0; c < 8; ++c) v[c] = Eq[lane * kInvLd + 8 * w + c];
+        const bool bd = quad_invert32(v, colbuf);
 #pragma unroll
-        for (int c = 0; c < 32; ++c) Eq[lane * kInvLd + c] = a[c];
-        if (lane == 0 && bd) bad = 1;
+        for (int c = 0; c < 8; ++c) Eq[lane * kInvLd + 8 * w + c] = v[c];
+        if (threadIdx.x == 0 && bd) bad = 1;
     }
     __syncthreads();
     block_gemm32(X, kInvLq, Eq, kInvLd, Bq, kInvLd, nullptr, 0, -1.0f);  // top right  -X S^-1, in place of B
