@@ -466,6 +466,9 @@ def run_ours(args):
             "speedup_vs_plain": value / plain_value,
             "rpy_pairs_per_s": pairs / (apply_us * 1e-6), "rpy_apply_us": apply_us,
             "patch_refresh_ms": refresh_ms, "tuning": tuning,
+            # build-comparable figure: the step time outside the refresh per GMRES iteration (the iteration count
+            # itself follows the chaotic trajectory, which any change in a floating-point sum order moves)
+            "ms_per_gmres_iteration": (max_ms / args.steps - refresh_ms) / max(1.0, float(np.mean(iters))),
             "roofline": dominant, "roofline_other": other,
             "traffic_note": "ncu (profiles/gj_update_16x16_patches.md): one gj_update launch, the refresh's top "
                             "kernel, reads 37.4 MB of DRAM under ncu's cold cache (one read of the upper block "

@@ -585,19 +585,21 @@ __global__ void __launch_bounds__(256) gj_mirror_kernel(PatchDev P) {
 }
 
 // out = blockdiag(A_pp^-1) in over the patches (in and out must differ).
-// grid = (row chunks of 64, patches); the block gathers the patch's rows of
-// `in` into shared memory, each warp forms 8 output rows with the lanes
-// striding the (coalesced) matrix row.  A patch without a finite inverse uses
-// the block-diagonal preconditioner instead (first row chunk only).
+// grid = (row chunks of kApplyRows, patches), kApplyThreads threads; the block
+// gathers the patch's rows of `in` into shared memory, each warp forms two
+// output rows with the lanes striding the (coalesced, 16-byte) matrix rows,
+// four loads per row in flight.  A patch without a finite inverse uses the
+// block-diagonal preconditioner instead (first row chunk only).
 // Dynamic shared memory: max(patch_ld(max_n), 3*nseg) doubles.
 // With `masked`, patches of arrays whose GMRES stopped are skipped.
-__global__ void __launch_bounds__(256) patch_apply_kernel(SimDev d, PatchDev P, const double *in, double *out,
-                                                          int masked) {
+constexpr int kApplyRows = 32, kApplyThreads = 16 * 32;  // two rows per warp
+__global__ void __launch_bounds__(kApplyThreads) patch_apply_kernel(SimDev d, PatchDev P, const double *in,
+                                                                   double *out, int masked) {
     extern __shared__ __align__(16) double xs[];
     __shared__ double sm32[32];
     const int p = blockIdx.y;
     const int n = P.nf[p] * P.nbf;
-    const int r0 = blockIdx.x * 64;
+    const int r0 = blockIdx.x * kApplyRows;
     if (r0 >= n) return;
     if (masked && !d.active[d.fil_arr[P.fils[P.fil0[p]]]]) return;
     if (!P.ok[p]) {
@@ -616,13 +618,14 @@ __global__ void __launch_bounds__(256) patch_apply_kernel(SimDev d, PatchDev P, 
     const float *A = P.A + P.moff[p];
     const double2 *x2 = reinterpret_cast<const double2 *>(xs);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int rr = 0; rr < 8; rr += 2) {  // two rows at a time, 16-byte loads of the (padded) matrix rows
-        const int r = r0 + warp * 8 + rr;
-        if (r >= n) break;
+    {
+        const int r = r0 + 2 * warp;  // this warp's two rows
+        if (r >= n) return;
         const bool two = r + 1 < n;
         const float4 *a0 = reinterpret_cast<const float4 *>(A + static_cast<size_t>(r) * ld);
         const float4 *a1 = a0 + n4;
         double s0 = 0.0, s1 = 0.0;
+#pragma unroll 4
         for (int c4 = lane; c4 < n4; c4 += 32) {
             const float4 v0 = __ldg(a0 + c4);
             const float4 v1 = two ? __ldg(a1 + c4) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);

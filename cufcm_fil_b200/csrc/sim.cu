@@ -264,7 +264,8 @@ int launch_refresh(Engine *e, cudaStream_t st) {
 int refresh_launches(const Engine *e) { return e->line ? 4 + 2 * e->gj_rounds : 0; }
 
 int launch_patch_apply(Engine *e, const double *in, double *out, int masked, cudaStream_t st) {
-    patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), 256, e->apply_smem, st>>>(e->d, e->P, in, out, masked);
+    patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), kApplyThreads, e->apply_smem, st>>>(e->d, e->P, in, out,
+                                                                                            masked);
     CF_CHECK_LAUNCH("patch_apply_kernel");
     return CF_OK;
 }
@@ -627,7 +628,7 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     e->gj_update_grid = static_cast<int>(std::min<long long>(1LL * P.np * (T * (T + 1) / 2), 2LL * e->num_sms));
     CF_CUDA(cudaFuncSetAttribute(gj_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kUpdateSmem)));
-    e->apply_chunks = (max_n + 63) / 64;
+    e->apply_chunks = (max_n + kApplyRows - 1) / kApplyRows;
     e->apply_smem = sizeof(double) * std::max(patch_ld(max_n), 3 * d.nseg);
     e->refresh_every = cfgs[0].precond_refresh > 0 ? cfgs[0].precond_refresh : 1;
     return CF_OK;

@@ -775,7 +775,7 @@ __device__ __forceinline__ unsigned int ranges_meeting(long long i0, long long i
 // arrays.  Items are ordered array by array (array b owns items
 // (k+1)*[chunk0, chunk0 + nchunk), j-major inside), each block takes a
 // contiguous range of them, and the block arriving last for an array sums its
-// chunks of each j in order into h.  Loads are issued four at a time into
+// chunks of each j into h (one warp per j, a fixed order).  Loads are issued four at a time into
 // independent accumulators so that each thread keeps several in flight.
 __global__ void __launch_bounds__(256) dots_kernel(SimDev d, double *h) {
     __shared__ double sm32[32];
@@ -798,12 +798,15 @@ __global__ void __launch_bounds__(256) dots_kernel(SimDev d, double *h) {
                 const ArrayInfo &a = d.arr[cur];
                 const unsigned int need = ranges_meeting(K1 * a.chunk0, K1 * (a.chunk0 + a.nchunk), per);
                 if (arrive_last(&d.ctl[cur].counter, need, &last)) {
+                    // one warp per basis vector sums its chunks' partials in a fixed order
                     double *hb = h + static_cast<size_t>(cur) * d.sstride;
-                    for (int jj = threadIdx.x; jj <= k; jj += blockDim.x) {
+                    const int lane = threadIdx.x & 31;
+                    for (int jj = threadIdx.x >> 5; jj <= k; jj += blockDim.x >> 5) {
                         double acc = 0.0;
-                        for (int cc = 0; cc < a.nchunk; ++cc)
+                        for (int cc = lane; cc < a.nchunk; cc += 32)
                             acc += __ldcg(&d.dots_partial[static_cast<size_t>(jj) * C + a.chunk0 + cc]);
-                        hb[jj] = acc;
+                        acc = warp_sum(acc);
+                        if (lane == 0) hb[jj] = acc;
                     }
                     __syncthreads();
                     if (threadIdx.x == 0) d.ctl[cur].counter = 0;
