@@ -7,7 +7,7 @@ part (z - P_bd(w)) / s that the block-diagonal preconditioner misses
 library's own kernels (FilamentMLP.train_step: BF16 tensor-core GEMMs, Adam).
 `compare` runs the same state with and without the network, the check that
 decides whether a trained network is worth using: the block-diagonal
-preconditioner stays the fallback and the judge.
+preconditioner stays the fallback and the reference point.
 """
 from __future__ import annotations
 

@@ -3,7 +3,7 @@
 Features are checked against the oracle's restatement (float32 storage: 1e-6
 relative); training uses the library's own kernels; the comparison with the
 block-diagonal preconditioner on a state the network has not seen is reported
-(gain = block-diagonal iterations / learned iterations) and the judge's choice is
+(gain = block-diagonal iterations / learned iterations) and compare's choice is
 checked against it.  Whatever the network does, a converged learned step
 satisfies the oracle's FP64 system (the residual is formed with the exact operator).
 """
@@ -58,7 +58,7 @@ def test_collected_pairs_shape_and_values():
     assert bool(x.isfinite().all()) and bool(t.isfinite().all())
 
 
-def test_trained_network_gain_is_measured_and_judged():
+def test_trained_network_gain_is_measured_and_decided():
     x, t = learned.collect(make_sim, seeds=(10, 11, 12), max_pairs=120)
     with FilamentMLP(182, 256, 62, max_batch=4096, seed=0) as net:
         losses = learned.train(net, x, t, steps=1500, batch=2048, lr=1e-3, report_every=500)
