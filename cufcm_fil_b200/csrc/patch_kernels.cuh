@@ -305,13 +305,15 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
 // memory as U[s][c].  The pass writes
 //   rbuf[s][j] = (D^-1 U)[s][j] outside the pivot columns, -D^-1[s][j - k0] inside,
 //   cbuf[s][j] = U[s][j]         for j outside the pivot rows (zero inside),
-// both [64][n] with row stride n.  Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
+// both [64][ld].  Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
 // block's or disjoint from it.  Each thread owns 4 rows x 4 columns of
-// D^-1 U (rows ty + 16u, columns tx + 16v).  grid = (tiles, patches).
+// D^-1 U (rows 4ty + u, columns 4tx + v); the loads and stores of the
+// product's operands and results move 16 bytes each.  grid = (tiles, patches).
 __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     static_assert(kGjTile == kGjBlock, "column tiles are pivot-block wide");
-    __shared__ float Dv[kGjBlock][kGjBlock + 1];
-    __shared__ float Us[kGjBlock][kGjTile + 1];
+    constexpr int LD = kGjTile + 4;  // 16-byte rows
+    __shared__ __align__(16) float DvT[kGjBlock][LD];  // DvT[s][r] = D^-1[r][s]
+    __shared__ __align__(16) float Us[kGjBlock][LD];
     const int p = blockIdx.y;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
@@ -334,44 +336,73 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
         }
         return;
     }
-    for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) Dv[e / kGjBlock][e % kGjBlock] = dv[e];
+    // D^-1, 16-byte loads, stored transposed
+    for (int e4 = threadIdx.x; e4 < kGjBlock * kGjBlock / 4; e4 += blockDim.x) {
+        const int r = e4 >> 4, c4 = 4 * (e4 & 15);
+        const float4 v = *reinterpret_cast<const float4 *>(dv + r * kGjBlock + c4);
+        DvT[c4][r] = v.x;
+        DvT[c4 + 1][r] = v.y;
+        DvT[c4 + 2][r] = v.z;
+        DvT[c4 + 3][r] = v.w;
+    }
+    // U, 16-byte chunks of rows of A; chunks at or beyond the row stride are zeros, and so are the padding
+    // columns [n, ld) inside it, so U[s][c] is zero for s >= b or c >= w as the product needs
     if (j0 > k0) {  // U[s][c] = A[k0 + s][j0 + c]
-        for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
-            const int s_ = e / kGjTile, c = e - s_ * kGjTile;
-            Us[s_][c] = (s_ < b && c < w) ? A[(k0 + s_) * ld + j0 + c] : 0.0f;
+        for (int e4 = threadIdx.x; e4 < kGjBlock * kGjTile / 4; e4 += blockDim.x) {
+            const int s_ = e4 >> 4, c4 = 4 * (e4 & 15);
+            float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (s_ < b && j0 + c4 < static_cast<int>(ld)) v = *reinterpret_cast<const float4 *>(A + (k0 + s_) * ld + j0 + c4);
+            *reinterpret_cast<float4 *>(&Us[s_][c4]) = v;
         }
-    } else {  // j0 + 64 <= k0: U[s][c] = A[j0 + c][k0 + s], rows of A read contiguously
-        for (int e = threadIdx.x; e < kGjTile * kGjBlock; e += blockDim.x) {
-            const int c = e / kGjBlock, s_ = e - c * kGjBlock;
-            Us[s_][c] = (s_ < b) ? A[(j0 + c) * ld + k0 + s_] : 0.0f;
+    } else {  // j0 + 64 <= k0: U[s][c] = A[j0 + c][k0 + s], rows of A read contiguously, stored transposed
+        for (int e4 = threadIdx.x; e4 < kGjTile * kGjBlock / 4; e4 += blockDim.x) {
+            const int c = e4 >> 4, s4 = 4 * (e4 & 15);
+            float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (k0 + s4 < static_cast<int>(ld)) v = *reinterpret_cast<const float4 *>(A + (j0 + c) * ld + k0 + s4);
+            Us[s4][c] = v.x;
+            Us[s4 + 1][c] = v.y;
+            Us[s4 + 2][c] = v.z;
+            Us[s4 + 3][c] = v.w;
         }
     }
     __syncthreads();
+    // rows 4ty + u, columns 4tx + v of D^-1 U: one float4 of each operand per step
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     float acc[4][4] = {};
 #pragma unroll 8
     for (int s_ = 0; s_ < kGjBlock; ++s_) {
-        float dr[4], uc[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) dr[u] = Dv[ty + 16 * u][s_];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) uc[v] = Us[s_][tx + 16 * v];
+        const float4 d4 = *reinterpret_cast<const float4 *>(&DvT[s_][4 * ty]);
+        const float4 u4 = *reinterpret_cast<const float4 *>(&Us[s_][4 * tx]);
+        const float dr[4] = {d4.x, d4.y, d4.z, d4.w}, uc[4] = {u4.x, u4.y, u4.z, u4.w};
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
             for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(dr[u], uc[v], acc[u][v]);
     }
+    const int c0 = 4 * tx;
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < 4; ++u) {  // rows >= b: zeros (D^-1 is zero-padded)
+        float *dst = rb + (4 * ty + u) * ld + j0 + c0;
+        if (c0 + 3 < w) {
+            *reinterpret_cast<float4 *>(dst) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+        } else {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int c = tx + 16 * v;
-            if (c < w) rb[(ty + 16 * u) * ld + j0 + c] = acc[u][v];  // rows >= b: zeros
+            for (int v = 0; v < 4; ++v)
+                if (c0 + v < w) dst[v] = acc[u][v];
         }
+    }
     // the pivot-row entries of the tile's columns
-    for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
-        const int s_ = e / kGjTile, c = e - s_ * kGjTile;
-        if (c < w) cb[s_ * ld + j0 + c] = Us[s_][c];
+    for (int e4 = threadIdx.x; e4 < kGjBlock * kGjTile / 4; e4 += blockDim.x) {
+        const int s_ = e4 >> 4, c4 = 4 * (e4 & 15);
+        const float4 v = *reinterpret_cast<const float4 *>(&Us[s_][c4]);
+        float *dst = cb + s_ * ld + j0 + c4;
+        if (c4 + 3 < w) {
+            *reinterpret_cast<float4 *>(dst) = v;
+        } else {
+            if (c4 < w) dst[0] = v.x;
+            if (c4 + 1 < w) dst[1] = v.y;
+            if (c4 + 2 < w) dst[2] = v.z;
+        }
     }
 }
 
