@@ -154,35 +154,48 @@ __device__ __forceinline__ bool quad_invert32(float (&v)[8], float (*colbuf)[32]
 }
 
 // O[i][j] (+)= sign * sum_k L[i][k] R[k][j] for 32x32 blocks in shared memory
-// (leading dimensions ldl, ldr, ldo); all 256 threads, 4 entries each.
+// (leading dimensions ldl, ldr, ldo); all 256 threads, each 2 rows x 2
+// columns (rows 2ty, 2ty + 1, columns tx, tx + 16): one shared load per FMA.
 __device__ __forceinline__ void block_gemm32(const float *L, int ldl, const float *R, int ldr, float *O, int ldo,
                                              const float *Add, int lda, float sign) {
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const int o = threadIdx.x + 256 * m, i = o >> 5, j = o & 31;
-        float acc = 0.0f;
+    const int i0 = 2 * (threadIdx.x >> 4), j0 = threadIdx.x & 15;
+    float a00 = 0.0f, a01 = 0.0f, a10 = 0.0f, a11 = 0.0f;
 #pragma unroll 8
-        for (int k = 0; k < 32; ++k) acc = fmaf(L[i * ldl + k], R[k * ldr + j], acc);
-        O[i * ldo + j] = (Add ? Add[i * lda + j] : 0.0f) + sign * acc;
+    for (int k = 0; k < 32; ++k) {
+        const float l0 = L[i0 * ldl + k], l1 = L[(i0 + 1) * ldl + k];
+        const float r0 = R[k * ldr + j0], r1 = R[k * ldr + j0 + 16];
+        a00 = fmaf(l0, r0, a00);
+        a01 = fmaf(l0, r1, a01);
+        a10 = fmaf(l1, r0, a10);
+        a11 = fmaf(l1, r1, a11);
     }
+    const float acc[2][2] = {{a00, a01}, {a10, a11}};
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            const int i = i0 + u, j = j0 + 16 * v;
+            O[i * ldo + j] = (Add ? Add[i * lda + j] : 0.0f) + sign * acc[u][v];
+        }
 }
 
-// acc = L R for 64x64 blocks in shared memory (leading dimension kInvLd); each
-// of the 256 threads owns rows 4*(tid/16) + u and columns tid%16 + 16v.
-constexpr int kInvLd = kGjBlock + 1;
+// acc = L R for 64x64 blocks in shared memory (leading dimension kInvLd, 16-byte
+// rows); each of the 256 threads owns rows 4*(tid/16) + u and columns
+// 4*(tid%16) + v, the R operand read as one float4 per step.
+constexpr int kInvLd = kGjBlock + 4;
 __device__ __forceinline__ void block_gemm64(const float *L, const float *R, float (&acc)[4][4]) {
-    const int r0 = 4 * (threadIdx.x >> 4), c0 = threadIdx.x & 15;
+    const int r0 = 4 * (threadIdx.x >> 4), c0 = 4 * (threadIdx.x & 15);
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) acc[u][v] = 0.0f;
 #pragma unroll 8
     for (int k = 0; k < kGjBlock; ++k) {
-        float l[4], r[4];
+        float l[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) l[u] = L[(r0 + u) * kInvLd + k];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) r[v] = R[k * kInvLd + c0 + 16 * v];
+        const float4 r4 = *reinterpret_cast<const float4 *>(&R[k * kInvLd + c0]);
+        const float r[4] = {r4.x, r4.y, r4.z, r4.w};
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -262,18 +275,18 @@ __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int 
     float acc[4][4];
     block_gemm64(W, D, acc);
     __syncthreads();
-    const int r0 = 4 * (threadIdx.x >> 4), c0 = threadIdx.x & 15;
+    const int r0 = 4 * (threadIdx.x >> 4), c0 = 4 * (threadIdx.x & 15);
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) W[(r0 + u) * kInvLd + c0 + 16 * v] = (r0 + u == c0 + 16 * v ? 1.0f : 0.0f) - acc[u][v];
+        for (int v = 0; v < 4; ++v) W[(r0 + u) * kInvLd + c0 + v] = (r0 + u == c0 + v ? 1.0f : 0.0f) - acc[u][v];
     __syncthreads();
     block_gemm64(D, W, acc);
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const int r = r0 + u, c = c0 + 16 * v;
+            const int r = r0 + u, c = c0 + v;
             dv[r * kGjBlock + c] = (r < b && c < b) ? D[r * kInvLd + c] + acc[u][v] : 0.0f;
         }
     if (threadIdx.x == 0) {
@@ -290,7 +303,7 @@ __device__ __forceinline__ void pivot_invert_patch(const PatchDev &P, int p, int
 // Round 0, part (a): the first pivot block of every patch (later pivot blocks
 // are inverted by the previous round's update, see gj_update_kernel).
 __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
-    __shared__ float ws[kInvWs];
+    __shared__ __align__(16) float ws[kInvWs];
     const int p = blockIdx.x;
     const int n = P.nf[p] * P.nbf;
     if (K * kGjBlock >= n) return;
