@@ -87,7 +87,8 @@ __global__ void patch_mobility_kernel(SimDev d, PatchDev P) {
             const float dz = static_cast<float>(d.xd[3 * gi + 2] - d.xd[3 * gj + 2]);
             wall_pair_f32<3, 3>(dx, dy, dz, zi, static_cast<float>(d.xd[3 * gj + 2]), f, v);
         }
-        for (int q = 0; q < 3; ++q) A[(r0 + q) * ld + c0 + c] = v[q];
+        for (int q = 0; q < 3; ++q)  // the sweep reads the upper block triangle only
+            if ((r0 + q) / kGjTile <= (c0 + c) / kGjTile) A[(r0 + q) * ld + c0 + c] = v[q];
     }
 }
 
@@ -592,6 +593,21 @@ __global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, in
                 }
             }
             if (bad) P.ok[cur.p] = 0;
+            if (last && cur.row0 < cur.col0) {
+                // final values: also the transposed tile of the lower block triangle (A^-1 is symmetric); its
+                // columns row0 + 4ty .. + 3 lie in a full row tile, below n
+                float *At = P.A + P.moff[cur.p] + cur.row0 + 4 * ty;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int jt = j + v;  // the lower tile's row
+                    if (jt >= n) continue;
+                    const float4 t4 = make_float4(v == 0 ? res[0].x : v == 1 ? res[0].y : v == 2 ? res[0].z : res[0].w,
+                                                  v == 0 ? res[1].x : v == 1 ? res[1].y : v == 2 ? res[1].z : res[1].w,
+                                                  v == 0 ? res[2].x : v == 1 ? res[2].y : v == 2 ? res[2].z : res[2].w,
+                                                  v == 0 ? res[3].x : v == 1 ? res[3].y : v == 2 ? res[3].z : res[3].w);
+                    *reinterpret_cast<float4 *>(At + static_cast<size_t>(jt) * ld) = t4;
+                }
+            }
             if (cur.diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
                 __syncthreads();
                 pivot_invert_patch(P, cur.p, K + 1, st);
@@ -602,30 +618,6 @@ __global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, in
         stage ^= 1;
     }
     cp_async_wait<0>();
-}
-
-// After the last round: fills the lower block triangle from the upper one
-// (tile (ti, tj), ti > tj, from the transpose of tile (tj, ti)); the matrix is
-// then -A_pp^-1 in full.  grid = (tiles, patches).
-__global__ void __launch_bounds__(256) gj_mirror_kernel(PatchDev P) {
-    __shared__ float tile[kGjTile][kGjTile + 1];
-    const int p = blockIdx.y;
-    const int n = P.nf[p] * P.nbf;
-    const int T = (n + kGjTile - 1) / kGjTile;
-    if (static_cast<int>(blockIdx.x) >= T * T) return;
-    const int ti = blockIdx.x / T, tj = blockIdx.x - ti * T;
-    if (ti <= tj) return;
-    float *A = P.A + P.moff[p];
-    const int r0 = tj * kGjTile, c0 = ti * kGjTile;  // the source tile, upper triangle
-    for (int e = threadIdx.x; e < kGjTile * kGjTile; e += blockDim.x) {
-        const int r = e / kGjTile, c = e - r * kGjTile;
-        tile[r][c] = (r0 + r < n && c0 + c < n) ? A[static_cast<size_t>(r0 + r) * patch_ld(n) + c0 + c] : 0.0f;
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < kGjTile * kGjTile; e += blockDim.x) {
-        const int r = e / kGjTile, c = e - r * kGjTile;  // destination (c0 + r, r0 + c)
-        if (c0 + r < n && r0 + c < n) A[static_cast<size_t>(c0 + r) * patch_ld(n) + r0 + c] = tile[c][r];
-    }
 }
 
 // out = blockdiag(A_pp^-1) in over the patches (in and out must differ).

@@ -256,12 +256,10 @@ int launch_refresh(Engine *e, cudaStream_t st) {
         gj_update_kernel<<<e->gj_update_grid, 256, kUpdateSmem, st>>>(P, K, e->gj_cols, P.counter + K);
         CF_CHECK_LAUNCH("gj_update_kernel");
     }
-    gj_mirror_kernel<<<dim3(e->gj_tiles, P.np), 256, 0, st>>>(P);
-    CF_CHECK_LAUNCH("gj_mirror_kernel");
     return CF_OK;
 }
 
-int refresh_launches(const Engine *e) { return e->line ? 4 + 2 * e->gj_rounds : 0; }
+int refresh_launches(const Engine *e) { return e->line ? 3 + 2 * e->gj_rounds : 0; }
 
 int launch_patch_apply(Engine *e, const double *in, double *out, int masked, cudaStream_t st) {
     patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), kApplyThreads, e->apply_smem, st>>>(e->d, e->P, in, out,
