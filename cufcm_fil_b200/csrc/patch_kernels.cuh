@@ -92,29 +92,28 @@ __global__ void patch_mobility_kernel(SimDev d, PatchDev P) {
     }
 }
 
-// Rate entries -K / -K^T of each filament of a patch (one block per patch).
+// Rate rows and columns of a patch: -K / -K^T of each filament, zero between
+// filaments and between rates.  grid = (entry chunks, patches).
 __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
-    const int p = blockIdx.x;
+    const int p = blockIdx.y;
     const int nfp = P.nf[p];
-    const int ld = patch_ld(nfp * P.nbf);
-    const int nl = 3 * d.nseg;
+    const int n = nfp * P.nbf, ld = patch_ld(n);
+    const int nl = 3 * d.nseg, nr = P.nbf - nl;  // lambda rows and rate rows per filament
     float *A = P.A + P.moff[p];
-    for (int e = threadIdx.x; e < nfp * nl; e += blockDim.x) {
-        const int a = e / nl, li = e - a * nl;
-        const int g3 = 3 * P.fils[P.fil0[p] + a] * d.nseg + li;  // entry of kp / ka
-        const long long r = static_cast<long long>(a) * P.nbf + li;
-        long long c = static_cast<long long>(a) * P.nbf + nl;
-        if (d.dyn_phase) {
-            const float v = -static_cast<float>(d.kp[g3]);
-            A[r * ld + c] = v;
-            A[c * ld + r] = v;
-            ++c;
+    // every (row, rate column) entry and its transpose: -k of the row's own filament, zero elsewhere (the
+    // matrix is not cleared between rebuilds: the lambda block is assembled in full, and this covers the rest)
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * nfp * nr; e += gridDim.x * blockDim.x) {
+        const int rc = e / n, r = e - rc * n;
+        const int a = rc / nr, q = rc - a * nr;  // rate column: filament a, rate q (phase first)
+        const int c = a * P.nbf + nl + q;
+        const int ar = r / P.nbf, li = r - ar * P.nbf;
+        float v = 0.0f;
+        if (ar == a && li < nl) {
+            const int g3 = 3 * P.fils[P.fil0[p] + a] * d.nseg + li;  // entry of kp / ka
+            v = -static_cast<float>((d.dyn_phase && q == 0) ? d.kp[g3] : d.ka[g3]);
         }
-        if (d.dyn_angle) {
-            const float v = -static_cast<float>(d.ka[g3]);
-            A[r * ld + c] = v;
-            A[c * ld + r] = v;
-        }
+        A[static_cast<size_t>(r) * ld + c] = v;
+        A[static_cast<size_t>(c) * ld + r] = v;
     }
 }
 

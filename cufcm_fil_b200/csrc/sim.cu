@@ -79,7 +79,7 @@ struct Engine {
     PatchDev P{};
     long long patch_floats = 0;
     int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_cols = 1, gj_tiles = 1;
-    int apply_chunks = 1, gj_update_grid = 1;
+    int apply_chunks = 1, gj_update_grid = 1, rates_grid = 1;
     bool refreshed_last = false;
     size_t apply_smem = 0;
     cudaGraph_t rgraph = nullptr;
@@ -242,11 +242,10 @@ int launch_combine(Engine *e, cudaStream_t st) {
 // Assembles and inverts every patch block for the current kinematics.
 int launch_refresh(Engine *e, cudaStream_t st) {
     const PatchDev &P = e->P;
-    CF_CUDA(cudaMemsetAsync(P.A, 0, sizeof(float) * e->patch_floats, st));
     CF_CUDA(cudaMemsetAsync(P.counter, 0, sizeof(int) * e->gj_rounds, st));
     patch_mobility_kernel<<<dim3(e->mob_grid, P.np), 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_mobility_kernel");
-    patch_rates_kernel<<<P.np, 256, 0, st>>>(e->d, P);
+    patch_rates_kernel<<<dim3(e->rates_grid, P.np), 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_rates_kernel");
     gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, 0);  // later pivot blocks: inverted inside the previous update
     CF_CHECK_LAUNCH("gj_pivot_kernel");
@@ -607,6 +606,7 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     CF_TRY(eng_upload(e, const_cast<long long **>(&P.roff), roff.data(), roff.size()));
     CF_TRY(eng_upload(e, const_cast<long long **>(&P.rows), rows.data(), rows.size()));
     CF_TRY(eng_alloc(e, &P.A, static_cast<size_t>(mo)));
+    CF_CUDA(cudaMemset(P.A, 0, sizeof(float) * static_cast<size_t>(mo)));  // the padding columns stay zero
     P.max_ld = patch_ld(max_n);
     CF_TRY(eng_alloc(e, &P.cbuf, static_cast<size_t>(P.np) * P.max_ld * kGjBlock));
     CF_TRY(eng_alloc(e, &P.rbuf, static_cast<size_t>(P.np) * P.max_ld * kGjBlock));
@@ -621,6 +621,7 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     e->mob_grid = static_cast<int>((ns * ns + 255) / 256);
     e->gj_rounds = (max_n + kGjBlock - 1) / kGjBlock;
     const int T = (max_n + kGjTile - 1) / kGjTile;
+    e->rates_grid = std::max(1, (max_n * max_nf * (nbf - nl) + 255) / 256);
     e->gj_cols = T;
     e->gj_tiles = T * T;
     e->gj_update_grid = static_cast<int>(std::min<long long>(1LL * P.np * (T * (T + 1) / 2), 2LL * e->num_sms));
