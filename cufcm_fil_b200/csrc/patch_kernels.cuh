@@ -75,6 +75,7 @@ __global__ void patch_mobility_kernel(SimDev d, PatchDev P) {
     float *A = P.A + P.moff[p];
     const long long r0 = static_cast<long long>(ai) * P.nbf + 3 * ki;
     const long long c0 = static_cast<long long>(aj) * P.nbf + 3 * kj;
+    if (r0 / kGjTile > (c0 + 2) / kGjTile) return;  // wholly in the lower block triangle, which the sweep never reads
     const float zi = static_cast<float>(d.xd[3 * gi + 2]);
     for (int c = 0; c < 3; ++c) {
         float f[3] = {0.0f, 0.0f, 0.0f}, v[3] = {0.0f, 0.0f, 0.0f};
