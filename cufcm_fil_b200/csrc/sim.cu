@@ -78,7 +78,7 @@ struct Engine {
     bool line = false;
     PatchDev P{};
     long long patch_floats = 0;
-    int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_cols = 1, gj_tiles = 1;
+    int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_cols = 1;
     int apply_chunks = 1, gj_update_grid = 1, rates_grid = 1;
     bool refreshed_last = false;
     size_t apply_smem = 0;
@@ -623,7 +623,6 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     const int T = (max_n + kGjTile - 1) / kGjTile;
     e->rates_grid = std::max(1, (max_n * max_nf * (nbf - nl) + 255) / 256);
     e->gj_cols = T;
-    e->gj_tiles = T * T;
     e->gj_update_grid = static_cast<int>(std::min<long long>(1LL * P.np * (T * (T + 1) / 2), 2LL * e->num_sms));
     CF_CUDA(cudaFuncSetAttribute(gj_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kUpdateSmem)));
