@@ -92,6 +92,7 @@ SIGNATURES = {
     "cf_apply_mobility": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "cf_apply_mobility_device": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "cf_rpy_wall_segments_noalloc": [_vp, _vp, _vp, _i, _vp],
+    "cf_set_wait_limit": [ctypes.c_uint],
     "cf_fcm_create": [ctypes.POINTER(FcmConfig), ctypes.POINTER(_vp)],
     "cf_fcm_destroy": [_vp],
     "cf_fcm_apply": [_vp, _vp, _vp, _vp],
@@ -121,6 +122,7 @@ SIGNATURES = {
     "cf_sim_assemble_rhs": [_vp, _i, _vp],
     "cf_sim_apply_preconditioner": [_vp, _vp, _vp],
     "cf_sim_system_matvec": [_vp, _vp, _vp],
+    "cf_sim_solve": [_vp, _vp, _vp, _d, _i, ctypes.POINTER(_i), ctypes.POINTER(_d)],
     "cf_sim_autotune": [_vp, _i, _vp],
     "cf_sim_refresh_preconditioner": [_vp],
     "cf_sim_learned_dims": [_vp, _vp, _vp],
@@ -140,6 +142,8 @@ SIGNATURES = {
     "cf_mlp_get_params": [_vp, _vp],
     "cf_mlp_set_params": [_vp, _vp],
     "cf_mlp_stream": [_vp, ctypes.POINTER(_vp)],
+    "cf_precond_save": [_vp, _d, ctypes.c_char_p],
+    "cf_precond_load": [ctypes.c_char_p, _i, _i, ctypes.POINTER(_vp), ctypes.POINTER(_d)],
     "cf_batch_create": [_vp, _i, ctypes.POINTER(_vp)],
     "cf_batch_destroy": [_vp],
     "cf_batch_shape": [_vp, _vp, _vp, _vp, _vp],

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstring>
 #include <new>
 #include <random>
 #include <string>
@@ -415,6 +417,101 @@ extern "C" int cf_mlp_set_params(cf_mlp *h, const float *params) {
     CF_CUDA(cudaSetDevice(h->device));
     CF_CUDA(cudaStreamSynchronize(h->stream));
     CF_CUDA(cudaMemcpy(h->params, params, sizeof(float) * h->nparam, cudaMemcpyHostToDevice));
+    return CF_OK;
+}
+
+// ------------------------------------------------------------ checkpoints
+// Versioned file of a trained network: the reference keeps no learned state,
+// so the layout is this library's own (little-endian):
+//   char magic[8] = "CFPRECN\0"; uint32 version = 1; uint32 kind = 1 (three
+//   layers, ReLU); int32 in, hidden, out; float64 weight (the correction weight
+//   alpha); int64 nparam; uint64 FNV-1a hash of the parameter bytes;
+//   float32 params[nparam] (W1, b1, W2, b2, W3, b3 as cf_mlp_get_params).
+namespace {
+constexpr char kPrecondMagic[8] = {'C', 'F', 'P', 'R', 'E', 'C', 'N', '\0'};
+constexpr uint32_t kPrecondVersion = 1, kPrecondKind = 1;
+
+uint64_t fnv1a(const void *data, size_t n) {
+    const unsigned char *p = static_cast<const unsigned char *>(data);
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+struct PrecondHeader {
+    char magic[8];
+    uint32_t version, kind;
+    int32_t in, hidden, out, pad;
+    double weight;
+    int64_t nparam;
+    uint64_t hash;
+};
+static_assert(sizeof(PrecondHeader) == 56, "checkpoint header layout");
+}  // namespace
+
+extern "C" int cf_precond_save(cf_mlp *h, double weight, const char *path) {
+    clear_error();
+    CF_REQUIRE(h && path, "cf_precond_save: null argument");
+    CF_REQUIRE(weight == weight, "cf_precond_save: weight is NaN");
+    std::vector<float> params(static_cast<size_t>(h->nparam));
+    CF_TRY(cf_mlp_get_params(h, params.data()));
+    PrecondHeader hd{};
+    std::memcpy(hd.magic, kPrecondMagic, sizeof(hd.magic));
+    hd.version = kPrecondVersion;
+    hd.kind = kPrecondKind;
+    hd.in = h->in;
+    hd.hidden = h->hid;
+    hd.out = h->out;
+    hd.weight = weight;
+    hd.nparam = h->nparam;
+    hd.hash = fnv1a(params.data(), params.size() * sizeof(float));
+    std::FILE *f = std::fopen(path, "wb");
+    if (!f) return set_error(CF_EINVAL, "cf_precond_save: cannot open %s for writing", path);
+    const bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1 &&
+                    std::fwrite(params.data(), sizeof(float), params.size(), f) == params.size();
+    const bool closed = std::fclose(f) == 0;
+    if (!ok || !closed) return set_error(CF_EINVAL, "cf_precond_save: write to %s failed", path);
+    return CF_OK;
+}
+
+extern "C" int cf_precond_load(const char *path, int max_batch, int device, cf_mlp **out, double *weight) {
+    clear_error();
+    CF_REQUIRE(path && out, "cf_precond_load: null argument");
+    *out = nullptr;
+    std::FILE *f = std::fopen(path, "rb");
+    if (!f) return set_error(CF_EINVAL, "cf_precond_load: cannot open %s", path);
+    PrecondHeader hd{};
+    std::vector<float> params;
+    const char *bad = nullptr;
+    if (std::fread(&hd, sizeof(hd), 1, f) != 1) bad = "truncated header";
+    else if (std::memcmp(hd.magic, kPrecondMagic, sizeof(hd.magic)) != 0) bad = "not a preconditioner checkpoint";
+    else if (hd.version != kPrecondVersion) bad = "unsupported version";
+    else if (hd.kind != kPrecondKind) bad = "unsupported network kind";
+    else if (hd.in <= 0 || hd.hidden <= 0 || hd.out <= 0 || hd.in > 4096 || hd.hidden > 4096 || hd.out > 4096)
+        bad = "bad layer widths";
+    else if (hd.nparam != static_cast<int64_t>(hd.in) * hd.hidden + hd.hidden +
+                              static_cast<int64_t>(hd.hidden) * hd.hidden + hd.hidden +
+                              static_cast<int64_t>(hd.hidden) * hd.out + hd.out)
+        bad = "parameter count does not match the widths";
+    if (!bad) {
+        params.resize(static_cast<size_t>(hd.nparam));
+        if (std::fread(params.data(), sizeof(float), params.size(), f) != params.size()) bad = "truncated parameters";
+        else if (fnv1a(params.data(), params.size() * sizeof(float)) != hd.hash) bad = "parameter hash mismatch";
+    }
+    std::fclose(f);
+    if (bad) return set_error(CF_EINVAL, "cf_precond_load: %s: %s", path, bad);
+    cf_mlp *h = nullptr;
+    CF_TRY(cf_mlp_create(hd.in, hd.hidden, hd.out, max_batch, 0ull, device, &h));
+    const int rc = cf_mlp_set_params(h, params.data());
+    if (rc != CF_OK) {
+        cf_mlp_destroy(h);
+        return rc;
+    }
+    *out = h;
+    if (weight) *weight = hd.weight;
     return CF_OK;
 }
 

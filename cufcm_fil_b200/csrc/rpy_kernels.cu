@@ -13,6 +13,7 @@
 #include "tma.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 namespace cufil {
 
@@ -34,6 +35,7 @@ struct TileParams {
     int nt, ns, split, ntp;
     float at, as, inv_mu;
     int *err;
+    unsigned wait_limit;  // tries of the first wait for the staged sources
 };
 
 template <int VD>
@@ -133,11 +135,14 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_tile_kernel(TilePara
         for (int c = 0; c < VD; ++c) hi[k][c] = lo[k][c] = 0.0f;
 
     if (nsrc > 0) {
-        if (!mbar_wait_bounded(bar, 0)) {
-            if (threadIdx.x == 0) {
-                atomicOr(p.err, kErrTmaTimeout);
-                mbar_wait_bounded(bar, 0);  // give the copies in flight a second bounded chance
-            }
+        if (!mbar_wait_bounded(bar, 0, p.wait_limit)) {
+            // Gave up: flag it, skip the sum and the stores, and let every
+            // thread drain the copies already issued (one more bounded wait
+            // with the full limit) before it exits, so that no copy lands in
+            // shared memory that another block has been given.  A copy still
+            // in flight after that second limit is not handled.
+            if (threadIdx.x == 0) atomicOr(p.err, kErrTmaTimeout);
+            mbar_wait_bounded(bar, 0);
             return;
         }
         bool diag = false;
@@ -336,6 +341,7 @@ struct ReduceParams {
     const float4 *partial;
     const float4 *xt, *ft, *tt;  // self block inputs (wall, self set)
     float *out;
+    const int *err;  // may be null; when the word is non-zero every output is a quiet NaN
     int nsplit, nt, ntp, stride, mode;
 };
 
@@ -381,6 +387,12 @@ __global__ void rpy_reduce_kernel(ReduceParams p) {
         for (int c = 0; c < VD; ++c) v[c] += vs[c];
     }
     float *o = p.out + static_cast<size_t>(i) * p.stride;
+    if (p.err && *p.err) {
+        // A tile block gave up waiting and left its partials unwritten: poison
+        // the result instead of summing stale partials.
+        for (int c = 0; c < p.stride; ++c) o[c] = __int_as_float(0x7fc00000);
+        return;
+    }
     if (p.mode == kOutAdd) {
 #pragma unroll
         for (int c = 0; c < VD; ++c) o[c] = static_cast<float>(static_cast<double>(o[c]) + v[c]);
@@ -439,6 +451,7 @@ int launch_tiles_t(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, 
     p.as = d.as;
     p.inv_mu = 1.0f / d.mu;
     p.err = dev_err;
+    p.wait_limit = rpy_wait_limit();
     dim3 grid(plan.tiles, plan.nsplit);
     kern<<<grid, kThreads, plan.smem, st>>>(p);
     CF_CHECK_LAUNCH("rpy_tile_kernel");
@@ -577,10 +590,11 @@ int rpy_prepare(const RpyBlockDesc &d, const RpyPlan &plan) {
 }
 
 int rpy_launch_reduce_f32(const RpyBlockDesc &d, const RpyPlan &plan, const float4 *scratch, float *out_f,
-                          int stride, int mode, cudaStream_t st) {
+                          int stride, int mode, cudaStream_t st, const int *dev_err) {
     if (d.nt <= 0) return CF_OK;
     ReduceParams p;
     p.partial = scratch;
+    p.err = dev_err;
     p.xt = d.xt;
     p.ft = d.fs;
     p.tt = d.ts;
@@ -625,10 +639,28 @@ int rpy_block_product(const RpyBlockDesc &d, float4 *scratch, size_t scratch_cap
     if (plan.scratch_float4 > scratch_cap)
         return set_error(CF_EINVAL, "rpy: scratch too small (%zu < %zu float4)", scratch_cap, plan.scratch_float4);
     if (d.ns > 0) CF_TRY(rpy_launch_tiles(d, plan, scratch, dev_err, st));
-    return rpy_launch_reduce_f32(d, plan, scratch, out_f, stride, mode, st);
+    return rpy_launch_reduce_f32(d, plan, scratch, out_f, stride, mode, st, plan.sym ? nullptr : dev_err);
 }
 
 }  // namespace cufil
+
+namespace {
+std::atomic<unsigned> g_wait_limit{cufil::kMbarSpinLimit};
+}
+
+namespace cufil {
+
+unsigned rpy_wait_limit() { return g_wait_limit.load(std::memory_order_relaxed); }
+
+}  // namespace cufil
+
+// Test hook: sets the tries of the first bounded wait of later tile launches
+// (0: give up at once); a value above the default is clamped to it.
+extern "C" int cf_set_wait_limit(unsigned limit) {
+    cufil::clear_error();
+    g_wait_limit.store(limit < cufil::kMbarSpinLimit ? limit : cufil::kMbarSpinLimit, std::memory_order_relaxed);
+    return CF_OK;
+}
 
 namespace cufil {
 

@@ -93,8 +93,14 @@ enum RpyOut : int { kOutWrite = 0, kOutAdd = 1 };
 // Reduces partials into out_f[i*stride + c] (float) for c < vd; components
 // vd..stride-1 are zeroed in write mode (the reference writes all six
 // entries of a segment velocity, cuda_functions.cu:460-469).
+// With dev_err given, every output of the launch is a quiet NaN when that
+// word is non-zero (a tile block gave up waiting for its sources).
 int rpy_launch_reduce_f32(const RpyBlockDesc &d, const RpyPlan &plan, const float4 *scratch, float *out_f,
-                          int stride, int mode, cudaStream_t st);
+                          int stride, int mode, cudaStream_t st, const int *dev_err = nullptr);
+
+// Tries of the tile kernel's first bounded wait for its staged sources
+// (cf_set_wait_limit); the default is the full limit.
+unsigned rpy_wait_limit();
 
 // Packing helpers between the reference's AoS host layouts and float4 arrays.
 int pack_xyz_to_float4(const float *aos3, float4 *out, int n, cudaStream_t st);

@@ -71,6 +71,8 @@ struct Engine {
     size_t kin_smem = 0, pre_smem = 0, givens_smem = 0;
     bool use_graph = true;
     bool stepped = false;
+    long long geometry = 0;         // kinematics launches so far (the geometry's version)
+    long long refresh_geometry = -1; // geometry version of the current patch inverses
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle handle = 0;
@@ -191,6 +193,7 @@ int apply_tuning(Engine *e, const Tuning &t) {
 int launch_kinematics(Engine *e, cudaStream_t st) {
     kinematics_kernel<<<e->d.F, e->fil_threads, e->kin_smem, st>>>(e->d);
     CF_CHECK_LAUNCH("kinematics_kernel");
+    e->geometry += 1;
     return CF_OK;
 }
 
@@ -242,6 +245,7 @@ int launch_combine(Engine *e, cudaStream_t st) {
 // Assembles and inverts every patch block for the current kinematics.
 int launch_refresh(Engine *e, cudaStream_t st) {
     const PatchDev &P = e->P;
+    e->refresh_geometry = e->geometry;
     CF_CUDA(cudaMemsetAsync(P.counter, 0, sizeof(int) * e->gj_rounds, st));
     patch_mobility_kernel<<<dim3(e->mob_grid, P.np), 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_mobility_kernel");
@@ -288,6 +292,7 @@ int maybe_refresh(Engine *e, int nt) {
     }
     if (e->rexec) CF_CUDA(cudaGraphLaunch(e->rexec, e->stream));
     else CF_TRY(launch_refresh(e, e->stream));
+    e->refresh_geometry = e->geometry;
     e->last_refresh_nt = nt;
     e->refreshed_last = true;
     return CF_OK;
@@ -1342,6 +1347,56 @@ extern "C" int cf_sim_system_matvec(cf_sim *s, const double *in, double *out) {
     CF_CUDA(cudaMemcpyAsync(out, s->d.w, b, cudaMemcpyDeviceToHost, s->stream));
     LoopCtl lc;
     return read_loop(s, &lc);
+}
+
+namespace {
+// The host-driven GMRES loop on the caller's RHS (already in d.rhs) and
+// initial guess (in d.sol); tolerance and iteration cap of this solve only.
+int solve_given(cf_sim *s, double tol, int max_iter) {
+    const int cap = s->arr[0].max_iter;
+    CF_CUDA(cudaMemcpyAsync(&s->d_arr[0].max_iter, &max_iter, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    const SimDev saved = s->d;
+    s->d.tol = tol;
+    s->d.rhs_given = 1;
+    int rc = launch_prologue(s, 0, s->stream);
+    LoopCtl lc{};
+    if (rc == CF_OK) rc = read_loop(s, &lc);
+    int guard = 0;
+    while (rc == CF_OK && lc.cond && guard++ <= s->d.mi_max) {
+        rc = launch_body(s, 0, s->stream);
+        if (rc == CF_OK) rc = read_loop(s, &lc);
+    }
+    if (rc == CF_OK) rc = launch_finish(s, s->stream);
+    s->d = saved;
+    const cudaError_t ce = cudaMemcpyAsync(&s->d_arr[0].max_iter, &cap, sizeof(int), cudaMemcpyHostToDevice,
+                                           s->stream);
+    if (rc != CF_OK) return rc;
+    return cuda_status(ce, "cudaMemcpyAsync", __FILE__, __LINE__);
+}
+}  // namespace
+
+extern "C" int cf_sim_solve(cf_sim *s, const double *rhs, double *x_inout, double tol, int max_iter, int *iters,
+                            double *relres) {
+    clear_error();
+    CF_REQUIRE(s && rhs && x_inout, "cf_sim_solve: null argument");
+    CF_REQUIRE(tol > 0.0 && tol < 1.0, "cf_sim_solve: tol must lie in (0, 1) (got %g)", tol);
+    CF_REQUIRE(max_iter >= 1 && max_iter <= s->d.mi_max,
+               "cf_sim_solve: max_iter must lie in [1, %d] (the handle's gmres_max_iter), got %d", s->d.mi_max,
+               max_iter);
+    CF_REQUIRE(s->geometry > 0, "cf_sim_solve: no geometry yet (call cf_sim_initial_guess or cf_sim_step first)");
+    CF_REQUIRE(!s->learned || s->net, "CF_PRECOND_LEARNED: no network attached (cf_sim_set_network)");
+    CF_CUDA(cudaSetDevice(s->device));
+    const size_t b = sizeof(double) * s->arr[0].n;
+    CF_TRY(launch_step_begin(s, -1, s->stream));
+    CF_CUDA(cudaMemcpyAsync(s->d.rhs, rhs, b, cudaMemcpyHostToDevice, s->stream));
+    CF_CUDA(cudaMemcpyAsync(s->d.sol, x_inout, b, cudaMemcpyHostToDevice, s->stream));
+    if (s->line && s->refresh_geometry != s->geometry) {  // patch inverses of the current geometry
+        CF_TRY(launch_refresh(s, s->stream));
+        s->last_refresh_nt = -1;
+    }
+    CF_TRY(solve_given(s, tol, max_iter));
+    CF_CUDA(cudaMemcpyAsync(x_inout, s->d.sol, b, cudaMemcpyDeviceToHost, s->stream));
+    return cf_sim_last_solve(s, iters, relres);
 }
 
 extern "C" int cf_sim_refresh_preconditioner(cf_sim *s) {

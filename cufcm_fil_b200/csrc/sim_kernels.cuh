@@ -109,6 +109,7 @@ struct SimDev {
     int lin, lout;            // feature and correction widths
     double lalpha;            // weight of the network correction (chosen by validation; 1 by default)
     int dyn_phase, dyn_angle; // rate blocks present
+    int rhs_given;            // solve of a caller's RHS (already in rhs): no RHS assembly, no iteration log
     int s_rows, s_cols;       // arclength table (0 rows: bisection)
     int n_phase_refs, n_angle_refs;
     int dots_chunk, C_tot;
@@ -467,8 +468,13 @@ __global__ void rhs_kernel(SimDev d) {
     double ss = 0.0;
     const bool lam_rows_zero = d.dyn_phase;
     for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-        const double v = lam_rows_zero ? 0.0 : d.phase_dot[m] * d.kp[fr.ks + j];
-        d.rhs[fr.lam + j] = v;
+        double v;
+        if (d.rhs_given) {
+            v = d.rhs[fr.lam + j];
+        } else {
+            v = lam_rows_zero ? 0.0 : d.phase_dot[m] * d.kp[fr.ks + j];
+            d.rhs[fr.lam + j] = v;
+        }
         ss += v * v;
     }
     for (int k = threadIdx.x; k < d.nseg; k += blockDim.x) {
@@ -476,7 +482,10 @@ __global__ void rhs_kernel(SimDev d) {
         d.f4[m * d.nseg + k] = make_float4(static_cast<float>(d.sol[r]), static_cast<float>(d.sol[r + 1]),
                                            static_cast<float>(d.sol[r + 2]), 0.0f);
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && d.rhs_given) {
+        if (fr.ar >= 0) ss += d.rhs[fr.ar] * d.rhs[fr.ar];
+        if (fr.pr >= 0) ss += d.rhs[fr.pr] * d.rhs[fr.pr];
+    } else if (threadIdx.x == 0) {
         const double w0 = d.omega0[m] * 0.5 / 3.14159265358979323846;
         if (fr.ar >= 0) {
             double q_angle = cyclic_spline(d.phase[m], d.angle_refs, d.n_angle_refs) * w0;
@@ -1014,7 +1023,7 @@ __global__ void __launch_bounds__(1024) backsub_kernel(SimDev d) {
         __syncthreads();
     }
     for (int i = it + threadIdx.x; i < d.mi_max; i += blockDim.x) y[i] = 0.0;
-    if (threadIdx.x == 0 && d.iter_log_cap > 0)
+    if (threadIdx.x == 0 && d.iter_log_cap > 0 && !d.rhs_given)
         d.iter_log[static_cast<size_t>(b) * d.iter_log_cap + d.lc->nt % d.iter_log_cap] = it;
 }
 

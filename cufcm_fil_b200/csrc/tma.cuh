@@ -44,10 +44,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
         : "memory");
 }
 
-// Waits for phase `parity` of the barrier; returns false after the spin limit.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Waits for phase `parity` of the barrier; returns false after `limit` tries
+// (limit 0: gives up at once without looking).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint32_t limit = kMbarSpinLimit) {
     const uint32_t addr = smem_u32(bar);
-    for (uint32_t it = 0; it < kMbarSpinLimit; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

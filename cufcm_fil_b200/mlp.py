@@ -7,6 +7,7 @@ Adam); tensors are torch CUDA tensors (float32, contiguous, row-major).
 from __future__ import annotations
 
 import ctypes
+import struct
 
 import numpy as np
 
@@ -19,13 +20,30 @@ def _ptr(t):
 
 class FilamentMLP:
     def __init__(self, n_in: int, hidden: int = 256, n_out: int = 62, max_batch: int = 8192, seed: int = 0,
-                 device: int = 0):
+                 device: int = 0, _handle=None):
         self.n_in, self.hidden, self.n_out, self.max_batch = int(n_in), int(hidden), int(n_out), int(max_batch)
-        h = ctypes.c_void_p()
-        _lib.call("cf_mlp_create", self.n_in, self.hidden, self.n_out, self.max_batch, ctypes.c_ulonglong(seed),
-                  int(device), ctypes.byref(h))
+        if _handle is None:
+            h = ctypes.c_void_p()
+            _lib.call("cf_mlp_create", self.n_in, self.hidden, self.n_out, self.max_batch, ctypes.c_ulonglong(seed),
+                      int(device), ctypes.byref(h))
+        else:
+            h = _handle
         self._h = h
         self.num_params = int(_lib.load().cf_mlp_num_params(h))
+
+    def save(self, path, weight: float = 1.0) -> None:
+        """Versioned checkpoint of the parameters and the correction weight (cf_precond_save)."""
+        _lib.call("cf_precond_save", self._h, float(weight), str(path).encode())
+
+    @classmethod
+    def load(cls, path, max_batch: int = 8192, device: int = 0):
+        """(network, weight) from a cf_precond_save checkpoint (cf_precond_load validates the file)."""
+        h = ctypes.c_void_p()
+        w = ctypes.c_double()
+        _lib.call("cf_precond_load", str(path).encode(), int(max_batch), int(device), ctypes.byref(h), ctypes.byref(w))
+        with open(path, "rb") as f:  # widths from the header the library just accepted
+            n_in, hidden, n_out = struct.unpack_from("<3i", f.read(56), 16)
+        return cls(n_in, hidden, n_out, max_batch, device=device, _handle=h), w.value
 
     def close(self):
         if getattr(self, "_h", None):

@@ -152,6 +152,16 @@ class WallCiliaSimulation:
         _lib.call("cf_sim_system_matvec", self._h, _p(v), _p(out))
         return out
 
+    def solve_linear_system(self, rhs, x0=None, tol: float = 1e-6, max_iter: int = 350):
+        """GMRES on a given RHS for the current geometry (cf_sim_solve); returns (x, GmresResult).
+        The solution becomes the next step's warm start and its rate rows the filament rates."""
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        x = np.zeros(self.size) if x0 is None else np.array(x0, np.float64)
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        rc = _lib.call("cf_sim_solve", self._h, _p(rhs), _p(x), float(tol), int(max_iter), ctypes.byref(it),
+                       ctypes.byref(rel), ok=(_lib.CF_OK, _lib.CF_NOT_CONVERGED, _lib.CF_NONFINITE))
+        return x, GmresResult(it.value, rel.value, rc)
+
     # -- state ------------------------------------------------------------
     def stream_handle(self) -> int:
         """cudaStream_t of the engine's stream (for events / external streams)."""

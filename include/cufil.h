@@ -132,9 +132,22 @@ CF_API int cf_apply_mobility_device(cf_mobility *h, const float *d_x_segs, const
  * resolves that array's device address; make it before any stream capture.
  * Asynchronous on `stream` (NULL: the legacy default stream).  All calls share
  * the one array, so calls that overlap on the GPU race: serialise them (one
- * stream, or events). */
+ * stream, or events).  It uses the split-source tile kernel, not the symmetric
+ * kernel of cf_evaluate_segment_segment_mobility, so the two agree to the
+ * mobility tolerance (1e-5 relative L2), not bit for bit.  It never
+ * synchronises, so a bounded device wait that gives up cannot be returned as
+ * CF_TIMEOUT: every entry of d_v_segs is then a quiet NaN instead. */
 CF_API int cf_rpy_wall_segments_noalloc(const float *d_x_segs, const float *d_f_segs, float *d_v_segs, int n_seg,
                                         void *stream);
+
+/* Test hook, no counterpart in the reference: the number of tries of the first
+ * bounded wait with which later launches of the staged tile kernel wait for
+ * their sources (process-wide; the default and the maximum are the full
+ * limit).  0 makes every such wait give up at once: the block still drains its
+ * copies with the full limit, skips its sum, and the product reports
+ * CF_TIMEOUT (handle path) or NaN outputs (cf_rpy_wall_segments_noalloc).
+ * Restore the default with cf_set_wait_limit(~0u). */
+CF_API int cf_set_wait_limit(unsigned limit);
 
 /* ================================================================ fcm ==
  * Fast force-coupling method in a triply periodic box: the reference's cuFCM
@@ -289,6 +302,18 @@ CF_API int cf_sim_assemble_rhs(cf_sim *s, int nt, double *rhs);
 CF_API int cf_sim_apply_preconditioner(cf_sim *s, const double *in, double *out);
 /* system_matrix_mult_new: out = A in (host vectors, system size). */
 CF_API int cf_sim_system_matvec(cf_sim *s, const double *in, double *out);
+/* solve_linear_system (mobility_solver.cpp:2187-2669) on a caller's right-hand
+ * side: GMRES with the handle's preconditioner on A x = rhs for the current
+ * geometry (that of the last cf_sim_step or cf_sim_initial_guess; CF_EINVAL
+ * before either), x_inout the initial guess on entry (discarded, as the
+ * reference does, when its residual exceeds |rhs|) and the solution on return.
+ * tol is the relative residual target, max_iter at most the handle's
+ * gmres_max_iter.  As in the reference, the solution also becomes the warm
+ * start of the next step and its rate rows the filament rates.  Status as
+ * cf_sim_step (CF_NOT_CONVERGED at the cap with the iterate returned); the
+ * iteration log of the steps is not touched. */
+CF_API int cf_sim_solve(cf_sim *s, const double *rhs, double *x_inout, double tol, int max_iter, int *iters,
+                        double *relres);
 
 /* Launch shapes of the iteration kernels: choice[5] = {pair-kernel CTAs per
  * SM, dot-product row chunk, dot-product blocks per SM, update blocks per SM,
@@ -331,6 +356,15 @@ CF_API int cf_mlp_train_step(cf_mlp *h, const float *x, const float *t, int n, f
 CF_API int cf_mlp_get_params(cf_mlp *h, float *params);
 CF_API int cf_mlp_set_params(cf_mlp *h, const float *params);
 CF_API int cf_mlp_stream(cf_mlp *h, void **stream);
+/* Versioned checkpoint of a trained network and its correction weight alpha
+ * (cf_sim_set_network_weight), for reuse across runs.  The reference keeps no
+ * learned state, so the file layout is this library's own: a 56-byte header
+ * (magic "CFPRECN", version 1, widths, alpha, parameter count, FNV-1a hash of
+ * the parameters) and the FP32 parameters.  cf_precond_load creates a new
+ * cf_mlp (max_batch rows, on `device`); a file with a wrong magic, version,
+ * width, size or hash gives CF_EINVAL and creates nothing.  weight may be NULL. */
+CF_API int cf_precond_save(cf_mlp *net, double weight, const char *path);
+CF_API int cf_precond_load(const char *path, int max_batch, int device, cf_mlp **out, double *weight);
 
 /* Learned preconditioner (CF_PRECOND_LEARNED, flexible GMRES): the
  * block-diagonal preconditioner plus a per-filament network correction

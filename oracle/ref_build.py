@@ -32,7 +32,14 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF_ROOT = Path(os.environ.get("CUFIL_REFERENCE_ROOT", "/root/reference"))
+# The reference tree: set by the caller (set_reference_root) or the
+# CUFIL_REFERENCE_ROOT environment variable; without it nothing is built.
+REF_ROOT = Path(os.environ["CUFIL_REFERENCE_ROOT"]) if os.environ.get("CUFIL_REFERENCE_ROOT") else None
+
+
+def set_reference_root(path) -> None:
+    global REF_ROOT
+    REF_ROOT = Path(path) if path else None
 WRAPPER = HERE / "ref_rpy_wrapper.cu"
 
 VARIANTS = {
@@ -58,7 +65,7 @@ def _config_text(switches: dict[str, str]) -> str:
 
 
 def available() -> bool:
-    return (REF_ROOT / "src" / "cilia" / "cuda_functions.cu").exists()
+    return REF_ROOT is not None and (REF_ROOT / "src" / "cilia" / "cuda_functions.cu").exists()
 
 
 FCM_SOURCES = ["CUFCM_SOLVER.cu", "CUFCM_FCM.cu", "CUFCM_CORRECTION.cu", "CUFCM_DATA.cu", "CUFCM_CELLLIST.cu",
@@ -72,6 +79,8 @@ def fcm_lib_path() -> Path:
 
 def build_fcm(verbose: bool = False, force: bool = False) -> Path | None:
     """The reference's cuFCM (src/cufcm, float build, ROTATION 0 as configured) with ref_fcm_wrapper.cu."""
+    if REF_ROOT is None:
+        return None
     src_dir = REF_ROOT / "src" / "cufcm"
     if not (src_dir / "CUFCM_SOLVER.cu").exists():
         return None
@@ -88,6 +97,97 @@ def build_fcm(verbose: bool = False, force: bool = False) -> Path | None:
         subprocess.run(cmd, check=True)
         os.replace(str(lib) + ".tmp", lib)
     return lib
+
+
+# The reference's whole prescribed-cilia step (ref_step_harness.cu drives the
+# reference's own host code).  Each variant edits switches of config.hpp:
+#   step_wgf_f64  the WRITE_GENERALISED_FORCES pre-run, FP64, host RPY back-end
+#   step_dyn_f64  the dynamic run, FP64, host RPY back-end (the whole-step CPU oracle)
+#   step_dyn_gpu  the dynamic run with the reference's own GPU back-end
+#                 (rpy_mobility_solver + Mss_mult), FP32 as the reference ships it
+# All use GMRES tolerance 1e-6 (LINEAR_SYSTEM_TOL) and a Fulford-Blake beat.
+STEP_SWITCHES = {"CILIA_TYPE": "3", "BODY_OR_SURFACE_TYPE": "0", "MOBILITY_TYPE": "1", "LINEAR_SYSTEM_TOL": "1e-6",
+                 "SHAPE_SEQUENCE": "1", "DYNAMIC_PHASE_EVOLUTION": "true", "DYNAMIC_SHAPE_ROTATION": "true",
+                 "INITIAL_CONDITIONS_TYPE": "0", "DISPLAYTIME": "false"}
+STEP_VARIANTS = {
+    "step_wgf_f64": ({"WRITE_GENERALISED_FORCES": "true", "FIL_USE_DOUBLE_PRECISION": "true"}, False),
+    "step_dyn_f64": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "true"}, False),
+    "step_dyn_gpu": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "false"}, True),
+}
+STEP_HOST_CPP = ["src/cilia/mobility/mobility_solver.cpp", "src/cilia/filament.cpp", "src/cilia/swimmer.cpp",
+                 "src/cilia/segment.cpp", "src/cilia/rigid_body.cpp", "src/cilia/broyden_solver.cpp",
+                 "src/general/matrix.cpp", "src/general/quaternion.cpp"]
+STEP_HOST_CU = ["src/cilia/seeding.cu", "src/general/util.cu", "globals.cu"]
+STEP_GPU_CU = ["src/cilia/cuda_functions.cu", "src/cilia/mobility/rpy_mobility_solver.cu"]
+STEP_HARNESS = HERE / "ref_step_harness.cu"
+LAPACK_SHIM = HERE / "lapack_shim.c"
+RPY_ORACLE = HERE / "rpy_oracle.c"
+
+
+def step_path(variant: str) -> Path:
+    return OUT / f"ref_{variant}"
+
+
+def _step_switch_text(extra: dict[str, str]) -> str:
+    text = (REF_ROOT / "config.hpp").read_text()
+    for key, val in {**STEP_SWITCHES, **extra}.items():
+        pat = re.compile(rf"^(\s*)#define {key} \S+", re.M)
+        if not pat.search(text):
+            raise RuntimeError(f"switch {key} not found in the reference config.hpp")
+        text = pat.sub(lambda m: f"{m.group(1)}#define {key} {val}", text, count=1)
+    return text
+
+
+def build_step(verbose: bool = False, force: bool = False) -> list[Path]:
+    """Builds the step-harness variants into oracle/_ref/ (objects under oracle/_ref/obj_<variant>/)."""
+    if not available():
+        return []
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    inc = ["-I", str(REF_ROOT), "-I", str(REF_ROOT / "src" / "cilia"), "-I", str(REF_ROOT / "src" / "cilia" / "mobility"),
+           "-I", str(REF_ROOT / "src" / "general")]
+    arch = ["-gencode", "arch=compute_100a,code=sm_100a"]
+    built = []
+    for name, (extra, gpu) in STEP_VARIANTS.items():
+        odir = OUT / f"obj_{name}"
+        odir.mkdir(parents=True, exist_ok=True)
+        cfg = odir / "config_variant.hpp"
+        text = _step_switch_text(extra)
+        if force or not cfg.exists() or cfg.read_text() != text:
+            cfg.write_text(text)
+        jobs = []  # (source, object, command prefix)
+        for rel in STEP_HOST_CPP:
+            src = REF_ROOT / rel
+            jobs.append((src, odir / (src.stem + ".o"),
+                         ["g++", "-std=c++17", "-O2", "-fopenmp", "-w", "-include", str(cfg), *inc,
+                          "-I", "/usr/local/cuda/include", "-c", str(src)]))
+        for rel in STEP_HOST_CU + (STEP_GPU_CU if gpu else []):
+            src = REF_ROOT / rel
+            jobs.append((src, odir / (src.stem + ".o"),
+                         [nvcc, *arch, "-std=c++17", "-O2", "-w", "-x", "cu", "-include", str(cfg), *inc,
+                          "-c", str(src)]))
+        jobs.append((STEP_HARNESS, odir / "ref_step_harness.o",
+                     [nvcc, *arch, "-std=c++17", "-O2", "-w", "-include", str(cfg), *inc,
+                      *(["-DREF_HARNESS_GPU"] if gpu else []), "-c", str(STEP_HARNESS)]))
+        jobs.append((LAPACK_SHIM, odir / "lapack_shim.o", ["gcc", "-O2", "-std=c11", "-c", str(LAPACK_SHIM)]))
+        if not gpu:
+            jobs.append((RPY_ORACLE, odir / "rpy_oracle_f64.o",
+                         ["gcc", "-O2", "-fopenmp", "-std=c11", "-c", str(RPY_ORACLE)]))
+        objs = []
+        for src, obj, cmd in jobs:
+            objs.append(obj)
+            if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, cfg.stat().st_mtime):
+                if verbose:
+                    print(" ".join(cmd + ["-o", str(obj)]), file=sys.stderr)
+                subprocess.run(cmd + ["-o", str(obj)], check=True)
+        exe = step_path(name)
+        if force or not exe.exists() or exe.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+            cmd = [nvcc, *arch, "-o", str(exe) + ".tmp", *map(str, objs), "-Xcompiler", "-fopenmp", "-lgomp"]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+            os.replace(str(exe) + ".tmp", exe)
+        built.append(exe)
+    return built
 
 
 def build(verbose: bool = False, force: bool = False) -> list[Path]:
@@ -118,9 +218,14 @@ def build(verbose: bool = False, force: bool = False) -> list[Path]:
     fcm = build_fcm(verbose, force)
     if fcm is not None:
         built.append(fcm)
+    built.extend(build_step(verbose, force))
     return built
 
 
 if __name__ == "__main__":
+    # python oracle/ref_build.py REFERENCE_ROOT [--force]
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    if args:
+        set_reference_root(args[0])
     for p in build(verbose=True, force="--force" in sys.argv):
         print(p)

@@ -11,7 +11,7 @@ the beat kinematics, the arclength bisection, the wall RPY mobility and the
 linear solve of that run.  Format: "count v_1 ... v_count" for the forces,
 "steps nseg s_1 ... s_(steps*nseg)" for the arclength table.
 
-Run: python tests/golden/make_golden.py [reference_root]
+Run: python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import sys
 from pathlib import Path
@@ -37,7 +37,7 @@ def read_table(p):
     return t
 
 
-def main(root="/root/reference"):
+def main(root):
     d = Path(root) / "input" / "forcing"
     tag = "NSEG=20_SEP=2.600000.dat"
     arrays = {
@@ -52,4 +52,6 @@ def main(root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+    main(sys.argv[1])

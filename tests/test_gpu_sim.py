@@ -42,7 +42,7 @@ def make_pair(nx, spacing, s_table, seed=0, **kw):
     tol = args.pop("gmres_tol", 1e-6)
     gpu = WallCiliaSimulation(bases=bases, gmres_tol=tol, **args)
     cpu = implicit.WallCilia(bases=bases, shape_sequence=1, gmres_tol=tol,
-                             **{k: v for k, v in args.items() if k not in ("beat",)})
+                             **{k: v for k, v in args.items() if k not in ("beat", "precond")})
     return gpu, cpu
 
 
@@ -175,3 +175,62 @@ def test_step_io_equals_separate_calls(s_table):
         xb, fb = gpu_b.segments()
         np.testing.assert_array_equal(x, xb)
         np.testing.assert_array_equal(f, fb)
+
+
+@pytest.mark.parametrize("precond", [_lib.CF_PRECOND_BLOCK_DIAG, _lib.CF_PRECOND_LINE])
+def test_solve_on_given_rhs_matches_oracle(s_table, precond):
+    # cf_sim_solve on a random RHS for the geometry of step 0, against the dense FP64 solve of the
+    # oracle's operator (system_matrix_mult_new restated): FP64 true residual below the solver
+    # tolerance plus the FP32 mobility contract, twice (cold start, then the solution as the guess).
+    gpu, cpu = make_pair(3, 30.0, s_table, seed=11, precond=precond)
+    with gpu:
+        gpu.initial_guess(0)
+        cpu.initial_guess(0)
+        n = cpu.size
+        A = np.stack([cpu.matvec(e) for e in np.eye(n)], axis=1)
+        rhs = np.random.default_rng(2).standard_normal(n)
+        x_exact = np.linalg.solve(A, rhs)
+        with pytest.raises(_lib.CufilError):
+            gpu.solve_linear_system(rhs, tol=1e-6, max_iter=10_000)   # cap above the handle's
+        x, res = gpu.solve_linear_system(rhs, tol=1e-6)
+        assert res.status == _lib.CF_OK and res.relative_residual <= 1e-6
+        assert np.linalg.norm(rhs - A @ x) / np.linalg.norm(rhs) < 2e-5
+        assert np.linalg.norm(x - x_exact) / np.linalg.norm(x_exact) < 1e-3
+        st = gpu.state()
+        np.testing.assert_array_equal(st["phase_dot"], x[3 * cpu.nseg_total:3 * cpu.nseg_total + cpu.nfil])
+        x2, res2 = gpu.solve_linear_system(rhs, x0=x, tol=1e-6)
+        assert res2.iterations == 0 and np.array_equal(x2, x)
+        _, res3 = gpu.solve_linear_system(rhs, tol=1e-12, max_iter=3)
+        assert res3.status == _lib.CF_NOT_CONVERGED and res3.iterations == 3
+
+
+TIPS = np.load(Path(__file__).resolve().parent / "golden" / "ref_tips_16x16_80a.npz")
+
+
+@pytest.mark.parametrize("precond", [_lib.CF_PRECOND_BLOCK_DIAG, _lib.CF_PRECOND_LINE])
+def test_300_steps_of_256_cilia_follow_the_reference_trajectory(precond):
+    # 256 cilia x 20 segments on a 16 x 16 lattice at 80a for 300 implicit steps (one beat period)
+    # against the reference's own step code in FP64 (tests/golden/make_tip_golden.py).  At 80a no
+    # segments of different cilia come within 19a of each other, so the saddle system stays well
+    # posed and the trajectory is not chaotic: the FP32 pair sums of the engine then move the tips
+    # by at most TIP_TOL of the filament length over the whole period.
+    TIP_TOL = 2e-4
+    nx = int(TIPS["nx"])
+    F = nx * nx
+    bases = workloads.lattice_bases(F, nx, float(TIPS["spacing"]), 1.3)
+    with WallCiliaSimulation(bases=bases, nseg=20, seg_sep=2.6, dt=1 / 300, phase0=TIPS["phase0"],
+                             angle0=TIPS["angle0"], spring_factor=0.01, phase_refs=GOLD["fb_phase"],
+                             angle_refs=GOLD["fb_angle"], s_table=TIPS["s_table"], gmres_tol=1e-6,
+                             precond=precond) as gpu:
+        L = 2.6 * 19
+        saved = list(TIPS["saved_steps"])
+        worst_tip = worst_phase = 0.0
+        for nt in range(int(TIPS["steps"])):
+            res = gpu.step(nt)
+            assert res.status == _lib.CF_OK and res.relative_residual <= 1e-6
+            if nt in saved:
+                q = saved.index(nt)
+                worst_tip = max(worst_tip, np.abs(gpu.tips() - TIPS["tips"][q]).max() / L)
+                worst_phase = max(worst_phase, np.abs(gpu.state()["phase"] - TIPS["phase"][q]).max())
+        print(f"256 cilia x 300 steps: worst tip error {worst_tip:.2e} L, worst phase error {worst_phase:.2e}")
+        assert worst_tip < TIP_TOL and worst_phase < 2 * np.pi * TIP_TOL

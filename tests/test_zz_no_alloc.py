@@ -60,3 +60,27 @@ def test_noalloc_rejects_sizes_beyond_its_limit(cuda):
                                                    ctypes.c_void_p(v.data_ptr()), n, None)
     assert rc == _lib.CF_EINVAL
     assert "8192" in _lib.last_error()
+
+
+def test_noalloc_given_up_wait_gives_nan_then_recovers(cuda):
+    # The entry point never synchronises, so a bounded wait that gives up
+    # (forced here by the cf_set_wait_limit test hook) shows as NaN outputs,
+    # never as stale partial sums of an earlier call; the next call with the
+    # default limit is correct again.
+    torch = cuda
+    x = workloads.vertical_lattice(4, 4, 20).astype(np.float32)
+    n = x.shape[0]
+    xd = torch.as_tensor(x.ravel(), device="cuda")
+    f = np.zeros((n, 6), np.float32)
+    f[:, :3] = workloads.random_forces(n, 3, seed=4)
+    fd = torch.as_tensor(f.ravel(), device="cuda")
+    good = _noalloc(torch, xd, fd, n)
+    try:
+        _lib.call("cf_set_wait_limit", 0)
+        bad = _noalloc(torch, xd, fd, n)
+    finally:
+        _lib.call("cf_set_wait_limit", 0xFFFFFFFF)
+    assert np.all(np.isnan(bad))
+    again = _noalloc(torch, xd, fd, n)
+    np.testing.assert_array_equal(again, good)
+
