@@ -122,6 +122,9 @@ SIGNATURES = {
     "cf_sim_assemble_rhs": [_vp, _i, _vp],
     "cf_sim_apply_preconditioner": [_vp, _vp, _vp],
     "cf_sim_system_matvec": [_vp, _vp, _vp],
+    "cf_sim_write_data": [_vp, _i, _d, ctypes.c_char_p],
+    "cf_sim_write_config": [_vp, ctypes.c_char_p, _i],
+    "cf_read_ic": [ctypes.c_char_p, _i, _vp, _vp, _vp],
     "cf_sim_solve": [_vp, _vp, _vp, _d, _i, ctypes.POINTER(_i), ctypes.POINTER(_d)],
     "cf_sim_autotune": [_vp, _i, _vp],
     "cf_sim_refresh_preconditioner": [_vp],

@@ -1649,3 +1649,152 @@ extern "C" int cf_batch_get_tuning(cf_batch *bt, int *choice) {
     engine_get_tuning(bt, choice);
     return CF_OK;
 }
+
+// =================================================================== files
+// The reference's data files for a wall of prescribed cilia, so that its
+// sweep drivers (pyfile/find_periodic, pyfile/bisection) read this engine's
+// output as they read the reference's.  Line formats follow
+// cilia_sim_main.cu:624-718, swimmer.cpp:1144-1158, filament.cpp:2210-2226,
+// rigid_body.cpp:565-569 and mobility_solver.cpp:3150-3279; the initial
+// condition file is read as filament.cpp:310-340 reads it.  States are FP64
+// here, so they are written with 15 significant digits (the reference's
+// OUTPUT_DIGIT of its FP64 build); velocities and forces with 10, as there.
+namespace {
+
+struct LineFile {
+    std::FILE *f = nullptr;
+    explicit LineFile(const std::string &path) { f = std::fopen(path.c_str(), "a"); }
+    ~LineFile() {
+        if (f) std::fclose(f);
+    }
+    void lead(long long k) { std::fprintf(f, "%lld ", k); }
+    void num(double v, int digits) { std::fprintf(f, "%.*e ", digits, v); }
+    bool end() {
+        std::fputc('\n', f);
+        return std::ferror(f) == 0;
+    }
+};
+
+int open_all(const std::string &prefix, const char *const *suffixes, int n, std::vector<LineFile *> &out) {
+    for (int i = 0; i < n; ++i) {
+        auto *lf = new LineFile(prefix + suffixes[i]);
+        out.push_back(lf);
+        if (!lf->f) return set_error(CF_EINVAL, "cf_sim_write_data: cannot open %s%s", prefix.c_str(), suffixes[i]);
+    }
+    return CF_OK;
+}
+
+}  // namespace
+
+extern "C" int cf_sim_write_data(cf_sim *s, int save_step, double period, const char *prefix) {
+    clear_error();
+    CF_REQUIRE(s && prefix, "cf_sim_write_data: null argument");
+    CF_REQUIRE(s->B == 1, "cf_sim_write_data: one array per handle");
+    CF_REQUIRE(s->geometry > 0, "cf_sim_write_data: no step has run yet");
+    CF_CUDA(cudaSetDevice(s->device));
+    const ArrayInfo a = s->arr[0];
+    const int F = a.F, N = a.N, nseg = s->d.nseg;
+    std::vector<double> phase(F), angle(F), pd(F), ad(F), x(3 * static_cast<size_t>(N)), sol(a.n), av(a.n);
+    std::vector<double> kp(3 * static_cast<size_t>(N)), ka(3 * static_cast<size_t>(N));
+    CF_TRY(copy_state_out(s, phase.data(), angle.data(), pd.data(), ad.data()));
+    CF_CUDA(cudaMemcpyAsync(x.data(), s->d.xd, x.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CF_CUDA(cudaMemcpyAsync(sol.data(), s->d.sol, sol.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CF_CUDA(cudaMemcpyAsync(kp.data(), s->d.kp, kp.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CF_CUDA(cudaMemcpyAsync(ka.data(), s->d.ka, ka.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CF_CUDA(cudaStreamSynchronize(s->stream));
+    // Segment velocities as the reference writes them: M applied to the solution's
+    // constraint forces (mobility_solver.cpp:3154-3156 recomputes the product
+    // before writing), i.e. the lambda rows of A sol plus the rate terms.
+    CF_TRY(cf_sim_system_matvec(s, sol.data(), av.data()));
+    const char *suffixes[] = {"_seg_states.dat", "_body_states.dat", "_true_states.dat", "_seg_vels.dat",
+                              "_seg_forces.dat"};
+    std::vector<LineFile *> files;
+    int rc = open_all(prefix, suffixes, 5, files);
+    if (rc == CF_OK) {
+        LineFile &seg = *files[0], &body = *files[1], &tru = *files[2], &vel = *files[3], &frc = *files[4];
+        seg.lead(save_step);
+        for (size_t i = 0; i < x.size(); ++i) seg.num(x[i], 15);
+        body.lead(save_step);  // the wall case has no moving body: at the origin, identity orientation
+        for (double v : {0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0}) body.num(v, 15);
+        tru.lead(save_step);
+        tru.num(period, 15);
+        for (int m = 0; m < F; ++m) tru.num(phase[m], 15);
+        if (s->d.dyn_angle)
+            for (int m = 0; m < F; ++m) tru.num(angle[m], 15);
+        vel.lead(save_step);
+        frc.lead(save_step);
+        for (int i = 0; i < N; ++i) {
+            const int m = i / nseg;
+            for (int c = 0; c < 3; ++c) {
+                double v = av[3 * i + c];
+                if (a.po >= 0) v += kp[3 * i + c] * sol[a.po + m];
+                if (a.ao >= 0) v += ka[3 * i + c] * sol[a.ao + m];
+                vel.num(v, 10);
+            }
+            for (int c = 0; c < 3; ++c) vel.num(0.0, 10);
+            for (int c = 0; c < 3; ++c) frc.num(sol[3 * i + c], 10);
+            for (int c = 0; c < 3; ++c) frc.num(0.0, 10);
+        }
+        for (LineFile *lf : files)
+            if (!lf->end()) rc = set_error(CF_EINVAL, "cf_sim_write_data: write under %s failed", prefix);
+    }
+    for (LineFile *lf : files) delete lf;
+    return rc;
+}
+
+extern "C" int cf_sim_write_config(cf_sim *s, const char *prefix, int total_steps) {
+    clear_error();
+    CF_REQUIRE(s && prefix, "cf_sim_write_config: null argument");
+    CF_REQUIRE(s->B == 1, "cf_sim_write_config: one array per handle");
+    CF_CUDA(cudaSetDevice(s->device));
+    const cf_sim_config &c = s->common;
+    const int F = s->arr[0].F, nseg = s->d.nseg;
+    std::vector<double> base(3 * static_cast<size_t>(F));
+    CF_CUDA(cudaMemcpy(base.data(), s->d.base, base.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    const std::string p(prefix);
+    // swimmer::write_reference_positions (swimmer.cpp:1114-1127): the filament base positions on one line
+    std::FILE *f = std::fopen((p + "_fil_references.dat").c_str(), "w");
+    if (!f) return set_error(CF_EINVAL, "cf_sim_write_config: cannot open %s_fil_references.dat", prefix);
+    for (double v : base) std::fprintf(f, "%.15g ", v);
+    std::fputc('\n', f);
+    const bool ok1 = std::fclose(f) == 0;
+    // The .par summary of cilia_sim_main.cu:178-232 (prescribed cilia)
+    f = std::fopen((p + ".par").c_str(), "w");
+    if (!f) return set_error(CF_EINVAL, "cf_sim_write_config: cannot open %s.par", prefix);
+    const double dl = c.seg_sep, L = dl * (nseg - 1);
+    std::fprintf(f, "%d %%%% NFIL\n%d %%%% NSEG\n%d %%%% NSWIM\n%d %%%% NBLOB\n", F, nseg, 1, 0);
+    std::fprintf(f, "%.15g %%%% MU\n%.15g %%%% RSEG\n%.15g %%%% DL\n%.15g %%%% FIL_LENGTH\n", 1.0, 1.0, dl, L);
+    std::fprintf(f, "%.15g %%%% RBLOB\n%.15g %%%% KB\n%.15g %%%% KT\n", 1.0, 1800.0, 1800.0);
+    std::fprintf(f, "%.15g %%%% TOL\n%d %%%% TOTAL_TIME_STEPS\n%.15g %%%% DT\n", c.gmres_tol, total_steps, c.dt);
+    std::fprintf(f, "%d %%%% PLOT_FREQUENCY_IN_STEPS\n%d %%%% STEPS_PER_PERIOD\n", 10, 300);
+    std::fprintf(f, "%d %%%% PRESCRIBED_CILIA\n", 1);
+    if (s->d.dyn_angle) std::fprintf(f, "%.15g %%%% TORSIONAL_SPRING_MAGNITUDE_FACTOR\n", c.spring_factor);
+    const bool ok2 = std::fclose(f) == 0;
+    if (!ok1 || !ok2) return set_error(CF_EINVAL, "cf_sim_write_config: write under %s failed", prefix);
+    return CF_OK;
+}
+
+extern "C" int cf_read_ic(const char *path, int n_fil, double *header, double *phase, double *angle) {
+    clear_error();
+    CF_REQUIRE(path && n_fil > 0 && phase && angle, "cf_read_ic: bad arguments");
+    std::FILE *f = std::fopen(path, "r");
+    if (!f) return set_error(CF_EINVAL, "cf_read_ic: cannot open %s", path);
+    double h[2] = {0.0, 0.0};
+    std::vector<double> v(2 * static_cast<size_t>(n_fil));
+    int got = 0;
+    for (int i = 0; i < 2 && std::fscanf(f, "%lf", &h[i]) == 1; ++i) ++got;
+    size_t nv = 0;
+    while (got == 2 && nv < v.size() && std::fscanf(f, "%lf", &v[nv]) == 1) ++nv;
+    std::fclose(f);
+    if (got < 2 || nv < v.size())
+        return set_error(CF_EINVAL,
+                         "cf_read_ic: %s holds %zu of the 2 + %d values (2 header values, %d phases, %d angles)",
+                         path, got + nv, 2 * n_fil, n_fil, n_fil);
+    if (header) {
+        header[0] = h[0];
+        header[1] = h[1];
+    }
+    std::memcpy(phase, v.data(), sizeof(double) * n_fil);
+    std::memcpy(angle, v.data() + n_fil, sizeof(double) * n_fil);
+    return CF_OK;
+}

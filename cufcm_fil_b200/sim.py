@@ -152,6 +152,15 @@ class WallCiliaSimulation:
         _lib.call("cf_sim_system_matvec", self._h, _p(v), _p(out))
         return out
 
+    def write_data(self, save_step: int, period: float, prefix: str) -> None:
+        """Appends the reference's data files <prefix>_{seg_states,body_states,true_states,seg_vels,seg_forces}.dat
+        (cf_sim_write_data)."""
+        _lib.call("cf_sim_write_data", self._h, int(save_step), float(period), str(prefix).encode())
+
+    def write_config(self, prefix: str, total_steps: int) -> None:
+        """<prefix>_fil_references.dat and <prefix>.par (cf_sim_write_config)."""
+        _lib.call("cf_sim_write_config", self._h, str(prefix).encode(), int(total_steps))
+
     def solve_linear_system(self, rhs, x0=None, tol: float = 1e-6, max_iter: int = 350):
         """GMRES on a given RHS for the current geometry (cf_sim_solve); returns (x, GmresResult).
         The solution becomes the next step's warm start and its rate rows the filament rates."""

@@ -315,6 +315,25 @@ CF_API int cf_sim_system_matvec(cf_sim *s, const double *in, double *out);
 CF_API int cf_sim_solve(cf_sim *s, const double *rhs, double *x_inout, double tol, int max_iter, int *iters,
                         double *relres);
 
+/* The reference's data files, appended as its main loop appends them every
+ * PLOT_FREQUENCY_IN_STEPS steps (cilia_sim_main.cu:624-718,
+ * mobility_solver.cpp:3150-3279): <prefix>_seg_states.dat (segment centres),
+ * _body_states.dat (the wall case's fixed body), _true_states.dat
+ * ("step period phases angles", what pyfile/find_periodic and
+ * pyfile/bisection read), _seg_vels.dat (M applied to the constraint forces,
+ * six slots per segment) and _seg_forces.dat (six slots per segment), each
+ * line led by save_step.  Call after a step. */
+CF_API int cf_sim_write_data(cf_sim *s, int save_step, double period, const char *prefix);
+/* <prefix>_fil_references.dat (filament base positions,
+ * swimmer.cpp:1114-1127) and <prefix>.par (cilia_sim_main.cu:178-232). */
+CF_API int cf_sim_write_config(cf_sim *s, const char *prefix, int total_steps);
+/* The initial-condition file in the reference's psi.dat layout
+ * (filament.cpp:310-340): two header values (the sweep drivers write the
+ * spring constant and the period there; header may be NULL), then n_fil
+ * phases, then n_fil shape-rotation angles.  A file with fewer values gives
+ * CF_EINVAL (the reference silently keeps its defaults).  No GPU needed. */
+CF_API int cf_read_ic(const char *path, int n_fil, double *header, double *phase, double *angle);
+
 /* Launch shapes of the iteration kernels: choice[5] = {pair-kernel CTAs per
  * SM, dot-product row chunk, dot-product blocks per SM, update blocks per SM,
  * update tile rows (32, 64, 128 or 256)}.

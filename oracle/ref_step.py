@@ -79,11 +79,13 @@ class RefRun:
     phase_dot: np.ndarray
     angle_dot: np.ndarray
     tips: np.ndarray         # [steps, F, 3] last segment of each filament
+    files: dict | None = None  # data file suffix -> text, when run(write=True)
 
 
 def run(*, nfil: int, fil_x_dim: int, spacing: float, phase0, angle0, steps: int, phase_refs, angle_refs,
         s_table, nseg: int = 20, seg_sep: float = 2.6, spring_factor: float = 0.01,
-        variant: str = "step_dyn_f64", timeout: float = 3600.0, budget: float | None = None) -> RefRun:
+        variant: str = "step_dyn_f64", timeout: float = 3600.0, budget: float | None = None,
+        write: bool = False) -> RefRun:
     """Dynamic run of the reference's step on an nfil lattice (fil_x_dim columns, spacing in radii).
     With `budget` (seconds) the run is stopped after that time and the steps finished so far are returned."""
     F = int(nfil)
@@ -100,6 +102,8 @@ def run(*, nfil: int, fil_x_dim: int, spacing: float, phase0, angle0, steps: int
         (d / "psi.dat").write_text("0 0 " + " ".join(repr(float(x)) for x in ic))
         cmd = [str(binary(variant)), "run", str(nseg), str(F), str(int(fil_x_dim)), repr(float(spacing)),
                repr(float(seg_sep)), repr(float(spring_factor)), str(int(steps)), "psi.dat", "out.bin"]
+        if write:
+            cmd.append("write")
         if budget is None:
             subprocess.run(cmd, cwd=d, check=True, capture_output=True, timeout=timeout)
         else:
@@ -110,6 +114,9 @@ def run(*, nfil: int, fil_x_dim: int, spacing: float, phase0, angle0, steps: int
         width = 2 + 7 * F
         raw = np.fromfile(d / "out.bin") if (d / "out.bin").exists() else np.zeros(0)
         rec = raw[:raw.size // width * width].reshape(-1, width)
-    return RefRun(iterations=rec[:, 0].astype(int), seconds=rec[:, 1], phase=rec[:, 2:2 + F],
+        files = None
+        if write:
+            files = {p.name[len("ref_step"):]: p.read_text() for p in d.glob("ref_step_*.dat")}
+    return RefRun(files=files, iterations=rec[:, 0].astype(int), seconds=rec[:, 1], phase=rec[:, 2:2 + F],
                   angle=rec[:, 2 + F:2 + 2 * F], phase_dot=rec[:, 2 + 2 * F:2 + 3 * F],
                   angle_dot=rec[:, 2 + 3 * F:2 + 4 * F], tips=rec[:, 2 + 4 * F:].reshape(-1, F, 3))

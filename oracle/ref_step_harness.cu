@@ -30,9 +30,13 @@
 //       the WRITE_GENERALISED_FORCES pre-run (binary built with that switch):
 //       writes input/forcing/..._{phase,angle}_generalised_forces_... and
 //       ..._s_values_... exactly as the reference does.
-//   ref_step_* run  <nseg> <nfil> <fil_x_dim> <spacing> <seg_sep> <spring> <steps> <ic_file> <out.bin>
+//   ref_step_* run  <nseg> <nfil> <fil_x_dim> <spacing> <seg_sep> <spring> <steps> <ic_file> <out.bin> [write]
 //       the dynamic run.  out.bin: per step, doubles
 //       [iterations, seconds, phase[F], angle[F], phase_dot[F], angle_dot[F], x_tip[3F]].
+//       With "write", the reference's data files (ref_step_seg_states.dat, _body_states.dat,
+//       _true_states.dat, _seg_vels.dat, _seg_forces.dat) are appended every
+//       PLOT_FREQUENCY_IN_STEPS steps by the reference's own writers, as its main loop does
+//       (cilia_sim_main.cu:624-718).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -165,6 +169,11 @@ void set_globals(int nseg, int nfil, double fil_x_dim, double spacing, double se
     SIMULATION_FILE = "ref_step";
     SIMULATION_ICSTATE_NAME = ic_file;
     SIMULATION_NAME = SIMULATION_DIR + SIMULATION_FILE;
+    SIMULATION_SEG_STATE_NAME = SIMULATION_NAME + "_seg_states.dat";
+    SIMULATION_BODY_STATE_NAME = SIMULATION_NAME + "_body_states.dat";
+    SIMULATION_SEG_VEL_NAME = SIMULATION_NAME + "_seg_vels.dat";
+    SIMULATION_SEG_FORCES_NAME = SIMULATION_NAME + "_seg_forces.dat";
+    SIMULATION_TRUESTATE_NAME = SIMULATION_NAME + "_true_states.dat";
 #if WRITE_GENERALISED_FORCES
     NSWIM = 1;
     NFIL = 1;
@@ -200,7 +209,8 @@ int main(int argc, char **argv) {
     set_globals(std::atoi(argv[2]), 1, 1, 1, std::atof(argv[3]), 0, STEPS_PER_PERIOD, "none");
     out_name = argv[4];
 #else
-    if (mode != "run" || argc != 11) usage();
+    if (mode != "run" || (argc != 11 && argc != 12)) usage();
+    const bool write_files = argc == 12 && std::string(argv[11]) == "write";
     set_globals(std::atoi(argv[2]), std::atoi(argv[3]), std::atof(argv[4]), std::atof(argv[5]), std::atof(argv[6]),
                 std::atof(argv[7]), std::atoi(argv[8]), argv[9]);
     out_name = argv[10];
@@ -276,6 +286,27 @@ int main(int argc, char **argv) {
             for (int c = 0; c < 3; c++)
                 rec[2 + 4 * F + 3 * m + c] = mobility.x_segs_host[3 * (m * NSEG + NSEG - 1) + c];
         }
+#if !WRITE_GENERALISED_FORCES
+        if (write_files && nt % PLOT_FREQUENCY_IN_STEPS == 0) {
+            // The reference's writers in its main loop's order (cilia_sim_main.cu:628-700); prescribed
+            // cilia save the step index itself (explicit description).
+            std::ofstream seg_state_file(SIMULATION_SEG_STATE_NAME, std::ios::app);
+            seg_state_file << nt << " " << std::scientific << std::setprecision(OUTPUT_DIGIT);
+            std::ofstream body_state_file(SIMULATION_BODY_STATE_NAME, std::ios::app);
+            body_state_file << nt << " " << std::scientific << std::setprecision(OUTPUT_DIGIT);
+            for (int n = 0; n < NSWIM; n++) swimmers[n].write_data(seg_state_file, body_state_file);
+            seg_state_file << std::endl;
+            body_state_file << std::endl;
+            mobility.write_data(nt, swimmers);
+            std::ofstream true_states_file(SIMULATION_TRUESTATE_NAME, std::ios::app);
+            true_states_file << std::scientific << std::setprecision(OUTPUT_DIGIT) << nt << " " << PERIOD << " ";
+            for (int n = 0; n < NSWIM; n++)
+                for (int m = 0; m < NFIL; m++) true_states_file << swimmers[n].filaments[m].phase << " ";
+            for (int n = 0; n < NSWIM; n++)
+                for (int m = 0; m < NFIL; m++) true_states_file << swimmers[n].filaments[m].shape_rotation_angle << " ";
+            true_states_file << std::endl;
+        }
+#endif
         for (int i = 0; i < NSWIM; i++) swimmers[i].end_of_step(nt);
         rec[1] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::fwrite(rec.data(), sizeof(double), rec.size(), out);
