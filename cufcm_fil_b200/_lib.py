@@ -67,6 +67,12 @@ class FcmConfig(ctypes.Structure):
                 ("boxsize", ctypes.c_double), ("device", ctypes.c_int)]
 
 
+class FlowConfig(ctypes.Structure):
+    _fields_ = [("max_flow", ctypes.c_int), ("max_seg", ctypes.c_int), ("max_blob", ctypes.c_int),
+                ("max_bodies", ctypes.c_int), ("mu", ctypes.c_double), ("remove_net_force", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _d = ctypes.c_double
@@ -101,6 +107,10 @@ SIGNATURES = {
     "cf_fcm_info": [_vp, _vp],
     "cf_fcm_set_timing": [_vp, _i],
     "cf_fcm_stage_times": [_vp, _vp],
+    "cf_flow_create": [ctypes.POINTER(FlowConfig), ctypes.POINTER(_vp)],
+    "cf_flow_destroy": [_vp],
+    "cf_flow_velocities": [_vp, _vp, _i, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp],
+    "cf_flow_velocities_device": [_vp, _vp, _i, _vp, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp],
     "cf_sim_create": [ctypes.POINTER(SimConfig), ctypes.POINTER(_vp)],
     "cf_sim_destroy": [_vp],
     "cf_sim_step": [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_d)],

@@ -186,6 +186,37 @@ CF_API int cf_fcm_stage_times(cf_fcm *h, float *ms);
 /* Derived parameters: [ngd, dx, sigma, Sigma, Rc, Mx, My, Mz, self mobility] */
 CF_API int cf_fcm_info(cf_fcm *h, double *info);
 
+/* ========================================================== flow field ==
+ * Flow velocities at field points from saved segment and blob forces: the
+ * reference's flow-field post-processor (src/flow_field/flow_field_evaluator.cu,
+ * flow_velocities :13-217, prefactor 1/(8 pi mu) :545-557).  Per flow point:
+ * a Stokeslet per segment force with Blake's image system of a wall at z = 0
+ * when the data has no blobs (n_blob_per_body == 0), a rotlet per segment
+ * torque, a Stokeslet per blob force, and with remove_net_force minus a
+ * Stokeslet of every source's force at its body's position.  Layouts are the
+ * reference's: x_flow [3 n_flow], x_segs [3 n_seg], f_segs [6 n_seg] (force,
+ * torque), x_blobs / f_blobs [3 n_blob], x_bodies [3 n_bodies] with segment j
+ * on body j / n_seg_per_body and blob k on body k / n_blob_per_body.  A flow
+ * point on a source gives non-finite values, as in the reference. */
+typedef struct cf_flow cf_flow;
+typedef struct cf_flow_config {
+    int max_flow, max_seg, max_blob, max_bodies;  /* capacities */
+    double mu;                                     /* MU */
+    int remove_net_force;                          /* REMOVE_NET_FORCE_STOKESLET */
+    int device;
+} cf_flow_config;
+CF_API int cf_flow_create(const cf_flow_config *cfg, cf_flow **out);
+CF_API int cf_flow_destroy(cf_flow *h);
+/* Host arrays in, host velocities out (synchronous). */
+CF_API int cf_flow_velocities(cf_flow *h, const float *x_flow, int n_flow, const float *x_segs, const float *f_segs,
+                              int n_seg, int n_seg_per_body, const float *x_blobs, const float *f_blobs, int n_blob,
+                              int n_blob_per_body, const float *x_bodies, float *v_flow);
+/* Same on device arrays, asynchronous on `stream` (NULL: the legacy default stream). */
+CF_API int cf_flow_velocities_device(cf_flow *h, const float *d_x_flow, int n_flow, const float *d_x_segs,
+                                     const float *d_f_segs, int n_seg, int n_seg_per_body, const float *d_x_blobs,
+                                     const float *d_f_blobs, int n_blob, int n_blob_per_body,
+                                     const float *d_x_bodies, float *d_v_flow, void *stream);
+
 /* ========================================================== simulation ==
  * Generic layer of mobility_solver for prescribed-shape cilia above a no-slip
  * wall (CILIA_TYPE 3, BODY_OR_SURFACE_TYPE 0, MOBILITY_TYPE 1,

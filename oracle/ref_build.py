@@ -190,6 +190,54 @@ def build_step(verbose: bool = False, force: bool = False) -> list[Path]:
     return built
 
 
+FLOW_WRAPPER = HERE / "ref_flow_wrapper.cu"
+
+
+def flow_lib_path() -> Path:
+    return OUT / "libref_flow.so"
+
+
+def build_flow(verbose: bool = False, force: bool = False) -> Path | None:
+    """The reference's flow_velocities kernel (src/flow_field/flow_field_evaluator.cu) in FP64, with the
+    reference's matrix/quaternion sources it links against and the BLAS/LAPACK shim."""
+    if not available():
+        return None
+    src = REF_ROOT / "src" / "flow_field" / "flow_field_evaluator.cu"
+    if not src.exists():
+        return None
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    odir = OUT / "obj_flow"
+    odir.mkdir(parents=True, exist_ok=True)
+    cfg = odir / "config_variant.hpp"
+    text = _step_switch_text({"FIL_USE_DOUBLE_PRECISION": "true", "WRITE_GENERALISED_FORCES": "false"})
+    if force or not cfg.exists() or cfg.read_text() != text:
+        cfg.write_text(text)
+    inc = ["-I", str(REF_ROOT), "-I", str(REF_ROOT / "src" / "general"), "-I", str(REF_ROOT / "src" / "flow_field")]
+    jobs = [(REF_ROOT / "src" / "general" / "matrix.cpp", odir / "matrix.o",
+             ["g++", "-std=c++17", "-O2", "-fPIC", "-w", "-include", str(cfg), *inc, "-c"]),
+            (REF_ROOT / "src" / "general" / "quaternion.cpp", odir / "quaternion.o",
+             ["g++", "-std=c++17", "-O2", "-fPIC", "-w", "-include", str(cfg), *inc, "-c"]),
+            (LAPACK_SHIM, odir / "lapack_shim.o", ["gcc", "-O2", "-fPIC", "-std=c11", "-c"]),
+            (FLOW_WRAPPER, odir / "ref_flow_wrapper.o",
+             [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-w", "-Xcompiler", "-fPIC",
+              "-include", str(cfg), *inc, "-c"])]
+    objs = []
+    for s_, o_, cmd in jobs:
+        objs.append(o_)
+        newest = max(s_.stat().st_mtime, cfg.stat().st_mtime, src.stat().st_mtime)
+        if force or not o_.exists() or o_.stat().st_mtime < newest:
+            if verbose:
+                print(" ".join(cmd + [str(s_), "-o", str(o_)]), file=sys.stderr)
+            subprocess.run(cmd + [str(s_), "-o", str(o_)], check=True)
+    lib = flow_lib_path()
+    if force or not lib.exists() or lib.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(lib) + ".tmp",
+               *map(str, objs)]
+        subprocess.run(cmd, check=True)
+        os.replace(str(lib) + ".tmp", lib)
+    return lib
+
+
 def build(verbose: bool = False, force: bool = False) -> list[Path]:
     """Builds every variant; a no-op returning [] when the reference tree is absent."""
     if not available():
@@ -219,6 +267,9 @@ def build(verbose: bool = False, force: bool = False) -> list[Path]:
     if fcm is not None:
         built.append(fcm)
     built.extend(build_step(verbose, force))
+    flow = build_flow(verbose, force)
+    if flow is not None:
+        built.append(flow)
     return built
 
 
