@@ -27,6 +27,7 @@ CF_PRECOND_NONE = 0
 CF_PRECOND_BLOCK_DIAG = 1
 CF_PRECOND_LEARNED = 2
 CF_PRECOND_LINE = 3
+CF_PRECOND_LEARNED_LINE = 4
 
 _STATUS_NAMES = {0: "CF_OK", 1: "CF_EINVAL", 2: "CF_ENOMEM", 3: "CF_ECUDA", 4: "CF_NOT_CONVERGED",
                  5: "CF_NONFINITE", 6: "CF_TIMEOUT", 7: "CF_ENOTSUP"}

@@ -9,7 +9,8 @@
 //            (the beat direction, where the hydrodynamic coupling is strongest),
 // and, unscaled, its segment positions relative to its base divided by the
 // filament length.  Its output delta_m (3*nseg + 2 values) corrects the
-// block-diagonal preconditioner:  z_m = P_bd(r)_m + s_m delta_m.
+// block-diagonal preconditioner (CF_PRECOND_LEARNED) or the line-patch
+// preconditioner (CF_PRECOND_LEARNED_LINE):  z_m = P(r)_m + s_m delta_m.
 // Training pairs come from the plain solver itself: after each Arnoldi
 // product w = A z (z = P_bd(q)) the features of w and the target
 // (z_m - P_bd(w)_m) / s_m are stored, so that the network learns the part of
@@ -68,8 +69,9 @@ __global__ void learned_features_kernel(SimDev d, const double *v, float *X, flo
     }
 }
 
-// Z_k += s_m delta_m (the current basis index k), copied to z; one block per filament.
-__global__ void learned_correct_kernel(SimDev d, const float *Y, const float *scale) {
+// Z_k = P(Q_k) + s_m delta_m (the current basis index k), copied to z; P(Q_k) is Z_k itself (block-diagonal
+// base) or z (line-patch base, base_z).  One block per filament.
+__global__ void learned_correct_kernel(SimDev d, const float *Y, const float *scale, int base_z) {
     const int m = blockIdx.x;
     const FilRows fr = fil_rows(d, m);
     if (!d.active[fr.b]) return;
@@ -79,19 +81,20 @@ __global__ void learned_correct_kernel(SimDev d, const float *Y, const float *sc
     const int nl = 3 * d.nseg;
     const double s = d.lalpha * scale[m];
     const float *y = Y + static_cast<size_t>(m) * d.lout;
+    const double *base = base_z ? d.z : zk;
     for (int j = threadIdx.x; j < nl; j += blockDim.x) {
-        const double val = zk[fr.lam + j] + s * y[j];
+        const double val = base[fr.lam + j] + s * y[j];
         zk[fr.lam + j] = val;
         d.z[fr.lam + j] = val;
     }
     if (threadIdx.x == 0) {
         if (fr.pr >= 0) {
-            const double val = zk[fr.pr] + s * y[nl];
+            const double val = base[fr.pr] + s * y[nl];
             zk[fr.pr] = val;
             d.z[fr.pr] = val;
         }
         if (fr.ar >= 0) {
-            const double val = zk[fr.ar] + s * y[nl + 1];
+            const double val = base[fr.ar] + s * y[nl + 1];
             zk[fr.ar] = val;
             d.z[fr.ar] = val;
         }

@@ -684,6 +684,95 @@ __global__ void __launch_bounds__(kApplyThreads) patch_apply_kernel(SimDev d, Pa
     }
 }
 
+// The preconditioning step of one GMRES iteration with the line patches in a
+// single launch (in place of arnoldi_precond_kernel + patch_apply_kernel +
+// pack_rows_kernel).  Block (a, p) serves filament a of patch p: it clears the
+// loop condition (block (0, 0)), gathers the patch's rows of the new basis
+// vector Q_k = src * inv_scale (src = r0 or A z in w, or rhs after a discarded
+// guess), stores its own filament's rows of Q_k (and of the copy t that the
+// network's features read), forms its filament's rows of z = P^-1 Q_k (the
+// refresh leaves -A_pp^-1: each warp two rows, lanes striding the 16-byte
+// matrix rows) and packs their forces for the pair kernel.  The filament rows
+// of A z are written by the saddle epilogue (epi_fil_rows): other blocks of
+// the patch still read w here.  A patch without a finite inverse falls back to
+// the block-diagonal preconditioner for the filament.
+// Dynamic shared memory: patch_ld(max_n) + max(nbf, 3*nseg) doubles.
+constexpr int kArnThreads = 512;
+__global__ void __launch_bounds__(kArnThreads, 2) patch_arnoldi_kernel(SimDev d, PatchDev P,
+                                                                       cudaGraphConditionalHandle h) {
+    extern __shared__ __align__(16) double xs[];
+    __shared__ double sm32[32];
+    const int p = blockIdx.y, a = blockIdx.x;
+    if (p == 0 && a == 0 && threadIdx.x == 0) set_loop(h, d.lc, 0);
+    if (a >= P.nf[p]) return;
+    const int m = P.fils[P.fil0[p] + a];
+    const FilRows fr = fil_rows(d, m);
+    if (!d.active[fr.b]) return;  // uniform over the block
+    const int k = d.lc->k;
+    if (k >= d.arr[fr.b].max_iter) return;  // defensive: the cap was reached
+    const GmresCtl &c = d.ctl[fr.b];
+    const double sc = c.inv_scale;
+    const double *src = (k == 0 && c.zero_guess) ? d.rhs : d.w;
+    double *q = d.Q + static_cast<size_t>(k) * d.ldq;
+    const int n = P.nf[p] * P.nbf, nbf = P.nbf, r_lo = a * nbf;
+    const long long *rows = P.rows + P.roff[p];
+    const int ld = patch_ld(n), n4 = ld >> 2;
+    double *zs = xs + ld;
+    for (int cc = threadIdx.x; cc < ld; cc += blockDim.x) xs[cc] = cc < n ? src[rows[cc]] * sc : 0.0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < nbf; r += blockDim.x) q[rows[r_lo + r]] = xs[r_lo + r];
+    if (d.learned)
+        for (int r = threadIdx.x; r < nbf; r += blockDim.x) d.t[rows[r_lo + r]] = xs[r_lo + r];
+    if (!P.ok[p]) {
+        __syncthreads();  // this block's rows of Q_k are in global memory
+        precond_block(d, m, fr, q, d.z, zs, sm32);
+        __syncthreads();
+        for (int kk = threadIdx.x; kk < d.nseg; kk += blockDim.x) {
+            const long long r = fr.lam + 3 * kk;
+            d.f4[m * d.nseg + kk] = make_float4(static_cast<float>(d.z[r]), static_cast<float>(d.z[r + 1]),
+                                                static_cast<float>(d.z[r + 2]), 0.0f);
+        }
+        return;
+    }
+    const float *A = P.A + P.moff[p];
+    const double2 *x2 = reinterpret_cast<const double2 *>(xs);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = 2 * warp; r < nbf; r += 2 * (kArnThreads / 32)) {
+        const bool two = r + 1 < nbf;
+        const float4 *a0 = reinterpret_cast<const float4 *>(A + static_cast<size_t>(r_lo + r) * ld);
+        const float4 *a1 = a0 + n4;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll 4
+        for (int c4 = lane; c4 < n4; c4 += 32) {
+            const float4 v0 = __ldg(a0 + c4);
+            const float4 v1 = two ? __ldg(a1 + c4) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const double2 xa = x2[2 * c4], xb = x2[2 * c4 + 1];
+            s0 = fma(static_cast<double>(v0.x), xa.x, s0);
+            s0 = fma(static_cast<double>(v0.y), xa.y, s0);
+            s0 = fma(static_cast<double>(v0.z), xb.x, s0);
+            s0 = fma(static_cast<double>(v0.w), xb.y, s0);
+            s1 = fma(static_cast<double>(v1.x), xa.x, s1);
+            s1 = fma(static_cast<double>(v1.y), xa.y, s1);
+            s1 = fma(static_cast<double>(v1.z), xb.x, s1);
+            s1 = fma(static_cast<double>(v1.w), xb.y, s1);
+        }
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+        if (lane == 0) {
+            d.z[rows[r_lo + r]] = -s0;
+            zs[r] = -s0;
+            if (two) {
+                d.z[rows[r_lo + r + 1]] = -s1;
+                zs[r + 1] = -s1;
+            }
+        }
+    }
+    __syncthreads();
+    for (int kk = threadIdx.x; kk < d.nseg; kk += blockDim.x)
+        d.f4[m * d.nseg + kk] = make_float4(static_cast<float>(zs[3 * kk]), static_cast<float>(zs[3 * kk + 1]),
+                                            static_cast<float>(zs[3 * kk + 2]), 0.0f);
+}
+
 // After a patch application: packs the force rows of z for the pair kernel
 // and writes the filament rows of A z (one block per filament), the work that
 // arnoldi_precond_kernel does itself with the block-diagonal preconditioner.

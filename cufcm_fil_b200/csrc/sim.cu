@@ -82,6 +82,8 @@ struct Engine {
     long long patch_floats = 0;
     int refresh_every = 1, last_refresh_nt = -1, mob_grid = 1, gj_rounds = 0, gj_cols = 1;
     int apply_chunks = 1, gj_update_grid = 1, rates_grid = 1;
+    int arn_fils = 1;  // blocks per patch of patch_arnoldi_kernel (largest filament count)
+    size_t arn_smem = 0;
     bool refreshed_last = false;
     size_t apply_smem = 0;
     cudaGraph_t rgraph = nullptr;
@@ -308,19 +310,20 @@ int launch_prologue(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
 }
 
 int launch_body(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
-    arnoldi_precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, h);
-    CF_CHECK_LAUNCH("arnoldi_precond_kernel");
-    if (e->learned) {  // z = P_bd(q) + s * net(features(q)), then the rows arnoldi_precond left to us
+    if (e->line) {  // Q_k, z = P^-1 Q_k and the packed forces in one launch
+        patch_arnoldi_kernel<<<dim3(e->arn_fils, e->P.np), kArnThreads, e->arn_smem, st>>>(e->d, e->P, h);
+        CF_CHECK_LAUNCH("patch_arnoldi_kernel");
+    } else {
+        arnoldi_precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, h);
+        CF_CHECK_LAUNCH("arnoldi_precond_kernel");
+    }
+    if (e->learned) {  // z = P(q) + s * net(features(q)), P block-diagonal or the line patches, then the rows
+                       // the previous kernel left to us
         learned_features_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.t, e->d.lx, e->d.lscale);
         CF_CHECK_LAUNCH("learned_features_kernel");
         CF_TRY(mlp_forward_dev(e->net, e->d.lx, e->d.F, e->d.ly, st));
-        learned_correct_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.ly, e->d.lscale);
+        learned_correct_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.ly, e->d.lscale, e->line ? 1 : 0);
         CF_CHECK_LAUNCH("learned_correct_kernel");
-        pack_rows_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.z, e->d.w);
-        CF_CHECK_LAUNCH("pack_rows_kernel");
-    }
-    if (e->line) {  // z = P^-1 Q_k from the copy in t, then the rows arnoldi_precond leaves to us
-        CF_TRY(launch_patch_apply(e, e->d.t, e->d.z, 1, st));
         pack_rows_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.z, e->d.w);
         CF_CHECK_LAUNCH("pack_rows_kernel");
     }
@@ -330,8 +333,12 @@ int launch_body(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
         learned_features_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.w,
                                                                    e->cx + e->c_pairs * F * e->d.lin, e->d.lscale);
         CF_CHECK_LAUNCH("learned_features_kernel");
-        precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, e->d.w, e->d.t);
-        CF_CHECK_LAUNCH("precond_kernel");
+        if (e->line) {
+            CF_TRY(launch_patch_apply(e, e->d.w, e->d.t, 0, st));
+        } else {
+            precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, e->d.w, e->d.t);
+            CF_CHECK_LAUNCH("precond_kernel");
+        }
         learned_target_kernel<<<e->d.F, e->fil_threads, 0, st>>>(e->d, e->d.z, e->d.t, e->d.lscale,
                                                                  e->ct + e->c_pairs * F * e->d.lout);
         CF_CHECK_LAUNCH("learned_target_kernel");
@@ -349,7 +356,7 @@ int launch_finish(Engine *e, cudaStream_t st) {
     backsub_kernel<<<e->B, 256, sizeof(double) * (e->d.mi_max + 1), st>>>(e->d);
     CF_CHECK_LAUNCH("backsub_kernel");
     CF_TRY(launch_combine(e, st));
-    if (e->line) CF_TRY(launch_patch_apply(e, e->d.t, e->d.z, 0, st));
+    if (e->line && !e->d.flexible) CF_TRY(launch_patch_apply(e, e->d.t, e->d.z, 0, st));
     finish_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d);
     CF_CHECK_LAUNCH("finish_kernel");
     return CF_OK;
@@ -508,7 +515,8 @@ int validate(const cf_sim_config *cfg, const char *who) {
     CF_REQUIRE(cfg->beat == CF_BEAT_FULFORD_BLAKE || cfg->beat == CF_BEAT_FULFORD_BLAKE_ORIGINAL,
                "%s: unknown beat %d", who, cfg->beat);
     CF_REQUIRE(cfg->precond == CF_PRECOND_NONE || cfg->precond == CF_PRECOND_BLOCK_DIAG ||
-                   cfg->precond == CF_PRECOND_LINE || cfg->precond == CF_PRECOND_LEARNED,
+                   cfg->precond == CF_PRECOND_LINE || cfg->precond == CF_PRECOND_LEARNED ||
+                   cfg->precond == CF_PRECOND_LEARNED_LINE,
                "%s: preconditioner %d not available in this entry point", who, cfg->precond);
     CF_REQUIRE(cfg->line_patch >= 0 && cfg->line_patch <= 32, "%s: line_patch must be 0..32 (got %d)", who,
                cfg->line_patch);
@@ -633,6 +641,16 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
                                  static_cast<int>(kUpdateSmem)));
     e->apply_chunks = (max_n + kApplyRows - 1) / kApplyRows;
     e->apply_smem = sizeof(double) * std::max(patch_ld(max_n), 3 * d.nseg);
+    e->arn_fils = max_nf;
+    e->arn_smem = sizeof(double) * (patch_ld(max_n) + std::max(nbf, 3 * d.nseg));
+    CF_REQUIRE(e->arn_smem <= 227 * 1024, "line patches of %d unknowns exceed the shared memory of one block", max_n);
+    if (e->arn_smem > 48 * 1024)
+        CF_CUDA(cudaFuncSetAttribute(patch_arnoldi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(e->arn_smem)));
+    if (e->apply_smem > 48 * 1024)
+        CF_CUDA(cudaFuncSetAttribute(patch_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(e->apply_smem)));
+    d.epi_fil_rows = 1;
     e->refresh_every = cfgs[0].precond_refresh > 0 ? cfgs[0].precond_refresh : 1;
     return CF_OK;
 }
@@ -724,9 +742,9 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     d.hstride = static_cast<long long>(mi_max + 2) * (mi_max + 1);
     d.sstride = mi_max + 2;
     d.precond = (c0.precond == CF_PRECOND_NONE) ? 0 : 1;
-    d.line = c0.precond == CF_PRECOND_LINE ? 1 : 0;
+    d.line = (c0.precond == CF_PRECOND_LINE || c0.precond == CF_PRECOND_LEARNED_LINE) ? 1 : 0;
     e->line = d.line != 0;
-    d.learned = c0.precond == CF_PRECOND_LEARNED ? 1 : 0;
+    d.learned = (c0.precond == CF_PRECOND_LEARNED || c0.precond == CF_PRECOND_LEARNED_LINE) ? 1 : 0;
     e->learned = d.learned != 0;
     d.flexible = d.learned;
     d.lin = 9 * ns + 2;   // own force rows, 2 rate rows, neighbour-mean force rows, shape
@@ -1280,8 +1298,8 @@ namespace {
 // step_begin + kinematics, rhs, pair, epilogue, residual + 7 per iteration + backsub, combine, finish;
 // the line-patch preconditioner adds 2 per iteration, 1 in the finish and the refresh when it ran.
 int launches_for(const Engine *e, int iters) {
-    int n = 1 + 5 + 7 * iters + 3;
-    if (e && e->line) n += 2 * iters + 1 + (e->refreshed_last ? refresh_launches(e) : 0);
+    int n = 1 + 5 + 7 * iters + 3;  // with the line patches, patch_arnoldi_kernel takes arnoldi_precond's place
+    if (e && e->line) n += (e->d.flexible ? 0 : 1) + (e->refreshed_last ? refresh_launches(e) : 0);
     if (e && e->learned) n += 6 * iters;  // features, 3 GEMMs, correction, packing
     return n;
 }
@@ -1474,8 +1492,8 @@ extern "C" int cf_sim_set_network_weight(cf_sim *s, double alpha) {
 extern "C" int cf_sim_collect_pairs(cf_sim *s, int nt, int max_pairs, float *x, float *t, int *rows) {
     clear_error();
     CF_REQUIRE(s && x && t && max_pairs > 0, "cf_sim_collect_pairs: bad arguments");
-    CF_REQUIRE(!s->learned && !s->line && s->d.precond == 1,
-               "cf_sim_collect_pairs: pairs come from the block-diagonal solver (CF_PRECOND_BLOCK_DIAG)");
+    CF_REQUIRE(!s->learned && s->d.precond == 1,
+               "cf_sim_collect_pairs: pairs come from the plain solver (CF_PRECOND_BLOCK_DIAG or CF_PRECOND_LINE)");
     CF_REQUIRE(nt >= 0, "cf_sim_collect_pairs: nt must be >= 0");
     CF_CUDA(cudaSetDevice(s->device));
     s->cx = x;

@@ -110,6 +110,7 @@ struct SimDev {
     double lalpha;            // weight of the network correction (chosen by validation; 1 by default)
     int dyn_phase, dyn_angle; // rate blocks present
     int rhs_given;            // solve of a caller's RHS (already in rhs): no RHS assembly, no iteration log
+    int epi_fil_rows;         // the saddle epilogue also writes the filament rows of A v (line patches)
     int s_rows, s_cols;       // arclength table (0 rows: bisection)
     int n_phase_refs, n_angle_refs;
     int dots_chunk, C_tot;
@@ -595,7 +596,7 @@ __global__ void arnoldi_precond_kernel(SimDev d, cudaGraphConditionalHandle h) {
     if (k >= d.arr[fr.b].max_iter) return;  // defensive: the cap was reached
     const GmresCtl &c = d.ctl[fr.b];
     const double sc = c.inv_scale;
-    const double *src = (k == 0) ? (c.zero_guess ? d.rhs : d.Q) : d.w;
+    const double *src = (k == 0 && c.zero_guess) ? d.rhs : d.w;  // r0 (residual kernel) or A z
     double *q = d.Q + static_cast<size_t>(k) * d.ldq;
     const int nb = 3 * d.nseg;
     for (int j = threadIdx.x; j < nb; j += blockDim.x) q[fr.lam + j] = src[fr.lam + j] * sc;
@@ -670,6 +671,27 @@ __global__ void __launch_bounds__(32 * kEpiWarps) saddle_epilogue_kernel(SimDev 
     red[wp][0][lane] = u0;
     red[wp][1][lane] = u1;
     red[wp][2][lane] = u2;
+    if (d.epi_fil_rows && (d.dyn_phase || d.dyn_angle)) {
+        // Filament rows out[pr] = -K_phase^T v_m, out[ar] = -K_angle^T v_m of the filaments whose first
+        // segment lies in this block's 32 segments (each filament in exactly one block), one warp each.
+        const int s0 = blockIdx.x * 32;
+        const int m_end = min(d.F, (s0 + 32 + d.nseg - 1) / d.nseg);
+        for (int m = (s0 + d.nseg - 1) / d.nseg + wp; m < m_end; m += kEpiWarps) {
+            const FilRows fr = fil_rows(d, m);
+            if (!d.active[fr.b]) continue;
+            double dp = 0.0, da = 0.0;
+            for (int j = lane; j < 3 * d.nseg; j += 32) {
+                dp += d.kp[fr.ks + j] * v[fr.lam + j];
+                da += d.ka[fr.ks + j] * v[fr.lam + j];
+            }
+            dp = warp_sum(dp);
+            da = warp_sum(da);
+            if (lane == 0) {
+                if (fr.pr >= 0) out[fr.pr] = -dp;
+                if (fr.ar >= 0) out[fr.ar] = -da;
+            }
+        }
+    }
     __syncthreads();
     if (wp != 0 || b < 0) return;
     double u[3] = {0.0, 0.0, 0.0};
@@ -717,20 +739,22 @@ __global__ void residual_decide_kernel(SimDev d, cudaGraphConditionalHandle h) {
     const FilRows fr = fil_rows(d, m);
     const int nb = 3 * d.nseg;
     double ss = 0.0;
+    // r0 = rhs - A x0 in place of A x0 in w (each entry read and written by the same thread):
+    // the first basis vector is r0 / |r0|, stored into Q_0 by the next kernel.
     for (int j = threadIdx.x; j < nb; j += blockDim.x) {
         const double r = d.rhs[fr.lam + j] - d.w[fr.lam + j];
-        d.Q[fr.lam + j] = r;
+        d.w[fr.lam + j] = r;
         ss += r * r;
     }
     if (threadIdx.x == 0) {
         if (fr.pr >= 0) {
             const double r = d.rhs[fr.pr] - d.w[fr.pr];
-            d.Q[fr.pr] = r;
+            d.w[fr.pr] = r;
             ss += r * r;
         }
         if (fr.ar >= 0) {
             const double r = d.rhs[fr.ar] - d.w[fr.ar];
-            d.Q[fr.ar] = r;
+            d.w[fr.ar] = r;
             ss += r * r;
         }
     }
@@ -1084,7 +1108,7 @@ __global__ void finish_kernel(SimDev d) {
     const bool iterated = st == kGmresConverged || st == kGmresMaxIter;
     if (iterated && !d.flexible && !d.line) precond_block(d, m, fr, d.t, d.t, smp, sm32);
     __syncthreads();
-    const double *dx = d.line ? d.z : d.t;  // the patch preconditioner left P^-1 t in z
+    const double *dx = (d.line && !d.flexible) ? d.z : d.t;  // the patch preconditioner left P^-1 t in z
     const bool reset = st == kGmresZeroRhs || (iterated && ctl->zero_guess);
     const bool add = iterated;
     for (int j = threadIdx.x; j < nb; j += blockDim.x) {

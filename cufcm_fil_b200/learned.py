@@ -1,13 +1,15 @@
-"""Training of the learned preconditioner's network (CF_PRECOND_LEARNED).
+"""Training of the learned preconditioner's network (CF_PRECOND_LEARNED, CF_PRECOND_LEARNED_LINE).
 
-The pairs come from the plain (block-diagonal) solver itself: every Arnoldi
-product w = A z of its steps gives, per filament, the features of w and the
-part (z - P_bd(w)) / s that the block-diagonal preconditioner misses
-(WallCiliaSimulation.collect_pairs).  The network is trained on them by the
-library's own kernels (FilamentMLP.train_step: BF16 tensor-core GEMMs, Adam).
-`compare` runs the same state with and without the network, the check that
-decides whether a trained network is worth using: the block-diagonal
-preconditioner stays the fallback and the reference point.
+The pairs come from the plain solver itself: every Arnoldi product w = A z of
+its steps gives, per filament, the features of w and the part (z - P(w)) / s
+that its preconditioner P misses (WallCiliaSimulation.collect_pairs), with P
+the block-diagonal preconditioner (base CF_PRECOND_BLOCK_DIAG, network mode
+CF_PRECOND_LEARNED) or the line patches (base CF_PRECOND_LINE, network mode
+CF_PRECOND_LEARNED_LINE).  The network is trained on them by the library's own
+kernels (FilamentMLP.train_step: BF16 tensor-core GEMMs, Adam).  `compare`
+runs the same state with and without the network, the check that decides
+whether a trained network is worth using: the base preconditioner stays the
+fallback and the reference point.
 """
 from __future__ import annotations
 
@@ -19,12 +21,15 @@ from . import _lib
 from .mlp import FilamentMLP
 
 
-def collect(make_sim, seeds, steps_per_seed=1, max_pairs=120):
-    """Training pairs from block-diagonal runs of `make_sim(seed, precond)` (one simulation per seed)."""
+LEARNED_MODE = {_lib.CF_PRECOND_BLOCK_DIAG: _lib.CF_PRECOND_LEARNED, _lib.CF_PRECOND_LINE: _lib.CF_PRECOND_LEARNED_LINE}
+
+
+def collect(make_sim, seeds, steps_per_seed=1, max_pairs=120, base=_lib.CF_PRECOND_BLOCK_DIAG):
+    """Training pairs from runs of `make_sim(seed, base)` (one simulation per seed)."""
     import torch
     xs, ts = [], []
     for seed in seeds:
-        with make_sim(seed, _lib.CF_PRECOND_BLOCK_DIAG) as sim:
+        with make_sim(seed, base) as sim:
             for nt in range(steps_per_seed):
                 x, t = sim.collect_pairs(nt, max_pairs)
                 xs.append(x)
@@ -61,7 +66,7 @@ class Comparison:
 
     @property
     def gain(self) -> float:
-        """Iterations of the block-diagonal solve over those of the learned one (>1: the network helps)."""
+        """Iterations of the base solve over those of the learned one (>1: the network helps)."""
         return self.block_diagonal_iterations / max(self.learned_iterations, 1)
 
     @property
@@ -69,14 +74,15 @@ class Comparison:
         return self.learned_status == _lib.CF_OK and self.learned_iterations < self.block_diagonal_iterations
 
 
-def compare(make_sim, seed, net: FilamentMLP, nt=0, weights=(1.0, 0.5, 0.25)) -> Comparison:
-    """Step nt of the same state with the block-diagonal preconditioner and with the network at each
+def compare(make_sim, seed, net: FilamentMLP, nt=0, weights=(1.0, 0.5, 0.25),
+            base=_lib.CF_PRECOND_BLOCK_DIAG) -> Comparison:
+    """Step nt of the same state with the base preconditioner and with the network on top of it at each
     correction weight; the weight with the fewest converged iterations is reported."""
-    with make_sim(seed, _lib.CF_PRECOND_BLOCK_DIAG) as sim:
+    with make_sim(seed, base) as sim:
         rb = sim.step(nt)
     by_weight = {}
     for w in weights:
-        with make_sim(seed, _lib.CF_PRECOND_LEARNED) as sim:
+        with make_sim(seed, LEARNED_MODE[base]) as sim:
             sim.set_network(net)
             sim.set_network_weight(w)
             r = sim.step(nt)

@@ -240,6 +240,7 @@ typedef struct cf_sim cf_sim;
 #define CF_PRECOND_BLOCK_DIAG 1          /* apply_preconditioner_new */
 #define CF_PRECOND_LEARNED 2             /* per-filament MLP (flexible GMRES) */
 #define CF_PRECOND_LINE 3                /* block-Jacobi over line patches along the beat direction */
+#define CF_PRECOND_LEARNED_LINE 4        /* line patches + per-filament MLP correction (flexible GMRES) */
 
 typedef struct cf_sim_config {
     int n_fil;              /* NFIL (one swimmer: the wall) */
@@ -426,9 +427,12 @@ CF_API int cf_precond_load(const char *path, int max_batch, int device, cf_mlp *
  * 3*nseg + 2.  cf_sim_learned_dims gives both widths.
  * cf_sim_set_network attaches a cf_mlp of those widths (batch >= n_fil); the
  * handle keeps the pointer, the caller keeps ownership.
- * cf_sim_collect_pairs runs step nt of a CF_PRECOND_BLOCK_DIAG handle and,
- * after each of its first max_pairs Arnoldi products w = A z, writes the
- * features of w and the target (z_m - P_bd(w)_m) / s_m of every filament into
+ * CF_PRECOND_LEARNED_LINE puts the same correction on top of the line
+ * patches, z_m = P_line(r)_m + s_m net(...).
+ * cf_sim_collect_pairs runs step nt of a CF_PRECOND_BLOCK_DIAG or
+ * CF_PRECOND_LINE handle and, after each of its first max_pairs Arnoldi
+ * products w = A z, writes the features of w and the target
+ * (z_m - P(w)_m) / s_m (P the handle's preconditioner) of every filament into
  * the device arrays x [max_pairs*n_fil][in] and t [max_pairs*n_fil][out];
  * rows = the number written.  cf_sim_features: features of a host vector
  * (system size) into host x [n_fil][in]. */

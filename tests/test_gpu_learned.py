@@ -92,3 +92,31 @@ def test_learned_handle_needs_a_network():
         with FilamentMLP(40, 16, 8, max_batch=64) as wrong:
             with pytest.raises(_lib.CufilError):
                 sim.set_network(wrong)
+
+
+def test_zero_weight_learned_line_equals_line_patches():
+    # With the correction weight 0 the learned-line mode is the line-patch preconditioner run in
+    # flexible GMRES: the same Krylov space, so the same iteration count (to one rounding step).
+    with make_sim(7, _lib.CF_PRECOND_LINE) as sim:
+        r_line = sim.step(0)
+    with FilamentMLP(182, 64, 62, max_batch=256, seed=1) as net, make_sim(7, _lib.CF_PRECOND_LEARNED_LINE) as sim:
+        sim.set_network(net)
+        sim.set_network_weight(0.0)
+        r = sim.step(0)
+    assert r.status == r_line.status == _lib.CF_OK
+    assert abs(r.iterations - r_line.iterations) <= 1
+
+
+def test_network_on_top_of_line_patches_is_measured():
+    # Pairs from line-patch runs (the correction learns what the patches miss: the coupling between
+    # lattice lines); held-out state; the gain is line-patch iterations / learned-line iterations.
+    x, t = learned.collect(make_sim, seeds=(20, 21, 22), max_pairs=60, base=_lib.CF_PRECOND_LINE)
+    assert x.shape[0] > 0 and bool(t.isfinite().all())
+    with FilamentMLP(182, 256, 62, max_batch=4096, seed=0) as net:
+        losses = learned.train(net, x, t, steps=1500, batch=2048, lr=1e-3, report_every=500)
+        cmp = learned.compare(make_sim, 98, net, base=_lib.CF_PRECOND_LINE)
+        print(f"held-out state: line patches {cmp.block_diagonal_iterations} iterations, learned-line "
+              f"{cmp.learned_iterations} at weight {cmp.weight} (status {cmp.learned_status}), gain "
+              f"{cmp.gain:.2f}; by weight {cmp.by_weight}; losses {losses}")
+        assert losses[-1] < losses[0]
+        assert cmp.use_learned == (cmp.learned_status == _lib.CF_OK and cmp.gain > 1.0)
