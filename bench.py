@@ -369,6 +369,60 @@ def run_large(local, inp, flush, steps=4):
                      "gmres_iters_per_step": float(np.mean(its)), "converged": bool(res.status == _lib.CF_OK)}
         sim.close()
     out["speedup"] = out["line_patches"]["timesteps_per_s"] / out["block_diagonal"]["timesteps_per_s"]
+    out["learned"] = run_learned_large(local, inp, flush, steps)
+    if out["learned"].get("timesteps_per_s"):
+        out["learned_vs_plain"] = out["learned"]["timesteps_per_s"] / out["block_diagonal"]["timesteps_per_s"]
+        out["learned_vs_line_patches"] = out["learned"]["timesteps_per_s"] / out["line_patches"]["timesteps_per_s"]
+    return out
+
+
+def run_learned_large(local, inp, flush, steps, seeds=(7, 8, 9), max_pairs=40):
+    """The learned preconditioner at the 32 x 32 size: a per-filament network trained by the library's own kernels
+    on ~1e5 (features, target) pairs that line-patch runs of three other seeded states produce, applied on top of
+    the line patches in flexible GMRES (CF_PRECOND_LEARNED_LINE) on the benchmark state; the correction weight
+    is chosen on that first step among 1, 0.5, 0.25, 0 (0: the network switched off)."""
+    import torch
+    from cufcm_fil_b200 import _lib, learned
+    from cufcm_fil_b200.mlp import FilamentMLP
+    from cufcm_fil_b200.sim import lattice_simulation
+
+    def make(seed, precond):
+        return lattice_simulation(32, spacing=SPACING, nseg=NSEG, seg_sep=SEG_SEP, s_table=inp["s_table"],
+                                  gmres_tol=GMRES_TOL, device=local, precond=precond, seed=seed)
+
+    t0 = time.perf_counter()
+    x, t = learned.collect(make, seeds=seeds, max_pairs=max_pairs, base=_lib.CF_PRECOND_LINE)
+    collect_s = time.perf_counter() - t0
+    n_pairs = int(x.shape[0])
+    net = FilamentMLP(x.shape[1], 256, t.shape[1], max_batch=4096, seed=0, device=local)
+    t0 = time.perf_counter()
+    losses = learned.train(net, x, t, steps=1500, batch=2048, lr=1e-3, report_every=500)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del x, t
+    by_weight = {}
+    for w in (1.0, 0.5, 0.25, 0.0):
+        with make(2024, _lib.CF_PRECOND_LEARNED_LINE) as sim:
+            sim.set_network(net)
+            sim.set_network_weight(w)
+            r = sim.step(0)
+            by_weight[w] = (r.iterations, r.status)
+    ok = [w for w in by_weight if by_weight[w][1] == _lib.CF_OK]
+    best = min(ok, key=lambda w: (by_weight[w][0], -w)) if ok else 0.0
+    out = {"pairs": n_pairs, "collect_s": collect_s, "train_s": train_s, "losses": losses, "weight": best,
+           "first_step_iterations_by_weight": {str(k): v[0] for k, v in by_weight.items()},
+           "network": f"{net.n_in} -> 256 -> 256 -> {net.n_out}, BF16 tensor-core GEMMs, FP32 accumulation"}
+    with make(2024, _lib.CF_PRECOND_LEARNED_LINE) as sim:
+        sim.set_network(net)
+        sim.set_network_weight(best)
+        stream = torch.cuda.ExternalStream(sim.stream_handle())
+        sim.step(0)
+        ms = time_steps(sim, stream, flush, 1, steps)
+        res = sim.last_solve()
+        its = sim.iteration_log(1 + steps)[1:1 + steps]
+        out.update({"timesteps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
+                    "gmres_iters_per_step": float(np.mean(its)), "converged": bool(res.status == _lib.CF_OK)})
+    net.close()
     return out
 
 
