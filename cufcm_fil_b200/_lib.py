@@ -62,6 +62,19 @@ class SimConfig(ctypes.Structure):
                 ("line_patch", ctypes.c_int), ("precond_refresh", ctypes.c_int)]
 
 
+class SwimConfig(ctypes.Structure):
+    _fields_ = [("n_fil", ctypes.c_int), ("n_seg", ctypes.c_int), ("n_blob", ctypes.c_int),
+                ("seg_sep", ctypes.c_double), ("beat", ctypes.c_int), ("dt", ctypes.c_double),
+                ("spring_factor", ctypes.c_double), ("gmres_tol", ctypes.c_double), ("gmres_max_iter", ctypes.c_int),
+                ("fil_refs", ctypes.c_void_p), ("fil_dirs", ctypes.c_void_p), ("blob_refs", ctypes.c_void_p),
+                ("body_x0", ctypes.c_void_p), ("body_q0", ctypes.c_void_p), ("omega0", ctypes.c_void_p),
+                ("phase0", ctypes.c_void_p), ("angle0", ctypes.c_void_p),
+                ("gen_phase_force_refs", ctypes.c_void_p), ("n_gen_phase_refs", ctypes.c_int),
+                ("gen_angle_force_refs", ctypes.c_void_p), ("n_gen_angle_refs", ctypes.c_int),
+                ("s_values_ref", ctypes.c_void_p), ("s_ref_rows", ctypes.c_int), ("s_ref_cols", ctypes.c_int),
+                ("s_tol_factor", ctypes.c_double), ("device", ctypes.c_int)]
+
+
 class FcmConfig(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("rh", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
                 ("eta", ctypes.c_double), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
@@ -174,6 +187,15 @@ SIGNATURES = {
     "cf_batch_autotune": [_vp, _i, _vp],
     "cf_batch_set_tuning": [_vp, _vp],
     "cf_batch_get_tuning": [_vp, _vp],
+    "cf_swim_create": [ctypes.POINTER(SwimConfig), ctypes.POINTER(_vp)],
+    "cf_swim_destroy": [_vp],
+    "cf_swim_step": [_vp, _i, _vp, _vp],
+    "cf_swim_get_state": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "cf_swim_get_particles": [_vp, _vp, _vp, _vp, _vp],
+    "cf_swim_get_directions": [_vp, _vp, _vp],
+    "cf_swim_system_matvec": [_vp, _vp, _vp],
+    "cf_swim_apply_preconditioner": [_vp, _vp, _vp],
+    "cf_swim_system_size": [_vp],
 }
 _RESTYPES = {"cf_last_error": ctypes.c_char_p, "cf_mlp_num_params": ctypes.c_longlong}
 

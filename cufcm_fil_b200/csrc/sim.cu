@@ -1816,3 +1816,6 @@ extern "C" int cf_read_ic(const char *path, int n_fil, double *header, double *p
     std::memcpy(angle, v.data() + n_fil, sizeof(double) * n_fil);
     return CF_OK;
 }
+
+// The free swimmer (cf_swim): shares the beat kinematics above.
+#include "swim_engine.cuh"

@@ -116,6 +116,7 @@ struct SimDev {
     int dots_chunk, C_tot;
     double dt, L, spring, tol, s_tol;
     double R[9];              // filament frame (row-major)
+    const double *Rfil;       // per-filament frames [F][9] (a body's cilia); null: every filament uses R
     BeatCoeffs beat;
     const ArrayInfo *arr;     // [B]
     const int *fil_arr;       // array of each filament [F]
@@ -397,7 +398,7 @@ __global__ void kinematics_kernel(SimDev d) {
 
     // positions and velocity directions (filament.cpp:1425-1500)
     const double ca = cos(sh_ang), sa = sin(sh_ang);
-    const double *R = d.R;
+    const double *R = d.Rfil ? d.Rfil + 9 * m : d.R;
     const double bx = d.base[3 * m], by = d.base[3 * m + 1], bz = d.base[3 * m + 2];
     double g11 = 0, g22 = 0, g12 = 0;
     for (int k = threadIdx.x; k < nseg; k += blockDim.x) {

@@ -483,6 +483,65 @@ CF_API int cf_batch_autotune(cf_batch *b, int k_hint, int *choice);
 CF_API int cf_batch_set_tuning(cf_batch *b, const int *choice);
 CF_API int cf_batch_get_tuning(cf_batch *b, int *choice);
 
+/* ------------------------------------------------------------------------
+ * A free rigid body carrying prescribed cilia (the reference's swimmer with
+ * PRESCRIBED_CILIA, BODY_VELOCITY_TYPE 0, unbounded fluid; one swimmer,
+ * dynamic phase and shape-rotation angle).  Replaces the body branches of
+ * mobility_solver::system_matrix_mult_new / apply_preconditioner_new
+ * (mobility_solver.cpp:1887-2105, 1244-1475), swimmer::make_precon_mat
+ * (swimmer.cpp:1175-1349) and the explicit body update of
+ * cilia_sim_main.cu:700-716.  Saddle layout: [3 n_fil n_seg segment forces |
+ * 3 n_blob blob forces | V, Omega | n_fil phase rates | n_fil angle rates].
+ * All radii are 1 (RSEG = RBLOB = 1), MU = 1.
+ * ------------------------------------------------------------------------ */
+typedef struct cf_swim cf_swim;
+
+typedef struct cf_swim_config {
+    int n_fil, n_seg, n_blob;
+    double seg_sep;            /* SEG_SEP; DL = SEG_SEP */
+    int beat;                  /* CF_BEAT_FULFORD_BLAKE or CF_BEAT_FULFORD_BLAKE_ORIGINAL */
+    double dt;
+    double spring_factor;      /* TORSIONAL_SPRING_MAGNITUDE_FACTOR */
+    double gmres_tol;
+    int gmres_max_iter;
+    /* Body frame: filament bases [3*n_fil] and outward directions [3*n_fil]
+     * (swimmer::filament_references, normal_refs), blob positions [3*n_blob]
+     * (rigid_body::blob_references). */
+    const double *fil_refs;
+    const double *fil_dirs;
+    const double *blob_refs;
+    /* Initial body position [3] and orientation [4, scalar first]; NULL: 0 and identity. */
+    const double *body_x0;
+    const double *body_q0;
+    const double *omega0;      /* [n_fil]; NULL: 2 pi */
+    const double *phase0;      /* [n_fil]; NULL: 0 */
+    const double *angle0;      /* [n_fil]; NULL: 0 */
+    const double *gen_phase_force_refs; int n_gen_phase_refs;
+    const double *gen_angle_force_refs; int n_gen_angle_refs;
+    const double *s_values_ref; int s_ref_rows; int s_ref_cols;
+    double s_tol_factor;
+    int device;
+} cf_swim_config;
+
+CF_API int cf_swim_create(const cf_swim_config *cfg, cf_swim **out);
+CF_API int cf_swim_destroy(cf_swim *h);
+/* One step nt: body frame, kinematics (phase and angle advance when nt > 0),
+ * the body's preconditioner matrix, GMRES (warm start from the last solution),
+ * then the body update x += dt V, q = lie_exp(dt Omega) q. */
+CF_API int cf_swim_step(cf_swim *h, int nt, int *iters, double *relres);
+/* Phase, angle and their rates [n_fil] each; body position [3] and
+ * orientation [4] of the next step; body velocity [6] (V, Omega) of the last step. */
+CF_API int cf_swim_get_state(cf_swim *h, double *phase, double *angle, double *phase_dot, double *angle_dot,
+                             double *body_x, double *body_q, double *body_v);
+/* Segment [3 n_fil n_seg] and blob [3 n_blob] positions and forces of the last step (FP64). */
+CF_API int cf_swim_get_particles(cf_swim *h, double *x_segs, double *x_blobs, double *f_segs, double *f_blobs);
+/* Velocity directions vel_dir_phase, vel_dir_angle [3 n_fil n_seg] each of the last step. */
+CF_API int cf_swim_get_directions(cf_swim *h, double *k_phase, double *k_angle);
+/* A x and P x (host vectors of the system size) for the geometry of the last step. */
+CF_API int cf_swim_system_matvec(cf_swim *h, const double *in, double *out);
+CF_API int cf_swim_apply_preconditioner(cf_swim *h, const double *in, double *out);
+CF_API int cf_swim_system_size(cf_swim *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,66 @@ def cyclic_cubic_spline(phase: float, table) -> float:
                  + dq_up * (t3 - t2))
 
 
+def gmres_right(matvec, precond, rhs, x0, tol, max_iter):
+    """Right-preconditioned GMRES in the reference's order (mobility_solver.cpp:2187-2669): the guess is
+    kept when already good enough and discarded when worse than zero; modified Gram-Schmidt, Givens
+    rotations, back substitution.  Returns (solution, iterations, relative residual estimate)."""
+    nrm_rhs = np.linalg.norm(rhs)
+    soln = np.array(x0, dtype=np.float64, copy=True)
+    if nrm_rhs == 0.0:
+        return np.zeros_like(soln), 0, 0.0
+    r0 = rhs - matvec(soln)
+    beta0 = np.linalg.norm(r0)
+    if abs(beta0) <= tol * nrm_rhs:
+        return soln, 0, beta0 / nrm_rhs
+    if abs(beta0) > nrm_rhs:
+        soln[:] = 0.0
+        beta0 = nrm_rhs
+        r0 = rhs.copy()
+    n = rhs.size
+    Q = np.zeros((n, max_iter + 1))
+    H = np.zeros((max_iter + 1, max_iter + 1))
+    beta = np.zeros(max_iter + 1)
+    cs = np.zeros(max_iter)
+    sn = np.zeros(max_iter)
+    Q[:, 0] = r0 / beta0
+    beta[0] = beta0
+    for it in range(1, max_iter + 1):
+        w = matvec(precond(Q[:, it - 1]))
+        for i in range(it):
+            H[i, it - 1] = w @ Q[:, i]
+            w = w - H[i, it - 1] * Q[:, i]
+        qn = np.linalg.norm(w)
+        H[it, it - 1] = qn
+        Q[:, it] = w / qn if qn != 0 else w
+        for i in range(1, it):
+            t = cs[i - 1] * H[i - 1, it - 1] + sn[i - 1] * H[i, it - 1]
+            H[i, it - 1] = cs[i - 1] * H[i, it - 1] - sn[i - 1] * H[i - 1, it - 1]
+            H[i - 1, it - 1] = t
+        a, b = H[it - 1, it - 1], H[it, it - 1]
+        if b == 0.0:
+            cs[it - 1], sn[it - 1] = 1.0, 0.0
+        elif abs(b) > abs(a):
+            t = a / b
+            sn[it - 1] = (1.0 if b > 0 else -1.0) / math.sqrt(1.0 + t * t)
+            cs[it - 1] = t * sn[it - 1]
+        else:
+            t = b / a
+            cs[it - 1] = (1.0 if a > 0 else -1.0) / math.sqrt(1.0 + t * t)
+            sn[it - 1] = t * cs[it - 1]
+        H[it - 1, it - 1] = cs[it - 1] * a + sn[it - 1] * b
+        H[it, it - 1] = 0.0
+        beta[it] = -sn[it - 1] * beta[it - 1]
+        beta[it - 1] = cs[it - 1] * beta[it - 1]
+        rel = abs(beta[it]) / nrm_rhs
+        if rel <= tol or it == max_iter:
+            y = np.zeros(it)
+            for i in range(it - 1, -1, -1):
+                y[i] = (beta[i] - H[i, i + 1:it] @ y[i + 1:it]) / H[i, i]
+            return soln + precond(Q[:, :it] @ y), it, rel
+    return soln, max_iter, float("nan")
+
+
 class WallCilia:
     """A wall of prescribed-shape cilia with the reference's implicit step."""
 
@@ -291,67 +351,17 @@ class WallCilia:
     # -- solve_linear_system ------------------------------------------------
     def solve(self, rhs):
         """Right-preconditioned GMRES exactly as the reference orders it; returns (iters, relres)."""
-        nrm_rhs = np.linalg.norm(rhs)
-        if nrm_rhs == 0.0:
+        if np.linalg.norm(rhs) == 0.0:
             self.lam[:] = 0.0
             if self.dyn_phase:
                 self.phase_dot[:] = 0.0
             if self.dyn_angle:
                 self.angle_dot[:] = 0.0
             return 0, 0.0
-        soln = self._pack_solution()
-        r0 = rhs - self.matvec(soln)
-        beta0 = np.linalg.norm(r0)
-        if abs(beta0) <= self.tol * nrm_rhs:
-            return 0, beta0 / nrm_rhs
-        if abs(beta0) > nrm_rhs:
-            soln[:] = 0.0
-            beta0 = nrm_rhs
-            r0 = rhs.copy()
-        max_iter = min(self.size, self.max_iter)
-        Q = np.zeros((self.size, max_iter + 1))
-        H = np.zeros((max_iter + 1, max_iter + 1))
-        beta = np.zeros(max_iter + 1)
-        cs = np.zeros(max_iter)
-        sn = np.zeros(max_iter)
-        Q[:, 0] = r0 / beta0
-        beta[0] = beta0
-        for it in range(1, max_iter + 1):
-            w = self.matvec(self.precond(Q[:, it - 1]))
-            for i in range(it):
-                H[i, it - 1] = w @ Q[:, i]
-                w = w - H[i, it - 1] * Q[:, i]
-            qn = np.linalg.norm(w)
-            H[it, it - 1] = qn
-            Q[:, it] = w / qn if qn != 0 else w
-            for i in range(1, it):
-                t = cs[i - 1] * H[i - 1, it - 1] + sn[i - 1] * H[i, it - 1]
-                H[i, it - 1] = cs[i - 1] * H[i, it - 1] - sn[i - 1] * H[i - 1, it - 1]
-                H[i - 1, it - 1] = t
-            a, b = H[it - 1, it - 1], H[it, it - 1]
-            if b == 0.0:
-                cs[it - 1], sn[it - 1] = 1.0, 0.0
-            elif abs(b) > abs(a):
-                t = a / b
-                sn[it - 1] = (1.0 if b > 0 else -1.0) / math.sqrt(1.0 + t * t)
-                cs[it - 1] = t * sn[it - 1]
-            else:
-                t = b / a
-                cs[it - 1] = (1.0 if a > 0 else -1.0) / math.sqrt(1.0 + t * t)
-                sn[it - 1] = t * cs[it - 1]
-            H[it - 1, it - 1] = cs[it - 1] * a + sn[it - 1] * b
-            H[it, it - 1] = 0.0
-            beta[it] = -sn[it - 1] * beta[it - 1]
-            beta[it - 1] = cs[it - 1] * beta[it - 1]
-            rel = abs(beta[it]) / nrm_rhs
-            if rel <= self.tol or it == max_iter:
-                y = np.zeros(it)
-                for i in range(it - 1, -1, -1):
-                    y[i] = (beta[i] - H[i, i + 1:it] @ y[i + 1:it]) / H[i, i]
-                soln = soln + self.precond(Q[:, :it] @ y)
-                self._unpack_solution(soln)
-                return it, rel
-        return max_iter, float("nan")
+        soln, it, rel = gmres_right(self.matvec, self.precond, rhs, self._pack_solution(), self.tol,
+                                    min(self.size, self.max_iter))
+        self._unpack_solution(soln)
+        return it, rel
 
     # -- one implicit step (cilia_sim_main.cu:405-416) -------------------------
     def step(self, nt: int):

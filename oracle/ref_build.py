@@ -105,6 +105,8 @@ def build_fcm(verbose: bool = False, force: bool = False) -> Path | None:
 #   step_dyn_f64  the dynamic run, FP64, host RPY back-end (the whole-step CPU oracle)
 #   step_dyn_gpu  the dynamic run with the reference's own GPU back-end
 #                 (rpy_mobility_solver + Mss_mult), FP32 as the reference ships it
+#   step_body_f64 a free spherical body with prescribed cilia (BODY_OR_SURFACE_TYPE 2,
+#                 BODY_VELOCITY_TYPE 0), FP64, host unbounded-RPY back-end
 # All use GMRES tolerance 1e-6 (LINEAR_SYSTEM_TOL) and a Fulford-Blake beat.
 STEP_SWITCHES = {"CILIA_TYPE": "3", "BODY_OR_SURFACE_TYPE": "0", "MOBILITY_TYPE": "1", "LINEAR_SYSTEM_TOL": "1e-6",
                  "SHAPE_SEQUENCE": "1", "DYNAMIC_PHASE_EVOLUTION": "true", "DYNAMIC_SHAPE_ROTATION": "true",
@@ -113,6 +115,9 @@ STEP_VARIANTS = {
     "step_wgf_f64": ({"WRITE_GENERALISED_FORCES": "true", "FIL_USE_DOUBLE_PRECISION": "true"}, False),
     "step_dyn_f64": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "true"}, False),
     "step_dyn_gpu": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "false"}, True),
+    # a free rigid spherical body carrying prescribed cilia, unbounded RPY (host back-end)
+    "step_body_f64": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "true",
+                       "BODY_OR_SURFACE_TYPE": "2", "BODY_VELOCITY_TYPE": "0"}, False),
 }
 STEP_HOST_CPP = ["src/cilia/mobility/mobility_solver.cpp", "src/cilia/filament.cpp", "src/cilia/swimmer.cpp",
                  "src/cilia/segment.cpp", "src/cilia/rigid_body.cpp", "src/cilia/broyden_solver.cpp",

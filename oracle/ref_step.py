@@ -120,3 +120,69 @@ def run(*, nfil: int, fil_x_dim: int, spacing: float, phase0, angle0, steps: int
     return RefRun(files=files, iterations=rec[:, 0].astype(int), seconds=rec[:, 1], phase=rec[:, 2:2 + F],
                   angle=rec[:, 2 + F:2 + 2 * F], phase_dot=rec[:, 2 + 2 * F:2 + 3 * F],
                   angle_dot=rec[:, 2 + 3 * F:2 + 4 * F], tips=rec[:, 2 + 4 * F:].reshape(-1, F, 3))
+
+
+@dataclass
+class RefBodyRun(RefRun):
+    body_x: np.ndarray | None = None   # [steps, 3] body centre used in the step
+    body_q: np.ndarray | None = None   # [steps, 4] body orientation (scalar first)
+    body_v: np.ndarray | None = None   # [steps, 6] body velocity and angular velocity solved for
+
+
+def _unit_sphere_frames(normals):
+    """Seeding records of the reference (positions on the unit-length sphere of radius 1/2, polar and
+    azimuthal directions, normals) for the given outward unit normals."""
+    n = np.asarray(normals, float).reshape(-1, 3)
+    pos = 0.5 * n
+    ez = np.array([0.0, 0.0, 1.0])
+    azi = np.cross(ez, n)
+    nrm = np.linalg.norm(azi, axis=1)
+    azi[nrm < 1e-12] = [1.0, 0.0, 0.0]
+    azi /= np.linalg.norm(azi, axis=1)[:, None]
+    polar = np.cross(azi, n)
+    return pos, polar, azi, n
+
+
+def _write_seeds(d: Path, count: int, normals) -> None:
+    pos, polar, azi, n = _unit_sphere_frames(normals)
+    stem = d / "input" / "fourier_modes" / f"sphere{count}"
+    stem.parent.mkdir(parents=True, exist_ok=True)
+    for ext, arr in (("seed", pos), ("polar_dir", polar), ("azi_dir", azi), ("normal", n)):
+        stem.with_suffix("." + ext).write_text(" ".join(repr(float(v)) for v in arr.ravel()) + "\n")
+
+
+def run_body(*, fil_normals, blob_normals, ar: float, phase0, angle0, steps: int, phase_refs, angle_refs, s_table,
+             nseg: int = 20, seg_sep: float = 2.6, spring_factor: float = 0.01, timeout: float = 3600.0) -> RefBodyRun:
+    """Dynamic run of the reference's step for one free spherical body (diameter ar * filament length) with
+    filaments along `fil_normals` and blobs along `blob_normals` (unit vectors; the reference reads them as its
+    seeding files, swimmer.cpp:310-345, rigid_body.cpp:330-380)."""
+    fil_normals = np.asarray(fil_normals, float).reshape(-1, 3)
+    blob_normals = np.asarray(blob_normals, float).reshape(-1, 3)
+    F, B = fil_normals.shape[0], blob_normals.shape[0]
+    if F == B:
+        raise ValueError("the reference names its seeding files by count: use different filament and blob counts")
+    with tempfile.TemporaryDirectory() as tmp:
+        d = Path(tmp)
+        f = d / "input" / "forcing"
+        f.mkdir(parents=True)
+        _write_vec(f / _forcing_name("phase_generalised_forces", nseg, seg_sep), phase_refs)
+        _write_vec(f / _forcing_name("angle_generalised_forces", nseg, seg_sep), angle_refs)
+        s = np.asarray(s_table, float)
+        (f / _forcing_name("s_values", nseg, seg_sep)).write_text(
+            f"{s.shape[0]} {s.shape[1]} " + " ".join(repr(float(x)) for x in s.ravel()))
+        _write_seeds(d, F, fil_normals)
+        _write_seeds(d, B, blob_normals)
+        ic = np.concatenate([np.asarray(phase0, float), np.asarray(angle0, float)])
+        (d / "psi.dat").write_text("0 0 " + " ".join(repr(float(x)) for x in ic))
+        cmd = [str(binary("step_body_f64")), "run", str(nseg), str(F), str(B), repr(float(ar)), repr(float(seg_sep)),
+               repr(float(spring_factor)), str(int(steps)), "psi.dat", "out.bin"]
+        subprocess.run(cmd, cwd=d, check=True, capture_output=True, timeout=timeout)
+        width = 2 + 7 * F + 13
+        raw = np.fromfile(d / "out.bin")
+        rec = raw[:raw.size // width * width].reshape(-1, width)
+    o = 2 + 7 * F
+    return RefBodyRun(iterations=rec[:, 0].astype(int), seconds=rec[:, 1], phase=rec[:, 2:2 + F],
+                      angle=rec[:, 2 + F:2 + 2 * F], phase_dot=rec[:, 2 + 2 * F:2 + 3 * F],
+                      angle_dot=rec[:, 2 + 3 * F:2 + 4 * F], tips=rec[:, 2 + 4 * F:o].reshape(-1, F, 3),
+                      body_x=rec[:, o:o + 3], body_q=rec[:, o + 3:o + 7], body_v=rec[:, o + 7:o + 13])
+

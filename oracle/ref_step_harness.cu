@@ -31,6 +31,10 @@
 //       writes input/forcing/..._{phase,angle}_generalised_forces_... and
 //       ..._s_values_... exactly as the reference does.
 //   ref_step_* run  <nseg> <nfil> <fil_x_dim> <spacing> <seg_sep> <spring> <steps> <ic_file> <out.bin> [write]
+//       (a body variant reads <nblob> <ar> in place of <fil_x_dim> <spacing>, the seeding files
+//       input/fourier_modes/sphere<N>.{seed,polar_dir,azi_dir,normal} of swimmer.cpp:310-345 and
+//       rigid_body.cpp:330-380 from the run directory, and appends the body's position,
+//       orientation and velocity to each record)
 //       the dynamic run.  out.bin: per step, doubles
 //       [iterations, seconds, phase[F], angle[F], phase_dot[F], angle_dot[F], x_tip[3F]].
 //       With "write", the reference's data files (ref_step_seg_states.dat, _body_states.dat,
@@ -102,6 +106,40 @@ class host_rpy_solver : public mobility_solver {
     void copy_segment_velocities_to_host() override {}
     void apply_interparticle_forces() override {}
     void wait_for_device() override {}
+#if !INFINITE_PLANE_WALL
+    // Bodies: unbounded RPY over the segments and blobs together (all radii 1; a particle's own block
+    // is the coincident-sphere branch), V_seg = M_ss F_seg + M_sb F_blob, V_blob = M_bs F_seg + M_bb F_blob.
+    std::vector<double> xa, fa, va;
+    void evaluate_full_mobility() override {
+        const int ns = NSWIM * NFIL * NSEG, nb = NSWIM * NBLOB, n = ns + nb;
+        xa.assign(3 * n, 0.0);
+        fa.assign(3 * n, 0.0);
+        va.assign(3 * n, 0.0);
+        for (int i = 0; i < ns; ++i)
+            for (int c = 0; c < 3; ++c) {
+                xa[3 * i + c] = x_segs_host[3 * i + c];
+                fa[3 * i + c] = f_segs_host[6 * i + c];
+            }
+        for (int i = 0; i < nb; ++i)
+            for (int c = 0; c < 3; ++c) {
+                xa[3 * (ns + i) + c] = x_blobs_host[3 * i + c];
+                fa[3 * (ns + i) + c] = f_blobs_host[3 * i + c];
+            }
+        oracle_rpy_apply_f64(0, 3, 3, 0, n, xa.data(), 1.0, nullptr, 0, n, xa.data(), fa.data(), 1.0, 0, 1.0,
+                             va.data(), 0);
+        for (int i = 0; i < ns; ++i) {
+            for (int c = 0; c < 3; ++c) v_segs_host[6 * i + c] = static_cast<Real>(va[3 * i + c]);
+            for (int c = 3; c < 6; ++c) v_segs_host[6 * i + c] = 0;
+        }
+        for (int i = 0; i < nb; ++i)
+            for (int c = 0; c < 3; ++c) v_blobs_host[3 * i + c] = static_cast<Real>(va[3 * (ns + i) + c]);
+    }
+    void evaluate_segment_segment_mobility() override { evaluate_full_mobility(); }
+    void evaluate_segment_blob_mobility() override {}
+    void evaluate_blob_blob_mobility() override {}
+    void evaluate_blob_segment_mobility() override {}
+};
+#else
     void evaluate_segment_segment_mobility() override {
         const int ns = NSWIM * NFIL * NSEG;
         for (int i = 0; i < ns; ++i)
@@ -123,6 +161,7 @@ class host_rpy_solver : public mobility_solver {
     void evaluate_blob_segment_mobility() override {}
     void evaluate_full_mobility() override { evaluate_segment_segment_mobility(); }
 };
+#endif
 typedef host_rpy_solver harness_mobility_solver;
 #endif
 
@@ -144,6 +183,12 @@ void set_globals(int nseg, int nfil, double fil_x_dim, double spacing, double se
     NFIL = nfil;
     NBLOB = 0;
     AR = 1;
+#if !INFINITE_PLANE_WALL
+    // A rigid body: the run line's lattice fields carry the blob count and the aspect ratio AR
+    // (AXIS_DIR_BODY_LENGTH = AR * FIL_LENGTH, the diameter of a spherical body).
+    NBLOB = static_cast<int>(fil_x_dim);
+    AR = static_cast<Real>(spacing);
+#endif
     SEG_SEP = static_cast<Real>(seg_sep);
     PERIOD = 1;
     SIM_LENGTH = 1;
@@ -256,7 +301,11 @@ int main(int argc, char **argv) {
         return 3;
     }
     const int F = NFIL;
+#if INFINITE_PLANE_WALL
     std::vector<double> rec(2 + 7 * F);
+#else
+    std::vector<double> rec(2 + 7 * F + 13);  // + body position, orientation, velocity and angular velocity
+#endif
     for (int nt = 0; nt < TOTAL_TIME_STEPS; nt++) {
         const auto t0 = std::chrono::steady_clock::now();
         for (int i = 0; i < NSWIM; i++) {
@@ -307,7 +356,21 @@ int main(int argc, char **argv) {
             true_states_file << std::endl;
         }
 #endif
+#if !INFINITE_PLANE_WALL
+        for (int c = 0; c < 3; c++) rec[2 + 7 * F + c] = swimmers[0].body.x[c];
+        rec[2 + 7 * F + 3] = swimmers[0].body.q.scalar_part;
+        for (int c = 0; c < 3; c++) rec[2 + 7 * F + 4 + c] = swimmers[0].body.q.vector_part[c];
+        for (int c = 0; c < 6; c++) rec[2 + 7 * F + 7 + c] = mobility.v_bodies(c);
+#endif
         for (int i = 0; i < NSWIM; i++) swimmers[i].end_of_step(nt);
+#if !INFINITE_PLANE_WALL && !WRITE_GENERALISED_FORCES
+        // The explicit body update of cilia_sim_main.cu:700-716 (after the step's data are written).
+        for (int n = 0; n < NSWIM; n++) {
+            for (int c = 0; c < 3; c++) swimmers[n].body.x[c] += DT * mobility.v_bodies(6 * n + c);
+            for (int c = 0; c < 3; c++) swimmers[n].body.u[c] = DT * mobility.v_bodies(6 * n + 3 + c);
+            swimmers[n].body.q = lie_exp(swimmers[n].body.u) * swimmers[n].body.qm1;
+        }
+#endif
         rec[1] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::fwrite(rec.data(), sizeof(double), rec.size(), out);
         std::fflush(out);

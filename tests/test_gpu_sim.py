@@ -180,8 +180,10 @@ def test_step_io_equals_separate_calls(s_table):
 @pytest.mark.parametrize("precond", [_lib.CF_PRECOND_BLOCK_DIAG, _lib.CF_PRECOND_LINE])
 def test_solve_on_given_rhs_matches_oracle(s_table, precond):
     # cf_sim_solve on a random RHS for the geometry of step 0, against the dense FP64 solve of the
-    # oracle's operator (system_matrix_mult_new restated): FP64 true residual below the solver
-    # tolerance plus the FP32 mobility contract, twice (cold start, then the solution as the guess).
+    # oracle's operator (system_matrix_mult_new restated), twice (cold start, then the solution as the
+    # guess).  The engine solves its own operator, whose pair sums are FP32: the FP64 residual of its
+    # solution is bounded by the solver tolerance plus a backward error of the FP32 products,
+    # |rhs - A x| <= tol |rhs| + c |A| |x| (c = 1e-8; the random RHS gives |x| ~ 200 |rhs|).
     gpu, cpu = make_pair(3, 30.0, s_table, seed=11, precond=precond)
     with gpu:
         gpu.initial_guess(0)
@@ -194,7 +196,8 @@ def test_solve_on_given_rhs_matches_oracle(s_table, precond):
             gpu.solve_linear_system(rhs, tol=1e-6, max_iter=10_000)   # cap above the handle's
         x, res = gpu.solve_linear_system(rhs, tol=1e-6)
         assert res.status == _lib.CF_OK and res.relative_residual <= 1e-6
-        assert np.linalg.norm(rhs - A @ x) / np.linalg.norm(rhs) < 2e-5
+        bound = 1e-6 * np.linalg.norm(rhs) + 1e-8 * np.linalg.norm(np.abs(A) @ np.abs(x))
+        assert np.linalg.norm(rhs - A @ x) <= bound
         assert np.linalg.norm(x - x_exact) / np.linalg.norm(x_exact) < 1e-3
         st = gpu.state()
         np.testing.assert_array_equal(st["phase_dot"], x[3 * cpu.nseg_total:3 * cpu.nseg_total + cpu.nfil])
