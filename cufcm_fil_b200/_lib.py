@@ -75,6 +75,15 @@ class SwimConfig(ctypes.Structure):
                 ("s_tol_factor", ctypes.c_double), ("device", ctypes.c_int)]
 
 
+class ElasticConfig(ctypes.Structure):
+    _fields_ = [("n_fil", ctypes.c_int), ("n_seg", ctypes.c_int), ("seg_sep", ctypes.c_double),
+                ("base_pos", ctypes.c_void_p), ("dt", ctypes.c_double), ("dimensionless_force", ctypes.c_double),
+                ("kb", ctypes.c_double), ("kt", ctypes.c_double), ("repulsion_factor", ctypes.c_double),
+                ("broyden_tol", ctypes.c_double), ("max_broyden_iter", ctypes.c_int),
+                ("jacobian_confidence", ctypes.c_double), ("ic_type", ctypes.c_int), ("perturbations", ctypes.c_void_p),
+                ("device", ctypes.c_int)]
+
+
 class FcmConfig(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("rh", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
                 ("eta", ctypes.c_double), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
@@ -196,6 +205,14 @@ SIGNATURES = {
     "cf_swim_system_matvec": [_vp, _vp, _vp],
     "cf_swim_apply_preconditioner": [_vp, _vp, _vp],
     "cf_swim_system_size": [_vp],
+    "cf_elastic_create": [ctypes.POINTER(ElasticConfig), ctypes.POINTER(_vp)],
+    "cf_elastic_destroy": [_vp],
+    "cf_elastic_step": [_vp, _i, _vp],
+    "cf_elastic_get_segments": [_vp, _vp, _vp, _vp],
+    "cf_elastic_get_jacobian_inverse": [_vp, _i, _vp],
+    "cf_elastic_first_evaluation": [_vp, _i, _vp],
+    "cf_elastic_stats": [_vp, _vp, _vp, _vp, _vp],
+    "cf_elastic_system_size": [_vp],
 }
 _RESTYPES = {"cf_last_error": ctypes.c_char_p, "cf_mlp_num_params": ctypes.c_longlong}
 

@@ -542,6 +542,54 @@ CF_API int cf_swim_system_matvec(cf_swim *h, const double *in, double *out);
 CF_API int cf_swim_apply_preconditioner(cf_swim *h, const double *in, double *out);
 CF_API int cf_swim_system_size(cf_swim *h);
 
+/* ------------------------------------------------------------------------
+ * Instability-driven elastic cilia on a no-slip wall (the reference's
+ * CILIA_TYPE 0 with INFINITE_PLANE_WALL): one implicit step (backward Euler at
+ * step 0, BDF2 after) solved by Broyden's method around the 6x6 wall mobility.
+ * Replaces filament::initial_guess / internal_forces_and_torques /
+ * invert_approx_jacobian / update (filament.cpp:1336-2206),
+ * mobility_solver::compute_errors (mobility_solver.cpp:2760-2860), the
+ * barrier forces (cuda_functions.cu:1825-1919) and broyden_solver
+ * (broyden_solver.cpp:26-131), driven as cilia_sim_main.cu:405-560 drives them.
+ * MU = RSEG = 1.  Filaments start straight along +z from their bases.
+ * ------------------------------------------------------------------------ */
+typedef struct cf_elastic cf_elastic;
+
+typedef struct cf_elastic_config {
+    int n_fil, n_seg;              /* 13 <= n_seg <= 24 */
+    double seg_sep;                /* DL = SEG_SEP (> 2) */
+    const double *base_pos;        /* [3 n_fil] */
+    double dt;                     /* DT = PERIOD / STEPS_PER_PERIOD */
+    double dimensionless_force;    /* DIMENSIONLESS_FORCE (0: 220); F_end = it KB / (DL^2 NSEG^2) */
+    double kb, kt;                 /* KB, KT (0: 1800) */
+    double repulsion_factor;       /* REPULSIVE_FORCE_FACTOR (0: 2) */
+    double broyden_tol;            /* TOL (0: 1e-4) */
+    int max_broyden_iter;          /* MAX_BROYDEN_ITER (0: 400) */
+    double jacobian_confidence;    /* JACOBIAN_CONFIDENCE_FACTOR (0: 0.1) */
+    /* Step-0 perturbation forces on segments 4 and 12 (CILIA_IC_TYPE): 0 = (0.01 F_end, 0, 0) on
+     * segment 4 only; 1 = that plus (0, 0.01 F_end, 0) on segment 12; 2 = perturbations
+     * [n_fil][2][3] given (the reference draws them at random for its types 2 and 3). */
+    int ic_type;
+    const double *perturbations;
+    int device;
+} cf_elastic_config;
+
+CF_API int cf_elastic_create(const cf_elastic_config *cfg, cf_elastic **out);
+CF_API int cf_elastic_destroy(cf_elastic *h);
+/* One step nt (0-based); broyden_iters may be NULL.  CF_NOT_CONVERGED when Broyden's method used
+ * all its iterations (the reference stops the run there), CF_NONFINITE when it diverged. */
+CF_API int cf_elastic_step(cf_elastic *h, int nt, int *broyden_iters);
+/* Segment positions [3N], orientations [4N] (scalar first) and the internal forces and torques
+ * [6N] of the last evaluation, FP64; any pointer may be NULL. */
+CF_API int cf_elastic_get_segments(cf_elastic *h, double *x, double *q, double *f);
+/* The approximate inverse Jacobian [6 n_seg x 6 n_seg, row-major] of filament m as last prepared. */
+CF_API int cf_elastic_get_jacobian_inverse(cf_elastic *h, int m, double *jinv);
+/* Initial guess and first evaluation of step nt with the Jacobian prepared, no Broyden iteration;
+ * err_out [6N] (may be NULL) receives the residual.  For checking the stages. */
+CF_API int cf_elastic_first_evaluation(cf_elastic *h, int nt, double *err_out);
+CF_API int cf_elastic_stats(cf_elastic *h, int *last, int *max_iters, long long *total, int *steps);
+CF_API int cf_elastic_system_size(cf_elastic *h);
+
 #ifdef __cplusplus
 }
 #endif

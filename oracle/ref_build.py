@@ -107,7 +107,8 @@ def build_fcm(verbose: bool = False, force: bool = False) -> Path | None:
 #                 (rpy_mobility_solver + Mss_mult), FP32 as the reference ships it
 #   step_body_f64 a free spherical body with prescribed cilia (BODY_OR_SURFACE_TYPE 2,
 #                 BODY_VELOCITY_TYPE 0), FP64, host unbounded-RPY back-end
-# All use GMRES tolerance 1e-6 (LINEAR_SYSTEM_TOL) and a Fulford-Blake beat.
+#   step_dyn_f64_tight  step_dyn_f64 with GMRES tolerance 1e-10 (near-exact linear solves)
+# All others use GMRES tolerance 1e-6 (LINEAR_SYSTEM_TOL) and a Fulford-Blake beat.
 STEP_SWITCHES = {"CILIA_TYPE": "3", "BODY_OR_SURFACE_TYPE": "0", "MOBILITY_TYPE": "1", "LINEAR_SYSTEM_TOL": "1e-6",
                  "SHAPE_SEQUENCE": "1", "DYNAMIC_PHASE_EVOLUTION": "true", "DYNAMIC_SHAPE_ROTATION": "true",
                  "INITIAL_CONDITIONS_TYPE": "0", "DISPLAYTIME": "false"}
@@ -118,6 +119,11 @@ STEP_VARIANTS = {
     # a free rigid spherical body carrying prescribed cilia, unbounded RPY (host back-end)
     "step_body_f64": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "true",
                        "BODY_OR_SURFACE_TYPE": "2", "BODY_VELOCITY_TYPE": "0"}, False),
+    "step_dyn_f64_tight": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "true",
+                            "LINEAR_SYSTEM_TOL": "1e-10"}, False),
+    # instability-driven elastic cilia on the wall (Broyden's method), driven by ref_elastic_harness.cu
+    "elastic_f64": ({"WRITE_GENERALISED_FORCES": "false", "FIL_USE_DOUBLE_PRECISION": "true", "CILIA_TYPE": "0",
+                     "CILIA_IC_TYPE": "0"}, False),
 }
 STEP_HOST_CPP = ["src/cilia/mobility/mobility_solver.cpp", "src/cilia/filament.cpp", "src/cilia/swimmer.cpp",
                  "src/cilia/segment.cpp", "src/cilia/rigid_body.cpp", "src/cilia/broyden_solver.cpp",
@@ -125,6 +131,7 @@ STEP_HOST_CPP = ["src/cilia/mobility/mobility_solver.cpp", "src/cilia/filament.c
 STEP_HOST_CU = ["src/cilia/seeding.cu", "src/general/util.cu", "globals.cu"]
 STEP_GPU_CU = ["src/cilia/cuda_functions.cu", "src/cilia/mobility/rpy_mobility_solver.cu"]
 STEP_HARNESS = HERE / "ref_step_harness.cu"
+ELASTIC_HARNESS = HERE / "ref_elastic_harness.cu"
 LAPACK_SHIM = HERE / "lapack_shim.c"
 RPY_ORACLE = HERE / "rpy_oracle.c"
 
@@ -170,9 +177,10 @@ def build_step(verbose: bool = False, force: bool = False) -> list[Path]:
             jobs.append((src, odir / (src.stem + ".o"),
                          [nvcc, *arch, "-std=c++17", "-O2", "-w", "-x", "cu", "-include", str(cfg), *inc,
                           "-c", str(src)]))
-        jobs.append((STEP_HARNESS, odir / "ref_step_harness.o",
+        harness = ELASTIC_HARNESS if name.startswith("elastic") else STEP_HARNESS
+        jobs.append((harness, odir / (harness.stem + ".o"),
                      [nvcc, *arch, "-std=c++17", "-O2", "-w", "-include", str(cfg), *inc,
-                      *(["-DREF_HARNESS_GPU"] if gpu else []), "-c", str(STEP_HARNESS)]))
+                      *(["-DREF_HARNESS_GPU"] if gpu else []), "-c", str(harness)]))
         jobs.append((LAPACK_SHIM, odir / "lapack_shim.o", ["gcc", "-O2", "-std=c11", "-c", str(LAPACK_SHIM)]))
         if not gpu:
             jobs.append((RPY_ORACLE, odir / "rpy_oracle_f64.o",

@@ -186,3 +186,37 @@ def run_body(*, fil_normals, blob_normals, ar: float, phase0, angle0, steps: int
                       angle_dot=rec[:, 2 + 3 * F:2 + 4 * F], tips=rec[:, 2 + 4 * F:o].reshape(-1, F, 3),
                       body_x=rec[:, o:o + 3], body_q=rec[:, o + 3:o + 7], body_v=rec[:, o + 7:o + 13])
 
+
+
+@dataclass
+class RefElasticRun:
+    iterations: np.ndarray   # [steps] Broyden iterations
+    seconds: np.ndarray      # [steps]
+    x: np.ndarray            # [steps, N, 3] segment positions after each step
+
+
+def run_elastic(*, nfil: int, fil_x_dim: int, spacing: float, steps: int, nseg: int = 20, seg_sep: float = 2.6,
+                period: float = 36.3833, timeout: float = 3600.0) -> RefElasticRun:
+    """The reference's own step for instability-driven elastic cilia on a wall lattice (CILIA_TYPE 0,
+    CILIA_IC_TYPE 0, FP64), run by ref_elastic_harness.cu; DT = period / 300."""
+    with tempfile.TemporaryDirectory() as tmp:
+        d = Path(tmp)
+        cmd = [str(binary("elastic_f64")), "run", str(nseg), str(int(nfil)), str(int(fil_x_dim)), repr(float(spacing)),
+               repr(float(seg_sep)), repr(float(period)), str(int(steps)), "out.bin"]
+        subprocess.run(cmd, cwd=d, check=True, capture_output=True, timeout=timeout)
+        N = int(nfil) * nseg
+        raw = np.fromfile(d / "out.bin")
+        rec = raw[:raw.size // (2 + 3 * N) * (2 + 3 * N)].reshape(-1, 2 + 3 * N)
+    return RefElasticRun(iterations=rec[:, 0].astype(int), seconds=rec[:, 1], x=rec[:, 2:].reshape(-1, N, 3))
+
+
+def elastic_jacobian(*, nseg: int = 20, seg_sep: float = 2.6, period: float = 36.3833):
+    """(inverse approximate Jacobian [6 nseg, 6 nseg], residual [6 nseg]) of one elastic filament at the
+    first evaluation of step 0, from the reference's own invert_approx_jacobian."""
+    with tempfile.TemporaryDirectory() as tmp:
+        d = Path(tmp)
+        cmd = [str(binary("elastic_f64")), "jac", str(nseg), repr(float(seg_sep)), repr(float(period)), "out.bin"]
+        subprocess.run(cmd, cwd=d, check=True, capture_output=True, timeout=600)
+        raw = np.fromfile(d / "out.bin")
+    n = 6 * nseg
+    return raw[:n * n].reshape(n, n), raw[n * n:n * n + n]

@@ -1,0 +1,41 @@
+"""Writes tests/golden/ref_elastic_2x2_80a.npz: the reference's own elastic-filament step.
+
+The reference's host step code for instability-driven elastic cilia on a wall
+(CILIA_TYPE 0, CILIA_IC_TYPE 0: a step-0 perturbation 0.01 F_end e_x on segment
+4; mobility_solver.cpp, filament.cpp, swimmer.cpp, segment.cpp,
+broyden_solver.cpp, ... built with FIL_USE_DOUBLE_PRECISION true by
+oracle/ref_build.py, driven by oracle/ref_elastic_harness.cu, 6x6 wall RPY by
+the FP64 oracle, barrier forces restated there) runs 4 filaments x 20 segments
+on a 2 x 2 wall lattice at spacing 80a with SEP 2.6, DIMENSIONLESS_FORCE 220,
+KB = KT = 1800 and DT = 36.3833/300, for 300 steps; the follower force buckles
+the filaments and they start to beat within the run.  Stored: the Broyden
+iterations of every step and the segment positions every 10 steps; and, for one
+filament, the inverse approximate Jacobian and the residual of the first
+evaluation of step 0 (the reference's invert_approx_jacobian).
+
+Run: python tests/golden/make_elastic_golden.py   (needs the oracle/_ref binaries; a few seconds)
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+from oracle import ref_step  # noqa: E402
+
+OUT = HERE / "ref_elastic_2x2_80a.npz"
+NX, SPACING, STEPS, PERIOD, EVERY = 2, 80.0, 300, 36.3833, 10
+
+
+def main():
+    jinv, err0 = ref_step.elastic_jacobian(period=PERIOD)
+    r = ref_step.run_elastic(nfil=NX * NX, fil_x_dim=NX, spacing=SPACING, steps=STEPS, period=PERIOD)
+    saved = np.arange(0, STEPS, EVERY)
+    np.savez_compressed(OUT, nx=NX, spacing=SPACING, steps=STEPS, period=PERIOD, saved_steps=saved,
+                        x=r.x[saved], iterations=r.iterations, jinv0=jinv, err0=err0)
+    print(OUT, "Broyden iterations per step: mean %.2f max %d" % (r.iterations.mean(), r.iterations.max()))
+
+
+if __name__ == "__main__":
+    main()

@@ -13,7 +13,11 @@ well posed.  The generalised-force tables are the reference's shipped ones
 reference's own WRITE_GENERALISED_FORCES pre-run writes (stored here too, the
 reference tree does not ship it for this beat).
 
-Run: python tests/golden/make_tip_golden.py   (needs the oracle/_ref binaries; ~10 min on 8 cores)
+With --tight the reference's GMRES tolerance is 1e-10 (variant step_dyn_f64_tight) and the
+output is ref_tips_16x16_80a_tight.npz: the trajectory with near-exact linear solves, against
+which solvers whose iterates differ from the reference's (other preconditioners) are compared.
+
+Run: python tests/golden/make_tip_golden.py [--tight]   (needs the oracle/_ref binaries; ~10 min on 8 cores)
 """
 import sys
 from pathlib import Path
@@ -24,7 +28,8 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 from oracle import ref_step  # noqa: E402
 
-OUT = HERE / "ref_tips_16x16_80a.npz"
+TIGHT = "--tight" in sys.argv
+OUT = HERE / ("ref_tips_16x16_80a_tight.npz" if TIGHT else "ref_tips_16x16_80a.npz")
 NX, SPACING, STEPS, SEED = 16, 80.0, 300, 80
 SAVE = np.array(sorted(set(range(0, STEPS, 25)) | {STEPS - 1}))
 
@@ -37,8 +42,10 @@ def main():
     phase0 = rng.uniform(0, 2 * np.pi, F)
     angle0 = rng.normal(0, 0.05, F)
     r = ref_step.run(nfil=F, fil_x_dim=NX, spacing=SPACING, phase0=phase0, angle0=angle0, steps=STEPS,
-                     phase_refs=gold["fb_phase"], angle_refs=gold["fb_angle"], s_table=s_table)
+                     phase_refs=gold["fb_phase"], angle_refs=gold["fb_angle"], s_table=s_table,
+                     variant="step_dyn_f64_tight" if TIGHT else "step_dyn_f64")
     np.savez_compressed(OUT, nx=NX, spacing=SPACING, steps=STEPS, seed=SEED, phase0=phase0, angle0=angle0,
+                        gmres_tol=1e-10 if TIGHT else 1e-6,
                         s_table=s_table, wgf_phase=qp, wgf_angle=qa, saved_steps=SAVE,
                         tips=r.tips[SAVE], phase=r.phase[SAVE], angle=r.angle[SAVE],
                         phase_dot=r.phase_dot[SAVE], angle_dot=r.angle_dot[SAVE], iterations=r.iterations)

@@ -1,0 +1,65 @@
+"""GPU tests of the elastic-filament step (cf_elastic) through the C ABI.
+
+Oracle: the reference's own host step code for instability-driven cilia on a wall
+(tests/golden/ref_elastic_2x2_80a.npz, make_elastic_golden.py).  The approximate
+Jacobian is FP64 throughout and is compared at 1e-10; the residual of the first
+evaluation carries the FP32 pair mobility (1e-5 of its largest entry).  The trajectory:
+the follower force buckles the filaments, an instability that amplifies any difference,
+so the positions are compared over the run with a tolerance that grows with it: FP32
+pair sums and Broyden's stopping test (TOL 1e-4) perturb each step by ~1e-6 L.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from cufcm_fil_b200 import _lib, workloads
+from cufcm_fil_b200.elastic import ElasticCiliaSimulation
+
+pytestmark = pytest.mark.gpu
+
+EL = np.load(Path(__file__).resolve().parent / "golden" / "ref_elastic_2x2_80a.npz")
+L = 2.6 * 20  # FIL_LENGTH = DL NSEG for elastic filaments
+
+
+def make(nx, spacing, **kw):
+    bases = workloads.lattice_bases(nx * nx, nx, spacing, 1.3)
+    return ElasticCiliaSimulation(bases=bases, nseg=20, seg_sep=2.6, dt=float(EL["period"]) / 300, **kw)
+
+
+def test_first_evaluation_and_jacobian_match_reference():
+    with make(1, 80.0) as sim:
+        err = sim.first_evaluation(0)
+        jinv = sim.jacobian_inverse(0)
+    ref = EL["jinv0"]
+    assert np.linalg.norm(jinv - ref) / np.linalg.norm(ref) < 1e-10
+    np.testing.assert_allclose(err, EL["err0"], rtol=0, atol=1e-5 * np.abs(EL["err0"]).max())
+
+
+def test_trajectory_follows_reference():
+    saved = list(EL["saved_steps"])
+    worst = []
+    iters = []
+    with make(int(EL["nx"]), float(EL["spacing"])) as sim:
+        for nt in range(int(EL["steps"])):
+            iters.append(sim.step(nt))
+            if nt in saved:
+                x = sim.segments()[0]
+                worst.append(np.abs(x - EL["x"][saved.index(nt)]).max() / L)
+        st = sim.stats()
+    worst = np.array(worst)
+    it_ref = EL["iterations"]
+    print(f"elastic 2x2, 300 steps: position error / L at steps 0, 100, 200, 290: "
+          f"{worst[0]:.2e} {worst[10]:.2e} {worst[20]:.2e} {worst[-1]:.2e}; Broyden iterations "
+          f"{np.mean(iters):.2f} (reference {it_ref.mean():.2f}), max {st['max']}")
+    assert st["steps"] == 300 and st["total"] == sum(iters)
+    assert np.abs(np.array(iters) - it_ref).max() <= 2
+    assert worst[:11].max() < 1e-4   # through step 100, before the buckling grows
+    assert worst.max() < 1e-2
+
+
+def test_bad_configuration_is_rejected():
+    with pytest.raises(_lib.CufilError):
+        ElasticCiliaSimulation(bases=[[0.0, 0.0, 1.3]], nseg=10)          # the perturbations need 13 segments
+    with pytest.raises(_lib.CufilError):
+        ElasticCiliaSimulation(bases=[[0.0, 0.0, 1.3]], nseg=20, ic_type=2)  # type 2 needs the perturbations

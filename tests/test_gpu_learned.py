@@ -2,10 +2,13 @@
 
 Features are checked against the oracle's restatement (float32 storage: 1e-6
 relative); training uses the library's own kernels; the comparison with the
-block-diagonal preconditioner on a state the network has not seen is reported
+block-diagonal preconditioner on a state the network has not seen is measured
 (gain = block-diagonal iterations / learned iterations) and compare's choice is
-checked against it.  Whatever the network does, a converged learned step
-satisfies the oracle's FP64 system (the residual is formed with the exact operator).
+checked against it.  A gain below 1 is an expected failure that carries the
+measured number: the filament-local correction has so far not beaten the
+preconditioner it corrects.  Whatever the network does, a converged learned
+step satisfies the oracle's FP64 system (the residual is formed with the exact
+operator).
 """
 import math
 from pathlib import Path
@@ -83,6 +86,10 @@ def test_trained_network_gain_is_measured_and_decided():
                                       st["angle_dot"]])
                 rhs = cpu.assemble_rhs()
                 assert np.linalg.norm(rhs - cpu.matvec(sol)) / np.linalg.norm(rhs) < 2e-5
+        if cmp.gain < 1.0:
+            pytest.xfail(f"the learned correction loses on the held-out state: gain {cmp.gain:.2f} "
+                         f"({cmp.block_diagonal_iterations} -> {cmp.learned_iterations} iterations)")
+        assert cmp.gain >= 1.0
 
 
 def test_learned_handle_needs_a_network():
@@ -120,3 +127,7 @@ def test_network_on_top_of_line_patches_is_measured():
               f"{cmp.gain:.2f}; by weight {cmp.by_weight}; losses {losses}")
         assert losses[-1] < losses[0]
         assert cmp.use_learned == (cmp.learned_status == _lib.CF_OK and cmp.gain > 1.0)
+        if cmp.gain < 1.0:
+            pytest.xfail(f"the learned correction on top of the line patches loses on the held-out state: gain "
+                         f"{cmp.gain:.2f} ({cmp.block_diagonal_iterations} -> {cmp.learned_iterations} iterations)")
+        assert cmp.gain >= 1.0

@@ -201,39 +201,63 @@ def test_solve_on_given_rhs_matches_oracle(s_table, precond):
         assert np.linalg.norm(x - x_exact) / np.linalg.norm(x_exact) < 1e-3
         st = gpu.state()
         np.testing.assert_array_equal(st["phase_dot"], x[3 * cpu.nseg_total:3 * cpu.nseg_total + cpu.nfil])
-        x2, res2 = gpu.solve_linear_system(rhs, x0=x, tol=1e-6)
+        # The solution as the guess: kept unchanged when its residual meets the tolerance.  The
+        # recomputed residual of x carries the FP32 product's rounding (~1e-5 of |rhs| here, as
+        # |x| ~ 200 |rhs|), so the guess test uses 1e-4; at 1e-6 a few iterations restore it.
+        x2, res2 = gpu.solve_linear_system(rhs, x0=x, tol=1e-4)
         assert res2.iterations == 0 and np.array_equal(x2, x)
+        _, res4 = gpu.solve_linear_system(rhs, x0=x, tol=1e-6)
+        assert res4.status == _lib.CF_OK and res4.iterations <= 10
         _, res3 = gpu.solve_linear_system(rhs, tol=1e-12, max_iter=3)
         assert res3.status == _lib.CF_NOT_CONVERGED and res3.iterations == 3
 
 
 TIPS = np.load(Path(__file__).resolve().parent / "golden" / "ref_tips_16x16_80a.npz")
+TIPS_TIGHT = np.load(Path(__file__).resolve().parent / "golden" / "ref_tips_16x16_80a_tight.npz")
 
 
-@pytest.mark.parametrize("precond", [_lib.CF_PRECOND_BLOCK_DIAG, _lib.CF_PRECOND_LINE])
-def test_300_steps_of_256_cilia_follow_the_reference_trajectory(precond):
-    # 256 cilia x 20 segments on a 16 x 16 lattice at 80a for 300 implicit steps (one beat period)
-    # against the reference's own step code in FP64 (tests/golden/make_tip_golden.py).  At 80a no
-    # segments of different cilia come within 19a of each other, so the saddle system stays well
-    # posed and the trajectory is not chaotic: the FP32 pair sums of the engine then move the tips
-    # by at most TIP_TOL of the filament length over the whole period.
-    TIP_TOL = 2e-4
-    nx = int(TIPS["nx"])
+def _run_300_steps(precond, tol, golden):
+    nx = int(golden["nx"])
     F = nx * nx
-    bases = workloads.lattice_bases(F, nx, float(TIPS["spacing"]), 1.3)
-    with WallCiliaSimulation(bases=bases, nseg=20, seg_sep=2.6, dt=1 / 300, phase0=TIPS["phase0"],
-                             angle0=TIPS["angle0"], spring_factor=0.01, phase_refs=GOLD["fb_phase"],
-                             angle_refs=GOLD["fb_angle"], s_table=TIPS["s_table"], gmres_tol=1e-6,
+    bases = workloads.lattice_bases(F, nx, float(golden["spacing"]), 1.3)
+    with WallCiliaSimulation(bases=bases, nseg=20, seg_sep=2.6, dt=1 / 300, phase0=golden["phase0"],
+                             angle0=golden["angle0"], spring_factor=0.01, phase_refs=GOLD["fb_phase"],
+                             angle_refs=GOLD["fb_angle"], s_table=golden["s_table"], gmres_tol=tol,
                              precond=precond) as gpu:
         L = 2.6 * 19
-        saved = list(TIPS["saved_steps"])
+        saved = list(golden["saved_steps"])
         worst_tip = worst_phase = 0.0
-        for nt in range(int(TIPS["steps"])):
+        for nt in range(int(golden["steps"])):
             res = gpu.step(nt)
-            assert res.status == _lib.CF_OK and res.relative_residual <= 1e-6
+            assert res.status == _lib.CF_OK and res.relative_residual <= tol
             if nt in saved:
                 q = saved.index(nt)
-                worst_tip = max(worst_tip, np.abs(gpu.tips() - TIPS["tips"][q]).max() / L)
-                worst_phase = max(worst_phase, np.abs(gpu.state()["phase"] - TIPS["phase"][q]).max())
-        print(f"256 cilia x 300 steps: worst tip error {worst_tip:.2e} L, worst phase error {worst_phase:.2e}")
-        assert worst_tip < TIP_TOL and worst_phase < 2 * np.pi * TIP_TOL
+                worst_tip = max(worst_tip, np.abs(gpu.tips() - golden["tips"][q]).max() / L)
+                worst_phase = max(worst_phase, np.abs(gpu.state()["phase"] - golden["phase"][q]).max())
+    return worst_tip, worst_phase
+
+
+def test_300_steps_of_256_cilia_follow_the_reference_trajectory():
+    # 256 cilia x 20 segments on a 16 x 16 lattice at 80a for 300 implicit steps (one beat period)
+    # against the reference's own step code in FP64 at the same GMRES tolerance (1e-6) with the same
+    # (block-diagonal) preconditioner (tests/golden/make_tip_golden.py).  At 80a no segments of
+    # different cilia come within 19a of each other, so the saddle system stays well posed and the
+    # trajectory is not chaotic: the engine takes the reference's Krylov path, and its FP32 pair
+    # sums move the tips by at most TIP_TOL of the filament length over the whole period.
+    TIP_TOL = 2e-4
+    worst_tip, worst_phase = _run_300_steps(_lib.CF_PRECOND_BLOCK_DIAG, 1e-6, TIPS)
+    print(f"256 cilia x 300 steps: worst tip error {worst_tip:.2e} L, worst phase error {worst_phase:.2e}")
+    assert worst_tip < TIP_TOL and worst_phase < 2 * np.pi * TIP_TOL
+
+
+def test_300_steps_with_line_patches_follow_the_converged_trajectory():
+    # A relative residual of 1e-6 leaves the phase and angle rates of this saddle system accurate to
+    # ~1e-3 only (the rate unknowns are weakly determined by the residual): at step 0 the reference's
+    # block-diagonal GMRES at 1e-6 is 8.3e-3 off the exact rates, the line patches at 1e-6 1.8e-3, so
+    # two preconditioners at 1e-6 follow trajectories ~1e-2 L apart after one period.  The line-patch
+    # engine is therefore compared with the reference's trajectory at GMRES tolerance 1e-10
+    # (make_tip_golden.py --tight), itself run at 1e-8.
+    TIP_TOL = 2e-4
+    worst_tip, worst_phase = _run_300_steps(_lib.CF_PRECOND_LINE, 1e-8, TIPS_TIGHT)
+    print(f"line patches at 1e-8, 300 steps: worst tip error {worst_tip:.2e} L, worst phase error {worst_phase:.2e}")
+    assert worst_tip < TIP_TOL and worst_phase < 2 * np.pi * TIP_TOL
