@@ -396,7 +396,7 @@ def run_learned_large(local, inp, flush, steps, seeds=(7, 8, 9), max_pairs=40):
     n_pairs = int(x.shape[0])
     net = FilamentMLP(x.shape[1], 256, t.shape[1], max_batch=4096, seed=0, device=local)
     t0 = time.perf_counter()
-    losses = learned.train(net, x, t, steps=1500, batch=2048, lr=1e-3, report_every=500)
+    losses = learned.train(net, x, t, steps=1500, batch=2048, lr=3e-4, report_every=500)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     del x, t
@@ -481,6 +481,51 @@ def run_fcm(local, flush, reps=5):
         out["gather_gbs"] = gather_bytes / (stages["gather"] * 1e-3) / 1e9
         out["gather_frac"] = out["gather_gbs"] / hbm
     return out
+
+
+def run_swimmer(steps=20):
+    """The free swimmer (cf_swim): 256 Fulford-Blake cilia x 20 segments on a sphere of diameter 6 filament
+    lengths (radius 148a) represented by 2562 blobs, 7942 particles; steps from the seeded state.  The step is
+    host-driven (one synchronisation per GMRES iteration): host wall clock around synchronous steps."""
+    import time
+    from cufcm_fil_b200 import swim
+    gold = np.load(ROOT / "tests" / "golden" / "reference_forcing_nseg20_sep2.6.npz")
+    tips = np.load(ROOT / "tests" / "golden" / "ref_tips_16x16_80a.npz")
+    F, B = 256, 2562
+    geo = swim.sphere_geometry(swim.fibonacci_normals(F), swim.fibonacci_normals(B, 0.3), ar=6.0)
+    rng = np.random.default_rng(12)
+    with swim.CiliatedSwimmer(geometry=geo, phase0=rng.uniform(0, 2 * np.pi, F), angle0=rng.normal(0, 0.05, F),
+                              phase_refs=gold["fb_phase"], angle_refs=gold["fb_angle"],
+                              s_table=tips["s_table"]) as s:
+        s.step(0)
+        t0 = time.perf_counter()
+        its = [s.step(nt).iterations for nt in range(1, 1 + steps)]
+        dt = time.perf_counter() - t0
+        bv = s.state()["body_v"]
+    return {"workload": f"free sphere (radius {geo.radius:.0f}a, {B} blobs) with {F} cilia x 20 segments, "
+                        f"{F * 20 + B} particles, GMRES tol 1e-6, the reference's body preconditioner",
+            "timesteps_per_s": steps / dt, "ms_per_step": 1e3 * dt / steps,
+            "gmres_iters_per_step": float(np.mean(its)), "body_speed": float(np.linalg.norm(bv[:3])),
+            "timing": "host wall clock around synchronous steps (steps 1..20)"}
+
+
+def run_elastic_sim(steps=30):
+    """Elastic instability cilia (cf_elastic): 256 filaments x 20 segments on a 16 x 16 wall lattice at 80a,
+    Broyden's method at the reference's settings; host wall clock around synchronous steps after step 0."""
+    import time
+    from cufcm_fil_b200 import workloads
+    from cufcm_fil_b200.elastic import ElasticCiliaSimulation
+    bases = workloads.lattice_bases(256, 16, 80.0, 1.3)
+    with ElasticCiliaSimulation(bases=bases) as sim:
+        sim.step(0)
+        t0 = time.perf_counter()
+        its = [sim.step(nt) for nt in range(1, 1 + steps)]
+        dt = time.perf_counter() - t0
+    return {"workload": "256 elastic cilia x 20 segments (instability-driven, DIMENSIONLESS_FORCE 220), 16x16 "
+                        "wall lattice at 80a, dt = 36.3833/300, Broyden tol 1e-4",
+            "timesteps_per_s": steps / dt, "ms_per_step": 1e3 * dt / steps,
+            "broyden_iters_per_step": float(np.mean(its)),
+            "timing": "host wall clock around synchronous steps (steps 1..30)"}
 
 
 def measured_hbm_gbs():
@@ -615,6 +660,8 @@ def run_ours(args):
     batched = run_batched(local, inp, world, rank) if not args.no_batched else None
     large = run_large(local, inp, flush) if (world == 1 and not args.no_batched) else None
     fcm = run_fcm(local, flush) if (world == 1 and not args.no_batched) else None
+    swimmer = run_swimmer() if (world == 1 and not args.no_batched) else None
+    elastic = run_elastic_sim() if (world == 1 and not args.no_batched) else None
     cpu = cpu_baseline(inp) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
 
     if rank == 0:
@@ -669,6 +716,8 @@ def run_ours(args):
             "batched": batched,
             "lattice_32x32": large,
             "fcm": fcm,
+            "swimmer": swimmer,
+            "elastic": elastic,
             "cpu_baseline": cpu,
             "vs_cpu_same_precond": (plain_value / cpu["value"]) if cpu else None,
         }
