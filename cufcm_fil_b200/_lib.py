@@ -213,6 +213,7 @@ SIGNATURES = {
     "cf_elastic_first_evaluation": [_vp, _i, _vp],
     "cf_elastic_stats": [_vp, _vp, _vp, _vp, _vp],
     "cf_elastic_system_size": [_vp],
+    "cf_tc_tile_product": [_vp, _vp, _vp, ctypes.c_uint],
 }
 _RESTYPES = {"cf_last_error": ctypes.c_char_p, "cf_mlp_num_params": ctypes.c_longlong}
 

@@ -29,6 +29,7 @@
 
 #include "rpy_pairs.cuh"
 #include "sim_kernels.cuh"
+#include "tc_tf32.cuh"
 
 namespace cufil {
 
@@ -39,7 +40,7 @@ struct PatchDev {
     int np;                  // patches
     int nbf;                 // unknowns per filament (3*nseg + rate rows)
     int max_n;               // largest patch system
-    int max_ld;              // patch_ld(max_n): row stride of the rbuf / cbuf slots
+    int T;                   // 64-wide tiles per side of the largest patch
     const int *fil0;         // first entry of each patch in `fils` [np]
     const int *nf;           // filaments per patch [np]
     const int *fils;         // filament ids (batch numbering), patch by patch
@@ -47,8 +48,11 @@ struct PatchDev {
     const long long *roff;   // first entry of each patch in `rows` [np]
     const long long *rows;   // batch-vector row of each local unknown
     float *A;                // patch matrices, then their inverses (row-major n x n, row stride patch_ld(n))
-    float *cbuf;             // pivot-row copies U, [np][kGjBlock][max_ld] (row stride patch_ld(n))
-    float *rbuf;             // scaled pivot rows, [np][kGjBlock][max_ld] (row stride patch_ld(n))
+    // Round operands of the tile update, per patch and 64-column tile, split for the tensor cores
+    // (tc_tf32.cuh: a TF32 high part and an FP32 remainder, 4096 floats each, canonical K-major
+    // layout with k the pivot row s and m or n the tile column c):
+    float *csplit;           // the pivot-row copies U[s][c], [np][T][2][4096]
+    float *rsplit;           // the scaled pivot rows (D^-1 U)[s][c] (-D^-1 in the pivot columns), same shape
     float *dinv;             // inverted pivot blocks, [np][kGjBlock][kGjBlock]
     int *ok;                 // [np] 1 when the inverse is finite
     int *counter;            // per-round tile counters of the update [rounds]
@@ -316,10 +320,12 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
 // maintained, so the pivot rows' entries are
 //   U[s][j] = A[k0 + s][j] for j >= k0,   A[j][k0 + s] for j < k0  (by symmetry);
 // both are read as 64 contiguous floats per row of A and staged in shared
-// memory as U[s][c].  The pass writes
-//   rbuf[s][j] = (D^-1 U)[s][j] outside the pivot columns, -D^-1[s][j - k0] inside,
-//   cbuf[s][j] = U[s][j]         for j outside the pivot rows (zero inside),
-// both [64][ld].  Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
+// memory as U[s][c].  The pass writes, for the tile's columns c (j = j0 + c),
+//   rsplit: (D^-1 U)[s][c] outside the pivot columns, -D^-1[s][c] inside,
+//   csplit: U[s][c]         outside the pivot columns (zero inside),
+// each split into its TF32 high part and FP32 remainder in the canonical layout of
+// the tensor-core operands (element (c, s) at tc::canon(c, s)), the form in which
+// the update pass multiplies them.  Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
 // block's or disjoint from it.  Each thread owns 4 rows x 4 columns of
 // D^-1 U (rows 4ty + u, columns 4tx + v); the loads and stores of the
 // product's operands and results move 16 bytes each.  grid = (tiles, patches).
@@ -337,16 +343,18 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     const int w = min(kGjTile, n - j0);  // columns in this tile
     const size_t ld = patch_ld(n);
     const float *A = P.A + P.moff[p];
-    float *rb = P.rbuf + static_cast<size_t>(p) * kGjBlock * P.max_ld;
-    float *cb = P.cbuf + static_cast<size_t>(p) * kGjBlock * P.max_ld;
+    float *rs = P.rsplit + (static_cast<size_t>(p) * P.T + blockIdx.x) * 2 * tc::kOperandFloats;
+    float *cs = P.csplit + (static_cast<size_t>(p) * P.T + blockIdx.x) * 2 * tc::kOperandFloats;
     const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
     if (j0 == k0) {  // the pivot columns: -D^-1, and no pivot-row copies
         for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
             const int r = e / kGjTile, c = e - r * kGjTile;
-            if (c < w) {
-                rb[static_cast<size_t>(r) * ld + j0 + c] = -dv[r * kGjBlock + c];  // zero-padded rows
-                cb[static_cast<size_t>(r) * ld + j0 + c] = 0.0f;
-            }
+            float h, l;
+            tc::split_tf32(c < w ? -dv[r * kGjBlock + c] : 0.0f, h, l);  // zero-padded rows
+            rs[tc::canon(c, r)] = h;
+            rs[tc::kOperandFloats + tc::canon(c, r)] = l;
+            cs[tc::canon(c, r)] = 0.0f;
+            cs[tc::kOperandFloats + tc::canon(c, r)] = 0.0f;
         }
         return;
     }
@@ -394,29 +402,32 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
             for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(dr[u], uc[v], acc[u][v]);
     }
     const int c0 = 4 * tx;
+    __syncthreads();  // DvT is free: it stages one 16 KB operand part at a time
+    float *buf = &DvT[0][0];
+    static_assert(kGjBlock * LD >= tc::kOperandFloats, "a staging part fits DvT");
+    for (int part = 0; part < 4; ++part) {  // rs high, rs low, cs high, cs low
+        if (part < 2) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {  // rows >= b: zeros (D^-1 is zero-padded)
-        float *dst = rb + (4 * ty + u) * ld + j0 + c0;
-        if (c0 + 3 < w) {
-            *reinterpret_cast<float4 *>(dst) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
-        } else {
+            for (int u = 0; u < 4; ++u)  // rows >= b: zeros (D^-1 is zero-padded); columns >= w: zeros
 #pragma unroll
-            for (int v = 0; v < 4; ++v)
-                if (c0 + v < w) dst[v] = acc[u][v];
+                for (int v = 0; v < 4; ++v) {
+                    float h, l;
+                    tc::split_tf32(c0 + v < w ? acc[u][v] : 0.0f, h, l);
+                    buf[tc::canon(c0 + v, 4 * ty + u)] = part == 0 ? h : l;
+                }
+        } else {  // the pivot-row entries of the tile's columns (zero beyond w, as U is)
+            for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
+                const int s_ = e >> 6, c = e & 63;
+                float h, l;
+                tc::split_tf32(Us[s_][c], h, l);
+                buf[tc::canon(c, s_)] = part == 2 ? h : l;
+            }
         }
-    }
-    // the pivot-row entries of the tile's columns
-    for (int e4 = threadIdx.x; e4 < kGjBlock * kGjTile / 4; e4 += blockDim.x) {
-        const int s_ = e4 >> 4, c4 = 4 * (e4 & 15);
-        const float4 v = *reinterpret_cast<const float4 *>(&Us[s_][c4]);
-        float *dst = cb + s_ * ld + j0 + c4;
-        if (c4 + 3 < w) {
-            *reinterpret_cast<float4 *>(dst) = v;
-        } else {
-            if (c4 < w) dst[0] = v.x;
-            if (c4 + 1 < w) dst[1] = v.y;
-            if (c4 + 2 < w) dst[2] = v.z;
-        }
+        __syncthreads();
+        float *dst = (part < 2 ? rs : cs) + (part & 1) * tc::kOperandFloats;
+        for (int c4 = threadIdx.x; c4 < tc::kOperandFloats / 4; c4 += blockDim.x)
+            *reinterpret_cast<float4 *>(dst + 4 * c4) = *reinterpret_cast<const float4 *>(buf + 4 * c4);
+        __syncthreads();
     }
 }
 
@@ -468,35 +479,24 @@ __device__ __forceinline__ GjTile gj_tile(const PatchDev &P, int K, int T, int i
     return t;
 }
 
-// Stage of the update pipeline: the tile's C (Cs[s][r] = cbuf[s][row0 + r]),
-// R (Rs[s][c] = rbuf[s][col0 + c]) and old values (Ao[r][c]), rows of 68
-// floats (16-byte aligned, and rows 4 apart fall on different banks).
-constexpr int kUpLd = kGjTile + 4;
-constexpr int kUpStage = 3 * kGjBlock * kUpLd;
-constexpr size_t kUpdateSmem = 2 * kUpStage * sizeof(float);
+// Stage of the update: the tile's split operands as the prep pass left them
+// (A = the pivot-row copies of its row tile, B = the scaled pivot rows of its
+// column tile, each a TF32 high part and an FP32 remainder in the canonical
+// layout, 4 x 16 KB).  The old values are read from global memory by the
+// epilogue.  One stage per block and two blocks per SM: one block's copies
+// overlap the other's products and stores.
+constexpr int kUpStage = 4 * tc::kOperandFloats;
+constexpr size_t kUpdateSmem = kUpStage * sizeof(float);
 
-// Issues the 16-byte copies of a tile into `stage`: 16 chunks of 4 floats per
-// row; chunks at or beyond the row stride are zero-filled (within it, the
-// padding columns hold values that only reach padding outputs).
+// Issues the 16-byte copies of a tile's operands into `stage` (contiguous blocks: 8 + 8 chunks per thread;
+// the pivot rows need B only).
 __device__ __forceinline__ void gj_issue_tile(const PatchDev &P, const GjTile &t, float *stage) {
-    float *Cs = stage, *Rs = stage + kGjBlock * kUpLd, *Ao = stage + 2 * kGjBlock * kUpLd;
-    const float *A = P.A + P.moff[t.p];
-    const float *cb = P.cbuf + static_cast<size_t>(t.p) * kGjBlock * P.max_ld;
-    const float *rb = P.rbuf + static_cast<size_t>(t.p) * kGjBlock * P.max_ld;
-    const int n = t.n, ld = patch_ld(n);
-    const int ch = threadIdx.x & 15, r0 = threadIdx.x >> 4;  // chunk of a row, first row (rows r0 + 16m)
-    const int j = t.col0 + 4 * ch, ir = t.row0 + 4 * ch;
-    const bool jok = j < ld, iok = ir < ld;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const int s_ = r0 + 16 * m;
-        cp_async16(&Rs[s_ * kUpLd + 4 * ch], jok ? rb + s_ * ld + j : rb, jok);
-        if (!t.prow) cp_async16(&Cs[s_ * kUpLd + 4 * ch], iok ? cb + s_ * ld + ir : cb, iok);
-        if (!t.prow && !t.pcol) {
-            const int i = t.row0 + s_;
-            const bool ok = i < n && jok;
-            cp_async16(&Ao[s_ * kUpLd + 4 * ch], ok ? A + static_cast<size_t>(i) * ld + j : A, ok);
-        }
+    float *Ab = stage, *Bb = stage + 2 * tc::kOperandFloats;
+    const float *csrc = P.csplit + (static_cast<size_t>(t.p) * P.T + t.row0 / kGjTile) * 2 * tc::kOperandFloats;
+    const float *rsrc = P.rsplit + (static_cast<size_t>(t.p) * P.T + t.col0 / kGjTile) * 2 * tc::kOperandFloats;
+    for (int c = threadIdx.x; c < 2 * tc::kOperandFloats / 4; c += blockDim.x) {
+        cp_async16(Bb + 4 * c, rsrc + 4 * c, true);
+        if (!t.prow) cp_async16(Ab + 4 * c, csrc + 4 * c, true);
     }
 }
 
@@ -504,120 +504,159 @@ __device__ __forceinline__ void gj_issue_tile(const PatchDev &P, const GjTile &t
 //   pivot rows       A[i, j] = rbuf[i - k0][j]      (-D^-1 in the pivot block)
 //   other rows       A[i, j] -= C_i . rbuf[:, j]   (j outside the pivot columns)
 //                    A[i, j]  = -C_i . rbuf[:, j]  (pivot columns: C_i D^-1)
-// with C_i = cbuf[:][i] -- the symmetric sweep, which leaves -A^-1 after the
-// last round.  Tiles and pivot blocks are both 64 wide, so a tile lies in the
-// pivot rows (ti == K, a copy), in the pivot columns (tj == K) or in neither.
-// Persistent blocks take tiles from a per-round counter and copy the next
-// tile's operands and old values into the other shared-memory stage
-// (cp.async) while they update the current one.  Each thread owns rows
-// 4ty + u and columns 4tx + v (one float4 of each operand per step, float4
-// stores).  The block that takes a patch's diagonal tile (K + 1, K + 1)
-// inverts it for the next round right after its update, while the other
-// blocks go on with the rest.  Dynamic shared memory: kUpdateSmem bytes.
+// with C_i = cbuf[:][i] (the pivot-row copies) and rbuf the scaled pivot rows
+// -- the symmetric sweep, which leaves -A^-1 after the last round.  Tiles and
+// pivot blocks are both 64 wide, so a tile lies in the pivot rows (ti == K, a
+// copy), in the pivot columns (tj == K) or in neither.  Persistent blocks (two
+// per SM) take tiles from a per-round counter.  The tile product C^T rbuf runs
+// on the tensor cores (tc_tf32.cuh: the operands as the prep pass split them,
+// three TF32 products accumulated in FP32 in tensor memory, issued by one
+// thread and committed to an mbarrier).  Read-back: warp w holds tile rows
+// 16 (w % 4) .. + 15 in lanes 0-15 and columns 32 (w / 4) .. + 31; each lane
+// pair (l, l + 16) then splits the 32 columns, so every thread writes 16
+// columns of one row.  The block that takes a patch's diagonal tile
+// (K + 1, K + 1) inverts it for the next round right after its update, while
+// the other blocks go on with the rest.  A wait for the products that gives up
+// (bounded) marks the tile's patch unusable -- it falls back to the
+// block-diagonal preconditioner -- and the block computes no further products.
+// Dynamic shared memory: kUpdateSmem.
 __global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, int T, int *counter) {
-    static_assert(kGjTile == 64 && kGjBlock == 64, "256 threads: 4x4 per thread");
-    static_assert(kUpStage >= kInvWs, "the inversion reuses a stage");
-    extern __shared__ __align__(16) float usm[];
+    static_assert(kGjTile == 64 && kGjBlock == 64 && tc::kTileMN == 64 && tc::kTileK == 64, "64-wide tiles");
+    static_assert(kUpStage >= kInvWs, "the inversion reuses the stage");
+    extern __shared__ __align__(128) float usm[];
     __shared__ int next_item;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tbase;
+    __shared__ int tc_ok, dead;
     const int total = P.np * (T * (T + 1) / 2);
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
     __syncthreads();
-    const int first = next_item;
-    if (first >= total) return;
-    GjTile cur = gj_tile(P, K, T, first);
-    int stage = 0;
-    if (cur.valid) gj_issue_tile(P, cur, usm);
-    cp_async_commit();
-    while (true) {
-        __syncthreads();  // every thread has read next_item and finished with the other stage
-        if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
-        __syncthreads();
-        const int nitem = next_item;
-        GjTile nxt{};
-        nxt.valid = false;
-        if (nitem < total) {
-            nxt = gj_tile(P, K, T, nitem);
-            if (nxt.valid) gj_issue_tile(P, nxt, usm + (stage ^ 1) * kUpStage);
-        }
-        cp_async_commit();
-        cp_async_wait<1>();  // the current stage has landed
-        __syncthreads();
+    int item = next_item;
+    if (item >= total) return;
+    if (warp == 0) tc::tmem_alloc(&tbase, tc::kTmemCols);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+        dead = 0;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tbase;
+    uint32_t products = 0;  // completed phases of `bar`
+    const float *Ab = usm, *Bb = usm + 2 * tc::kOperandFloats;
+    // this thread's output: tile row tr, columns tc0 .. tc0 + 15
+    const int tr = 16 * (warp & 3) + (lane & 15), tc0 = 32 * (warp >> 2) + 16 * (lane >> 4);
+    while (item < total) {
+        const GjTile cur = gj_tile(P, K, T, item);
         if (cur.valid) {
-            float *st = usm + stage * kUpStage;
-            const float *Cs = st, *Rs = st + kGjBlock * kUpLd, *Ao = st + 2 * kGjBlock * kUpLd;
+            gj_issue_tile(P, cur, usm);
+            cp_async_commit();
             const int n = cur.n, ld = patch_ld(n);
-            const int j = cur.col0 + 4 * tx;
-            float *Ar = P.A + P.moff[cur.p] + static_cast<size_t>(cur.row0 + 4 * ty) * ld + j;
-            float4 res[4];
-            if (cur.prow) {  // the pivot rows: rbuf itself (row0 == k0)
+            const int i = cur.row0 + tr, j = cur.col0 + tc0;
+            float *Arow = P.A + P.moff[cur.p] + static_cast<size_t>(i) * ld + j;
+            // the old values, while the operands land (the pivot columns and rows are overwritten)
+            float res[16];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) res[u] = *reinterpret_cast<const float4 *>(&Rs[(4 * ty + u) * kUpLd + 4 * tx]);
+            for (int q = 0; q < 16; ++q) res[q] = 0.0f;
+            if (!cur.prow && !cur.pcol && i < n) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4) {
+                    if (j + q < ld) {
+                        const float4 o4 = *reinterpret_cast<const float4 *>(Arow + q);
+                        res[q] = o4.x;
+                        res[q + 1] = o4.y;
+                        res[q + 2] = o4.z;
+                        res[q + 3] = o4.w;
+                    }
+                }
+            }
+            cp_async_wait<0>();
+            tc::fence_proxy_async();  // the operands are visible to the tensor cores
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            bool have = true;
+            if (cur.prow) {  // the pivot rows: the scaled pivot rows themselves (row0 == k0), high + low parts
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int e = tc::canon(tc0 + q, tr);
+                    res[q] = Bb[e] + Bb[tc::kOperandFloats + e];
+                }
+            } else if (dead) {
+                have = false;
             } else {
-                float acc[4][4] = {};
-#pragma unroll 8
-                for (int s_ = 0; s_ < kGjBlock; ++s_) {
-                    const float4 c4 = *reinterpret_cast<const float4 *>(&Cs[s_ * kUpLd + 4 * ty]);
-                    const float4 r4 = *reinterpret_cast<const float4 *>(&Rs[s_ * kUpLd + 4 * tx]);
-                    const float cr[4] = {c4.x, c4.y, c4.z, c4.w}, rr[4] = {r4.x, r4.y, r4.z, r4.w};
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(cr[u], rr[v], acc[u][v]);
+                if (threadIdx.x == 0) {
+                    tc::issue_tile_products(tmem, Ab, Ab + tc::kOperandFloats, Bb, Bb + tc::kOperandFloats);
+                    tc::commit(&bar);
+                    bool ok = mbar_wait_bounded(&bar, products & 1u);
+                    if (!ok) ok = mbar_wait_bounded(&bar, products & 1u);  // drain before going on
+                    tc_ok = ok ? 1 : 0;
+                    if (!ok) {
+                        dead = 1;
+                        P.ok[cur.p] = 0;
+                    }
                 }
+                ++products;
+                __syncthreads();
+                tc::fence_after_sync();
+                have = tc_ok != 0;
+                if (have) {
+                    float v[32];
+                    tc::tmem_ld32(tc::tmem_addr(tmem, warp, 32 * (warp >> 2)), v);
+                    // lanes l and l + 16 share row l's 32 columns: l keeps 0..15, l + 16 takes 16..31
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    if (!cur.pcol) o = *reinterpret_cast<const float4 *>(&Ao[(4 * ty + u) * kUpLd + 4 * tx]);
-                    res[u] = make_float4(o.x - acc[u][0], o.y - acc[u][1], o.z - acc[u][2], o.w - acc[u][3]);
-                }
-            }
-            // the patch's last round writes its final values: a non-finite one marks the inverse unusable
-            const bool last = (K + 1) * kGjBlock >= n;
-            bool bad = false;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int i = cur.row0 + 4 * ty + u;
-                if (i >= n || j >= n) continue;
-                if (last) {
-                    bad |= !isfinite(res[u].x) || (j + 1 < n && !isfinite(res[u].y)) ||
-                           (j + 2 < n && !isfinite(res[u].z)) || (j + 3 < n && !isfinite(res[u].w));
-                }
-                float *dst = Ar + static_cast<size_t>(u) * ld;
-                if (j + 3 < n) {
-                    *reinterpret_cast<float4 *>(dst) = res[u];
-                } else {  // the row's last, partial chunk: nothing beyond column n - 1
-                    dst[0] = res[u].x;
-                    if (j + 1 < n) dst[1] = res[u].y;
-                    if (j + 2 < n) dst[2] = res[u].z;
+                    for (int q = 0; q < 16; ++q) {
+                        const float hi16 = __shfl_sync(0xffffffffu, v[16 + q], lane & 15);
+                        res[q] -= (lane < 16) ? v[q] : hi16;
+                    }
+                    tc::fence_before_sync();
                 }
             }
-            if (bad) P.ok[cur.p] = 0;
-            if (last && cur.row0 < cur.col0) {
-                // final values: also the transposed tile of the lower block triangle (A^-1 is symmetric); its
-                // columns row0 + 4ty .. + 3 lie in a full row tile, below n
-                float *At = P.A + P.moff[cur.p] + cur.row0 + 4 * ty;
+            if (have) {
+                // the patch's last round writes its final values: a non-finite one marks the inverse unusable
+                const bool last = (K + 1) * kGjBlock >= n;
+                bool bad = false;
+                if (i < n) {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const int jt = j + v;  // the lower tile's row
-                    if (jt >= n) continue;
-                    const float4 t4 = make_float4(v == 0 ? res[0].x : v == 1 ? res[0].y : v == 2 ? res[0].z : res[0].w,
-                                                  v == 0 ? res[1].x : v == 1 ? res[1].y : v == 2 ? res[1].z : res[1].w,
-                                                  v == 0 ? res[2].x : v == 1 ? res[2].y : v == 2 ? res[2].z : res[2].w,
-                                                  v == 0 ? res[3].x : v == 1 ? res[3].y : v == 2 ? res[3].z : res[3].w);
-                    *reinterpret_cast<float4 *>(At + static_cast<size_t>(jt) * ld) = t4;
+                    for (int q = 0; q < 16; q += 4) {
+                        if (j + q + 3 < n) {
+                            *reinterpret_cast<float4 *>(Arow + q) = make_float4(res[q], res[q + 1], res[q + 2], res[q + 3]);
+                        } else {  // the row's last, partial chunk: nothing beyond column n - 1
+#pragma unroll
+                            for (int u = 0; u < 4; ++u)
+                                if (j + q + u < n) Arow[q + u] = res[q + u];
+                        }
+                    }
+                    if (last)
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) bad |= (j + q < n) && !isfinite(res[q]);
                 }
+                if (bad) P.ok[cur.p] = 0;
+                if (last && cur.row0 < cur.col0 && i < n) {
+                    // final values: also the transposed tile of the lower block triangle (A^-1 is symmetric)
+                    float *At = P.A + P.moff[cur.p] + i;
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        if (j + q < n) At[static_cast<size_t>(j + q) * ld] = res[q];
+                }
+            } else if (threadIdx.x == 0) {
+                P.ok[cur.p] = 0;
             }
             if (cur.diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
                 __syncthreads();
-                pivot_invert_patch(P, cur.p, K + 1, st);
+                pivot_invert_patch(P, cur.p, K + 1, usm);
             }
         }
-        if (nitem >= total) break;
-        cur = nxt;
-        stage ^= 1;
+        __syncthreads();  // every thread is done with the stage and with next_item
+        if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
+        __syncthreads();
+        item = next_item;
     }
-    cp_async_wait<0>();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, tc::kTmemCols);
 }
 
 // out = blockdiag(A_pp^-1) in over the patches (in and out must differ).

@@ -620,12 +620,12 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     CF_TRY(eng_upload(e, const_cast<long long **>(&P.rows), rows.data(), rows.size()));
     CF_TRY(eng_alloc(e, &P.A, static_cast<size_t>(mo)));
     CF_CUDA(cudaMemset(P.A, 0, sizeof(float) * static_cast<size_t>(mo)));  // the padding columns stay zero
-    P.max_ld = patch_ld(max_n);
-    CF_TRY(eng_alloc(e, &P.cbuf, static_cast<size_t>(P.np) * P.max_ld * kGjBlock));
-    CF_TRY(eng_alloc(e, &P.rbuf, static_cast<size_t>(P.np) * P.max_ld * kGjBlock));
-    // padding columns are read by whole 16-byte chunks: keep them finite
-    CF_CUDA(cudaMemset(P.cbuf, 0, sizeof(float) * P.np * P.max_ld * kGjBlock));
-    CF_CUDA(cudaMemset(P.rbuf, 0, sizeof(float) * P.np * P.max_ld * kGjBlock));
+    P.T = (max_n + kGjTile - 1) / kGjTile;
+    const size_t split_floats = static_cast<size_t>(P.np) * P.T * 2 * tc::kOperandFloats;
+    CF_TRY(eng_alloc(e, &P.csplit, split_floats));
+    CF_TRY(eng_alloc(e, &P.rsplit, split_floats));
+    CF_CUDA(cudaMemset(P.csplit, 0, sizeof(float) * split_floats));
+    CF_CUDA(cudaMemset(P.rsplit, 0, sizeof(float) * split_floats));
     CF_TRY(eng_alloc(e, &P.dinv, static_cast<size_t>(P.np) * kGjBlock * kGjBlock));
     CF_TRY(eng_alloc(e, &P.ok, P.np));
     CF_TRY(eng_alloc(e, &P.counter, std::max(1, (max_n + kGjBlock - 1) / kGjBlock)));

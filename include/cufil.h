@@ -590,6 +590,12 @@ CF_API int cf_elastic_first_evaluation(cf_elastic *h, int nt, double *err_out);
 CF_API int cf_elastic_stats(cf_elastic *h, int *last, int *max_iters, long long *total, int *steps);
 CF_API int cf_elastic_system_size(cf_elastic *h);
 
+/* One 64 x 64 x 64 tile product D = A^T B (A [k][m], B [k][n], D [m][n], host arrays, FP32) on the
+ * 5th-generation tensor cores as the line patches' refresh computes its tiles: three TF32 products
+ * (operands split into a TF32 high part and an FP32 remainder), FP32 accumulation in tensor memory.
+ * wait_limit: tries of the bounded wait for the products (0: default).  For checking. */
+CF_API int cf_tc_tile_product(const float *A, const float *B, float *D, unsigned wait_limit);
+
 #ifdef __cplusplus
 }
 #endif
