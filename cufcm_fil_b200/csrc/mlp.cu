@@ -5,9 +5,10 @@
 //
 // Every product is one GEMM kernel: C[M x N] = op(A)[M x K] op(B)[K x N] with
 // FP32 operands in memory, rounded to BF16 while they are staged in shared
-// memory, multiplied on the tensor cores by mma.sync m16n8k16 (BF16 x BF16,
-// FP32 accumulate), and an FP32 epilogue (bias, ReLU, or the ReLU mask of the
-// backward pass).  Forward:  A1 = relu(X W1 + b1), A2 = relu(A1 W2 + b2),
+// memory in the canonical K-major layout, multiplied on the 5th-generation
+// tensor cores (tcgen05.mma kind::f16, BF16 x BF16, FP32 accumulation in
+// tensor memory, 128 x 32 tiles, K in chunks of 64), and an FP32 epilogue
+// (bias, ReLU, or the ReLU mask of the backward pass) after tcgen05.ld.  Forward:  A1 = relu(X W1 + b1), A2 = relu(A1 W2 + b2),
 // Y = A2 W3 + b3.  Backward of the mean squared error:
 //   dY = 2 (Y - T) / (n out)      dW3 = A2^T dY    db3 = colsum dY
 //   dZ2 = (dY W3^T) o [A2 > 0]    dW2 = A1^T dZ2   db2 = colsum dZ2
@@ -15,6 +16,7 @@
 // then one Adam step on FP32 master weights.  Reductions (loss, bias
 // gradients) are fixed-order: results do not depend on the launch.
 #include "common.cuh"
+#include "tc_tf32.cuh"
 
 #include <cuda_bf16.h>
 
@@ -31,7 +33,12 @@
 namespace cufil {
 namespace {
 
-constexpr int kTm = 64, kTn = 64, kTk = 32, kPad = 8;
+constexpr int kTcM = 128, kTcN = 32, kTcK = 64;  // C tile and K chunk
+constexpr int kTcA = kTcM * kTcK, kTcB = kTcN * kTcK;  // BF16 elements of the staged operands
+// 20 KB of operands, requested as 32 KB so that at most 7 blocks share an SM: their 7 x 64 allocated
+// accumulator columns stay within the 512 of tensor memory, so no allocation ever waits for another block.
+constexpr size_t kTcSmem = 32 * 1024;
+static_assert(sizeof(__nv_bfloat16) * (kTcA + kTcB) <= kTcSmem, "operands fit the request");
 
 enum Epi : int { kEpiStore = 0, kEpiBias = 1, kEpiBiasRelu = 2, kEpiReluMask = 3 };
 
@@ -45,96 +52,111 @@ struct GemmArgs {
     int ta, tb, epi;
 };
 
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) | (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
-}
-
-// 64x64 tile of C per block of 4 warps (each warp 32x32 = 2 x 4 mma tiles).
-// Shared memory holds the tile of op(A) as [m][k] and of op(B) as [n][k], so
-// that both fragments read consecutive k pairs.
+// One 128 x 32 tile of C per block of 4 warps.  Per K chunk of 64 the block stages op(A) [128 x 64] and
+// op(B)^T [32 x 64] as BF16 in the canonical layout (consecutive threads read consecutive addresses of the
+// operand as it lies in memory), one thread issues four tcgen05.mma (K = 16 each) and commits them to an
+// mbarrier (bounded wait), and the next chunk is staged once they are done.  Row m of the accumulator lives
+// in TMEM lane m: warp w reads rows 32 w + lane, 32 columns.  A wait that gives up fills the tile with quiet
+// NaNs (the caller's residual then reports a non-finite value).
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
-    __shared__ __nv_bfloat16 As[kTm][kTk + kPad];
-    __shared__ __nv_bfloat16 Bs[kTn][kTk + kPad];
-    const int m0 = blockIdx.y * kTm, n0 = blockIdx.x * kTn;
+    extern __shared__ __align__(128) __nv_bfloat16 tsm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tbase;
+    __shared__ int ok_all;
+    __nv_bfloat16 *As = tsm, *Bs = tsm + kTcA;
+    const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int gq = lane >> 2, tq = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
-    for (int k0 = 0; k0 < g.K; k0 += kTk) {
-        // op(A)(m, k): A[m*lda + k] or A[k*lda + m]; consecutive threads walk the memory-contiguous index
-        for (int e = threadIdx.x; e < kTm * kTk; e += blockDim.x) {
-            int m, k;
-            if (g.ta) { k = e / kTm; m = e - k * kTm; } else { m = e / kTk; k = e - m * kTk; }
-            const int gm = m0 + m, gk = k0 + k;
-            float v = 0.0f;
-            if (gm < g.M && gk < g.K) v = g.ta ? g.A[static_cast<size_t>(gk) * g.lda + gm] : g.A[static_cast<size_t>(gm) * g.lda + gk];
-            As[m][k] = __float2bfloat16_rn(v);
-        }
-        // op(B)(k, n): B[k*ldb + n] or B[n*ldb + k]
-        for (int e = threadIdx.x; e < kTn * kTk; e += blockDim.x) {
-            int n, k;
-            if (g.tb) { n = e / kTk; k = e - n * kTk; } else { k = e / kTn; n = e - k * kTn; }
-            const int gn = n0 + n, gk = k0 + k;
-            float v = 0.0f;
-            if (gn < g.N && gk < g.K) v = g.tb ? g.B[static_cast<size_t>(gn) * g.ldb + gk] : g.B[static_cast<size_t>(gk) * g.ldb + gn];
-            Bs[n][k] = __float2bfloat16_rn(v);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int ks = 0; ks < kTk; ks += 16) {
-            uint32_t af[2][4], bf[4][2];
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                const int r = wm + mt * 16 + gq;
-                af[mt][0] = pack_bf16(As[r][ks + 2 * tq], As[r][ks + 2 * tq + 1]);
-                af[mt][1] = pack_bf16(As[r + 8][ks + 2 * tq], As[r + 8][ks + 2 * tq + 1]);
-                af[mt][2] = pack_bf16(As[r][ks + 2 * tq + 8], As[r][ks + 2 * tq + 9]);
-                af[mt][3] = pack_bf16(As[r + 8][ks + 2 * tq + 8], As[r + 8][ks + 2 * tq + 9]);
-            }
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const int c = wn + nt * 8 + gq;
-                bf[nt][0] = pack_bf16(Bs[c][ks + 2 * tq], Bs[c][ks + 2 * tq + 1]);
-                bf[nt][1] = pack_bf16(Bs[c][ks + 2 * tq + 8], Bs[c][ks + 2 * tq + 9]);
-            }
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) {
-                    float *d = acc[mt][nt];
-                    asm volatile(
-                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-                        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                        : "r"(af[mt][0]), "r"(af[mt][1]), "r"(af[mt][2]), "r"(af[mt][3]), "r"(bf[nt][0]),
-                          "r"(bf[nt][1]));
-                }
-        }
-        __syncthreads();
+    if (warp == 0) tc::tmem_alloc(&tbase, tc::kTmemCols);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+        ok_all = 1;
     }
-    // epilogue: accumulator (row g / g+8, columns 2t, 2t+1) of each mma tile
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tbase;
+    uint32_t phase = 0;
+    for (int k0 = 0; k0 < g.K; k0 += kTcK) {
+        // eight independent loads in flight per thread, then the conversions and stores
+        for (int e0 = threadIdx.x; e0 < kTcA; e0 += 8 * blockDim.x) {  // op(A)(m, k): A[m lda + k] or A[k lda + m]
+            float v[8];
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const int row = m0 + wm + mt * 16 + gq + (h >> 1) * 8;
-                const int col = n0 + wn + nt * 8 + 2 * tq + (h & 1);
-                if (row >= g.M || col >= g.N) continue;
-                float v = acc[mt][nt][h];
-                const size_t o = static_cast<size_t>(row) * g.ldc + col;
-                if (g.epi == kEpiBias || g.epi == kEpiBiasRelu) v += g.bias[col];
-                if (g.epi == kEpiBiasRelu) v = fmaxf(v, 0.0f);
-                if (g.epi == kEpiReluMask && !(g.mask[o] > 0.0f)) v = 0.0f;
-                g.C[o] = v;
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x;
+                int m, k;
+                if (g.ta) { k = e / kTcM; m = e - k * kTcM; } else { m = e / kTcK; k = e - m * kTcK; }
+                const int gm = m0 + m, gk = k0 + k;
+                v[u] = (gm < g.M && gk < g.K) ? (g.ta ? g.A[static_cast<size_t>(gk) * g.lda + gm] : g.A[static_cast<size_t>(gm) * g.lda + gk]) : 0.0f;
             }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x;
+                int m, k;
+                if (g.ta) { k = e / kTcM; m = e - k * kTcM; } else { m = e / kTcK; k = e - m * kTcK; }
+                As[tc::canon16(m, k)] = __float2bfloat16_rn(v[u]);
+            }
+        }
+        for (int e0 = threadIdx.x; e0 < kTcB; e0 += 8 * blockDim.x) {  // op(B)(k, n): B[k ldb + n] or B[n ldb + k]
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x;
+                int n, k;
+                if (g.tb) { n = e / kTcK; k = e - n * kTcK; } else { k = e / kTcN; n = e - k * kTcN; }
+                const int gn = n0 + n, gk = k0 + k;
+                v[u] = (gn < g.N && gk < g.K) ? (g.tb ? g.B[static_cast<size_t>(gn) * g.ldb + gk] : g.B[static_cast<size_t>(gk) * g.ldb + gn]) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * blockDim.x;
+                int n, k;
+                if (g.tb) { n = e / kTcK; k = e - n * kTcK; } else { k = e / kTcN; n = e - k * kTcN; }
+                Bs[tc::canon16(n, k)] = __float2bfloat16_rn(v[u]);
+            }
+        }
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (threadIdx.x == 0 && ok_all) {
+            const uint64_t da = tc::smem_desc16(As), db = tc::smem_desc16(Bs);
+#pragma unroll
+            for (int s = 0; s < kTcK / 16; ++s)
+                tc::mma_bf16(tmem, da + s * (256 >> 4), db + s * (256 >> 4), (k0 > 0 || s > 0) ? 1u : 0u);
+            tc::commit(&bar);
+            bool ok = mbar_wait_bounded(&bar, phase & 1u);
+            if (!ok) ok = mbar_wait_bounded(&bar, phase & 1u);  // drain before the operands are restaged
+            if (!ok) ok_all = 0;
+        }
+        ++phase;
+        tc::fence_before_sync();
+        __syncthreads();  // the products are done with the staged operands
+        tc::fence_after_sync();
+    }
+    const int row = m0 + 32 * warp + lane;
+    if (ok_all) {
+        float v[32];
+        tc::tmem_ld32(tc::tmem_addr(tmem, warp, 0), v);
+        if (row < g.M) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int col = n0 + j;
+                if (col >= g.N) continue;
+                float x = v[j];
+                const size_t o = static_cast<size_t>(row) * g.ldc + col;
+                if (g.epi == kEpiBias || g.epi == kEpiBiasRelu) x += g.bias[col];
+                if (g.epi == kEpiBiasRelu) x = fmaxf(x, 0.0f);
+                if (g.epi == kEpiReluMask && !(g.mask[o] > 0.0f)) x = 0.0f;
+                g.C[o] = x;
+            }
+        }
+    } else if (row < g.M) {
+        for (int j = 0; j < kTcN && n0 + j < g.N; ++j) g.C[static_cast<size_t>(row) * g.ldc + n0 + j] = __int_as_float(0x7fc00000);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, tc::kTmemCols);
 }
 
 // dY = 2 (Y - T) / (n * out) and per-block partial sums of (Y - T)^2.
@@ -185,9 +207,10 @@ __global__ void adam_kernel(float *p, const float *gr, float *m, float *v, long 
 int gemm_bf16(const float *A, int lda, int ta, const float *B, int ldb, int tb, float *C, int ldc, int M, int N, int K,
               const float *bias, const float *mask, int epi, cudaStream_t st) {
     if (M <= 0 || N <= 0) return CF_OK;
+    if (K <= 0) return set_error(CF_EINVAL, "gemm_bf16: empty inner dimension");
     GemmArgs g{A, B, C, bias, mask, lda, ldb, ldc, M, N, K, ta, tb, epi};
-    dim3 grid((N + kTn - 1) / kTn, (M + kTm - 1) / kTm);
-    gemm_bf16_kernel<<<grid, 128, 0, st>>>(g);
+    dim3 grid((N + kTcN - 1) / kTcN, (M + kTcM - 1) / kTcM);
+    gemm_bf16_kernel<<<grid, 128, kTcSmem, st>>>(g);
     CF_CHECK_LAUNCH("gemm_bf16_kernel");
     return CF_OK;
 }

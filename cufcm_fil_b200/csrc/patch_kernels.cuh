@@ -402,32 +402,25 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
             for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(dr[u], uc[v], acc[u][v]);
     }
     const int c0 = 4 * tx;
-    __syncthreads();  // DvT is free: it stages one 16 KB operand part at a time
-    float *buf = &DvT[0][0];
-    static_assert(kGjBlock * LD >= tc::kOperandFloats, "a staging part fits DvT");
-    for (int part = 0; part < 4; ++part) {  // rs high, rs low, cs high, cs low
-        if (part < 2) {
+    __syncthreads();  // DvT is free: it holds the product tile while it is written out
+    float(*Pt)[LD] = DvT;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)  // rows >= b: zeros (D^-1 is zero-padded); columns >= w: zeros
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    float h, l;
-                    tc::split_tf32(c0 + v < w ? acc[u][v] : 0.0f, h, l);
-                    buf[tc::canon(c0 + v, 4 * ty + u)] = part == 0 ? h : l;
-                }
-        } else {  // the pivot-row entries of the tile's columns (zero beyond w, as U is)
-            for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
-                const int s_ = e >> 6, c = e & 63;
-                float h, l;
-                tc::split_tf32(Us[s_][c], h, l);
-                buf[tc::canon(c, s_)] = part == 2 ? h : l;
-            }
-        }
-        __syncthreads();
-        float *dst = (part < 2 ? rs : cs) + (part & 1) * tc::kOperandFloats;
-        for (int c4 = threadIdx.x; c4 < tc::kOperandFloats / 4; c4 += blockDim.x)
-            *reinterpret_cast<float4 *>(dst + 4 * c4) = *reinterpret_cast<const float4 *>(buf + 4 * c4);
-        __syncthreads();
+    for (int u = 0; u < 4; ++u)  // rows >= b: zeros (D^-1 is zero-padded); columns >= w: zeros
+        *reinterpret_cast<float4 *>(&Pt[4 * ty + u][c0]) =
+            make_float4(c0 < w ? acc[u][0] : 0.0f, c0 + 1 < w ? acc[u][1] : 0.0f, c0 + 2 < w ? acc[u][2] : 0.0f,
+                        c0 + 3 < w ? acc[u][3] : 0.0f);
+    __syncthreads();
+    // both operands written in the canonical order (consecutive threads, consecutive addresses): element q of
+    // the layout is (c, s) = tc::canon_inverse(q); the pivot-row entries are U itself (zero beyond w, as U is)
+    for (int q = threadIdx.x; q < tc::kOperandFloats; q += blockDim.x) {
+        const int c = tc::canon_mn(q), s_ = tc::canon_k(q);
+        float h, l;
+        tc::split_tf32(Pt[s_][c], h, l);
+        rs[q] = h;
+        rs[tc::kOperandFloats + q] = l;
+        tc::split_tf32(Us[s_][c], h, l);
+        cs[q] = h;
+        cs[tc::kOperandFloats + q] = l;
     }
 }
 
@@ -736,13 +729,14 @@ __global__ void __launch_bounds__(kApplyThreads) patch_apply_kernel(SimDev d, Pa
 // the patch still read w here.  A patch without a finite inverse falls back to
 // the block-diagonal preconditioner for the filament.
 // Dynamic shared memory: patch_ld(max_n) + max(nbf, 3*nseg) doubles.
-constexpr int kArnThreads = 512;
-__global__ void __launch_bounds__(kArnThreads, 2) patch_arnoldi_kernel(SimDev d, PatchDev P,
+constexpr int kArnThreads = 256;
+constexpr int kArnParts = 2;  // blocks per filament: the rows of segments [0, ceil(nseg/2)) and the rest
+__global__ void __launch_bounds__(kArnThreads, 4) patch_arnoldi_kernel(SimDev d, PatchDev P,
                                                                        cudaGraphConditionalHandle h) {
     extern __shared__ __align__(16) double xs[];
     __shared__ double sm32[32];
-    const int p = blockIdx.y, a = blockIdx.x;
-    if (p == 0 && a == 0 && threadIdx.x == 0) set_loop(h, d.lc, 0);
+    const int p = blockIdx.y, a = blockIdx.x / kArnParts, part = blockIdx.x % kArnParts;
+    if (p == 0 && blockIdx.x == 0 && threadIdx.x == 0) set_loop(h, d.lc, 0);
     if (a >= P.nf[p]) return;
     const int m = P.fils[P.fil0[p] + a];
     const FilRows fr = fil_rows(d, m);
@@ -754,15 +748,19 @@ __global__ void __launch_bounds__(kArnThreads, 2) patch_arnoldi_kernel(SimDev d,
     const double *src = (k == 0 && c.zero_guess) ? d.rhs : d.w;
     double *q = d.Q + static_cast<size_t>(k) * d.ldq;
     const int n = P.nf[p] * P.nbf, nbf = P.nbf, r_lo = a * nbf;
+    // this block's rows of the filament: whole segments (3 rows each), the rate rows with the second part
+    const int split = 3 * ((d.nseg + 1) / 2);
+    const int r_beg = part == 0 ? 0 : split, r_end = part == 0 ? split : nbf;
     const long long *rows = P.rows + P.roff[p];
     const int ld = patch_ld(n), n4 = ld >> 2;
     double *zs = xs + ld;
     for (int cc = threadIdx.x; cc < ld; cc += blockDim.x) xs[cc] = cc < n ? src[rows[cc]] * sc : 0.0;
     __syncthreads();
-    for (int r = threadIdx.x; r < nbf; r += blockDim.x) q[rows[r_lo + r]] = xs[r_lo + r];
-    if (d.learned)
-        for (int r = threadIdx.x; r < nbf; r += blockDim.x) d.t[rows[r_lo + r]] = xs[r_lo + r];
-    if (!P.ok[p]) {
+    if (!P.ok[p]) {  // the first part alone: the whole filament through the block-diagonal preconditioner
+        if (part != 0) return;
+        for (int r = threadIdx.x; r < nbf; r += blockDim.x) q[rows[r_lo + r]] = xs[r_lo + r];
+        if (d.learned)
+            for (int r = threadIdx.x; r < nbf; r += blockDim.x) d.t[rows[r_lo + r]] = xs[r_lo + r];
         __syncthreads();  // this block's rows of Q_k are in global memory
         precond_block(d, m, fr, q, d.z, zs, sm32);
         __syncthreads();
@@ -773,11 +771,14 @@ __global__ void __launch_bounds__(kArnThreads, 2) patch_arnoldi_kernel(SimDev d,
         }
         return;
     }
+    for (int r = r_beg + threadIdx.x; r < r_end; r += blockDim.x) q[rows[r_lo + r]] = xs[r_lo + r];
+    if (d.learned)
+        for (int r = r_beg + threadIdx.x; r < r_end; r += blockDim.x) d.t[rows[r_lo + r]] = xs[r_lo + r];
     const float *A = P.A + P.moff[p];
     const double2 *x2 = reinterpret_cast<const double2 *>(xs);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int r = 2 * warp; r < nbf; r += 2 * (kArnThreads / 32)) {
-        const bool two = r + 1 < nbf;
+    for (int r = r_beg + 2 * warp; r < r_end; r += 2 * (kArnThreads / 32)) {
+        const bool two = r + 1 < r_end;
         const float4 *a0 = reinterpret_cast<const float4 *>(A + static_cast<size_t>(r_lo + r) * ld);
         const float4 *a1 = a0 + n4;
         double s0 = 0.0, s1 = 0.0;
@@ -807,7 +808,8 @@ __global__ void __launch_bounds__(kArnThreads, 2) patch_arnoldi_kernel(SimDev d,
         }
     }
     __syncthreads();
-    for (int kk = threadIdx.x; kk < d.nseg; kk += blockDim.x)
+    const int kk_end = min(d.nseg, r_end / 3);
+    for (int kk = r_beg / 3 + threadIdx.x; kk < kk_end; kk += blockDim.x)
         d.f4[m * d.nseg + kk] = make_float4(static_cast<float>(zs[3 * kk]), static_cast<float>(zs[3 * kk + 1]),
                                             static_cast<float>(zs[3 * kk + 2]), 0.0f);
 }

@@ -311,7 +311,7 @@ int launch_prologue(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
 
 int launch_body(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
     if (e->line) {  // Q_k, z = P^-1 Q_k and the packed forces in one launch
-        patch_arnoldi_kernel<<<dim3(e->arn_fils, e->P.np), kArnThreads, e->arn_smem, st>>>(e->d, e->P, h);
+        patch_arnoldi_kernel<<<dim3(kArnParts * e->arn_fils, e->P.np), kArnThreads, e->arn_smem, st>>>(e->d, e->P, h);
         CF_CHECK_LAUNCH("patch_arnoldi_kernel");
     } else {
         arnoldi_precond_kernel<<<e->d.F, e->fil_threads, e->pre_smem, st>>>(e->d, h);

@@ -29,6 +29,10 @@ constexpr uint32_t kTmemCols = 64;           // FP32 accumulator columns
 // Index (in floats) of element (mn, k) of a 64 x 64 operand in the canonical K-major layout.
 __host__ __device__ constexpr int canon(int mn, int k) { return (mn & 7) * 4 + (k & 3) + (k >> 2) * 32 + (mn >> 3) * 512; }
 
+// The inverse map: row (m or n) and k of the element at canonical index q.
+__host__ __device__ constexpr int canon_mn(int q) { return (q >> 9) * 8 + ((q & 31) >> 2); }
+__host__ __device__ constexpr int canon_k(int q) { return ((q & 511) >> 5) * 4 + (q & 3); }
+
 // FP32 -> (TF32 high part rounded to nearest, FP32 remainder).
 __device__ __forceinline__ void split_tf32(float a, float &hi, float &lo) {
     uint32_t h;
@@ -69,6 +73,28 @@ __device__ __forceinline__ void issue_tile_products(uint32_t tmem_d, const float
         mma_tf32(tmem_d, dah + o, dbl + o, 1u);
         mma_tf32(tmem_d, dah + o, dbh + o, 1u);
     }
+}
+
+// BF16 operands (kind::f16): 8 rows x 16 bytes (8 BF16 along K) per core matrix, the K chunks of a group of
+// 8 rows 128 B apart, the groups 1024 B apart (K chunk of 64); element (mn, k) at canon16(mn, k).
+__host__ __device__ constexpr int canon16(int mn, int k) { return (mn & 7) * 8 + (k & 7) + (k >> 3) * 64 + (mn >> 3) * 512; }
+
+__device__ __forceinline__ uint64_t smem_desc16(const void *p) {
+    const uint64_t addr = (static_cast<uint64_t>(smem_u32(p)) >> 4) & 0x3FFFull;
+    return addr | (static_cast<uint64_t>(128 >> 4) << 16) | (static_cast<uint64_t>(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = 32, M = 128.
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdescBf16), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
 }
 
 // Arrives on `bar` once every tcgen05.mma this thread issued has completed.

@@ -10,6 +10,10 @@
       bandwidth of spreading and interpolation against their algorithmic bytes
       (spread: N ngd^3 x 3 read-modify-writes of 4 bytes each way; gather:
       N ngd^3 x 3 reads of 4 bytes).
+  python -m cufcm_fil_b200.perf mlp --batch 1024 --reps 50
+      forward passes of the learned preconditioner's network (182 -> 256 -> 256
+      -> 62, BF16 GEMMs) at one filament per row, as one GMRES iteration of the
+      32 x 32 lattice runs it; CUDA events around each pass.
 Each prints one JSON line.
 """
 from __future__ import annotations
@@ -67,6 +71,28 @@ def run_fcm(grid: int, reps: int, hbm_gbs: float | None = None):
     return out
 
 
+def run_mlp(batch: int, reps: int):
+    import torch
+    from .mlp import FilamentMLP
+    with FilamentMLP(182, 256, 62, max_batch=batch, seed=0) as net:
+        x = torch.randn(batch, 182, device="cuda")
+        y = torch.empty(batch, 62, device="cuda")
+        st = torch.cuda.Stream()
+        torch.cuda.synchronize()
+        for _ in range(5):
+            net.forward(x, y, stream=st)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for a, b in ev:  # events on the stream the network's kernels run on
+            a.record(st)
+            net.forward(x, y, stream=st)
+            b.record(st)
+        st.synchronize()
+        us = sorted(1e3 * a.elapsed_time(b) for a, b in ev)
+    flop = 2 * batch * (182 * 256 + 256 * 256 + 256 * 62)
+    return {"batch": batch, "forward_us_median": us[len(us) // 2], "flop_per_forward": flop,
+            "tflops": flop / (us[len(us) // 2] * 1e-6) / 1e12}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m cufcm_fil_b200.perf")
     sub = ap.add_subparsers(dest="what", required=True)
@@ -79,9 +105,14 @@ def main(argv=None):
     fc.add_argument("--grid", type=int, default=512)
     fc.add_argument("--reps", type=int, default=5)
     fc.add_argument("--hbm-gbs", type=float, default=None)
+    ml = sub.add_parser("mlp")
+    ml.add_argument("--batch", type=int, default=1024)
+    ml.add_argument("--reps", type=int, default=50)
     a = ap.parse_args(argv)
     if a.what == "step":
         print(json.dumps(run_steps(a.nx, a.precond, a.steps, a.line_patch)))
+    elif a.what == "mlp":
+        print(json.dumps(run_mlp(a.batch, a.reps)))
     else:
         print(json.dumps(run_fcm(a.grid, a.reps, a.hbm_gbs)))
 

@@ -67,3 +67,19 @@ def test_bad_configuration_is_rejected():
         ElasticCiliaSimulation(bases=[[0.0, 0.0, 1.3]], nseg=10)          # the perturbations need 13 segments
     with pytest.raises(_lib.CufilError):
         ElasticCiliaSimulation(bases=[[0.0, 0.0, 1.3]], nseg=20, ic_type=2)  # type 2 needs the perturbations
+
+
+def test_broyden_cap_and_non_finite_state_are_reported():
+    # one Broyden iteration cannot reach TOL from the straight start: CF_NOT_CONVERGED, as the reference stops
+    with make(1, 80.0, max_broyden_iter=1) as sim:
+        with pytest.raises(_lib.CufilError) as e:
+            sim.step(0)
+        assert e.value.code == _lib.CF_NOT_CONVERGED
+    # a NaN perturbation makes the first residual non-finite: CF_NONFINITE, and the handle stays usable
+    pert = np.zeros((1, 2, 3))
+    pert[0, 0, 0] = np.nan
+    with make(1, 80.0, ic_type=2, perturbations=pert) as sim:
+        with pytest.raises(_lib.CufilError) as e:
+            sim.step(0)
+        assert e.value.code == _lib.CF_NONFINITE
+        sim.stats()

@@ -82,3 +82,14 @@ def test_bad_configuration_is_rejected():
         CiliatedSwimmer(geometry=geo, nseg=1, phase_refs=GOLD["fb_phase"], angle_refs=GOLD["fb_angle"])
     with pytest.raises(_lib.CufilError):
         CiliatedSwimmer(geometry=geo, nseg=20)  # no generalised-force tables
+
+
+def test_non_finite_state_is_reported():
+    phase0 = np.array(SWIM["phase0"], float)
+    phase0[3] = np.nan
+    geo = sphere_geometry(SWIM["fil_normals"], SWIM["blob_normals"], ar=float(SWIM["ar"]))
+    with CiliatedSwimmer(geometry=geo, phase0=phase0, angle0=SWIM["angle0"], phase_refs=GOLD["fb_phase"],
+                         angle_refs=GOLD["fb_angle"], s_table=SWIM["s_table"]) as s:
+        with pytest.raises(_lib.CufilError) as e:
+            s.step(0)
+        assert e.value.code == _lib.CF_NONFINITE
