@@ -5,7 +5,9 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstdarg>
+#include <cstdlib>
 #include <string>
+#include <utility>
 
 #include "../../include/cufil.h"
 
@@ -21,6 +23,41 @@ inline int cuda_status(cudaError_t e, const char *what, const char *file, int li
     if (e == cudaSuccess) return CF_OK;
     return set_error(e == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA, "%s failed at %s:%d: %s",
                      what, file, line, cudaGetErrorString(e));
+}
+
+// Programmatic dependent launch for the kernels of the implicit step's inner loops
+// (the GMRES iteration and the Gauss-Jordan rounds of the patch refresh).  A
+// kernel launched by launch_chained() may be scheduled while the previous kernel
+// of its stream drains (its blocks are scheduled as the previous kernel's blocks
+// exit); it calls chain_wait() before it touches global memory, which returns
+// once that kernel has completed and its writes are visible, so the stream's
+// order is kept and only the launch latency between the kernels is hidden.
+// chain_wait() is a no-op for an ordinary launch.  CUFIL_NO_PDL=1 makes
+// launch_chained() an ordinary launch.
+__device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+inline bool chained_launches() {
+    static const bool on = [] {
+        const char *v = std::getenv("CUFIL_NO_PDL");
+        return !(v && *v && *v != '0');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                  Args &&...args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = chained_launches() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 }  // namespace cufil

@@ -48,15 +48,24 @@ struct PatchDev {
     const long long *roff;   // first entry of each patch in `rows` [np]
     const long long *rows;   // batch-vector row of each local unknown
     float *A;                // patch matrices, then their inverses (row-major n x n, row stride patch_ld(n))
-    // Round operands of the tile update, per patch and 64-column tile, split for the tensor cores
-    // (tc_tf32.cuh: a TF32 high part and an FP32 remainder, 4096 floats each, canonical K-major
+    // Round operands of the tile update, per round parity, patch and 64-column tile, split for the tensor
+    // cores (tc_tf32.cuh: a TF32 high part and an FP32 remainder, 4096 floats each, canonical K-major
     // layout with k the pivot row s and m or n the tile column c):
-    float *csplit;           // the pivot-row copies U[s][c], [np][T][2][4096]
+    float *csplit;           // the pivot-row copies U[s][c], [2][np][T][2][4096]
     float *rsplit;           // the scaled pivot rows (D^-1 U)[s][c] (-D^-1 in the pivot columns), same shape
-    float *dinv;             // inverted pivot blocks, [np][kGjBlock][kGjBlock]
+    float *dinv;             // inverted pivot blocks, [2][np][kGjBlock][kGjBlock] (round parity)
     int *ok;                 // [np] 1 when the inverse is finite
-    int *counter;            // per-round tile counters of the update [rounds]
+    int *flow;               // dependency flags of the refresh (gj_flow_kernel), flow_ints(np, T)
 };
+
+// Round K's operand buffers of column tile t of patch p, and its pivot block's inverse: round parity
+// K & 1, so that one round's prep can run while the previous round's updates still read theirs.
+__device__ __forceinline__ size_t gj_split_off(const PatchDev &P, int K, int p, int t) {
+    return ((static_cast<size_t>(K & 1) * P.np + p) * P.T + t) * 2 * tc::kOperandFloats;
+}
+__device__ __forceinline__ float *gj_dinv(const PatchDev &P, int K, int p) {
+    return P.dinv + (static_cast<size_t>(K & 1) * P.np + p) * 64 * 64;
+}
 
 // Row stride of a patch system of n unknowns: rows start on 16 bytes, so tiles
 // move in 16-byte copies.  The padding columns [n, ld) are never part of a result.
@@ -122,68 +131,6 @@ __global__ void patch_rates_kernel(SimDev d, PatchDev P) {
     }
 }
 
-// Gauss-Jordan inversion without pivoting of a 32x32 block by warps 0-3 of the
-// block: the thread (warp w, lane r) holds columns 8w .. 8w+7 of row r in v[].
-// Per step the warp that owns the pivot column publishes it in shared memory
-// (double-buffered, so one 128-thread named barrier per step); each warp
-// takes the pivot row's entries of its own columns from lane t by shuffles.
-// colbuf: 2 x 32 floats of shared memory.  Returns true if a pivot was zero or
-// not finite.  Warps 4-7 must not call it.
-__device__ __forceinline__ bool quad_invert32(float (&v)[8], float (*colbuf)[32]) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    bool bad = false;
-#pragma unroll 2
-    for (int t = 0; t < 32; ++t) {
-        const int ow = t >> 3, oc = t & 7;  // owner warp and column slot of pivot column t
-        float *cb = colbuf[t & 1];
-        if (w == ow) {
-            float x = v[0];
-#pragma unroll
-            for (int c = 1; c < 8; ++c)
-                if (c == oc) x = v[c];
-            cb[lane] = x;
-        }
-        asm volatile("bar.sync 1, 128;" ::: "memory");
-        const float f = cb[lane], piv = cb[t];  // this row's entry in column t; the pivot
-        bad |= !(fabsf(piv) > 0.0f) || !isfinite(piv);
-        const float ip = 1.0f / piv;
-        const bool own = lane == t;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const float pr = __shfl_sync(0xffffffffu, v[c], t) * ip;  // scaled pivot row, this column
-            const bool pc = w == ow && c == oc;                        // this column is the pivot column
-            v[c] = pc ? (own ? ip : -f * ip) : (own ? pr : fmaf(-f, pr, v[c]));
-        }
-    }
-    return bad;
-}
-
-// O[i][j] (+)= sign * sum_k L[i][k] R[k][j] for 32x32 blocks in shared memory
-// (leading dimensions ldl, ldr, ldo); all 256 threads, each 2 rows x 2
-// columns (rows 2ty, 2ty + 1, columns tx, tx + 16): one shared load per FMA.
-__device__ __forceinline__ void block_gemm32(const float *L, int ldl, const float *R, int ldr, float *O, int ldo,
-                                             const float *Add, int lda, float sign) {
-    const int i0 = 2 * (threadIdx.x >> 4), j0 = threadIdx.x & 15;
-    float a00 = 0.0f, a01 = 0.0f, a10 = 0.0f, a11 = 0.0f;
-#pragma unroll 8
-    for (int k = 0; k < 32; ++k) {
-        const float l0 = L[i0 * ldl + k], l1 = L[(i0 + 1) * ldl + k];
-        const float r0 = R[k * ldr + j0], r1 = R[k * ldr + j0 + 16];
-        a00 = fmaf(l0, r0, a00);
-        a01 = fmaf(l0, r1, a01);
-        a10 = fmaf(l1, r0, a10);
-        a11 = fmaf(l1, r1, a11);
-    }
-    const float acc[2][2] = {{a00, a01}, {a10, a11}};
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-        for (int v = 0; v < 2; ++v) {
-            const int i = i0 + u, j = j0 + 16 * v;
-            O[i * ldo + j] = (Add ? Add[i * lda + j] : 0.0f) + sign * acc[u][v];
-        }
-}
-
 // acc = L R for 64x64 blocks in shared memory (leading dimension kInvLd, 16-byte
 // rows); each of the 256 threads owns rows 4*(tid/16) + u and columns
 // 4*(tid%16) + v, the R operand read as one float4 per step.
@@ -212,87 +159,134 @@ __device__ __forceinline__ void block_gemm64(const float *L, const float *R, flo
 __device__ __forceinline__ void load_pivot_block(const float *A, int n, int k0, int b, float *M) {
     for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) {
         const int r = e >> 6, c = e & 63;
-        M[r * kInvLd + c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * patch_ld(n) + k0 + c] : (r == c ? 1.0f : 0.0f);
+        M[r * kInvLd + c] = (r < b && c < b) ? __ldcg(A + static_cast<size_t>(k0 + r) * patch_ld(n) + k0 + c) : (r == c ? 1.0f : 0.0f);
     }
 }
 
 // Part (a) of a round: inverts pivot block K of patch p (rows and columns
 // [64K, 64K + b)) into its dinv block, zero-padded to 64 x 64; called by all
-// 256 threads of a block.  The 64x64 block D = [[P, B], [C, E]] (32x32
-// quarters, padded with the identity beyond b) is inverted through the Schur
-// complement S = E - C P^-1 B:
-//   D^-1 = [[P^-1 + P^-1 B S^-1 C P^-1, -P^-1 B S^-1], [-S^-1 C P^-1, S^-1]],
-// the two 32x32 inversions by four warps each (quad_invert32), the products by
-// the whole block.  Forming P^-1 explicitly loses accuracy when P is ill
-// conditioned, so the result X is refined by one Newton step,
+// 256 threads of a block.  The 64x64 block D (padded with the identity beyond
+// b) is inverted in place by Gauss-Jordan elimination without pivoting in
+// registers: thread (row r = tid / 4, quarter g = tid % 4) holds D[r][16g ..
+// 16g + 15], so warp w holds rows 8w .. 8w + 7.  The pivots are taken in eight
+// panels of eight (block Gauss-Jordan, two barriers per panel instead of one
+// per pivot; the loop below says how).  Forming the inverse explicitly loses accuracy
+// when D is ill conditioned, so the result X is refined by one Newton step,
 // X <- X + X (I - D X), which squares its residual.  A zero or non-finite
 // pivot clears the patch's ok flag.
 // A: the patch matrix (n x n), dv: its dinv block, ok: its flag, ws: shared
 // memory of at least kInvWs floats.
-constexpr int kInvLq = 33;
 constexpr int kInvWs = 2 * kGjBlock * kInvLd;
 __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int *ok, int K, float *ws) {
-    static_assert(kGjBlock == 64, "two 32x32 quarters");
-    static_assert(2 * 32 * kInvLq <= kGjBlock * kInvLd, "X and Y fit in the second buffer");
-    __shared__ float colbuf[2][32];
-    __shared__ int bad;
+    static_assert(kGjBlock == 64, "four threads of 16 columns per row, eight rows per warp");
     const int k0 = K * kGjBlock;
     const int b = min(kGjBlock, n - k0);
-    float *D = ws, *W = ws + kGjBlock * kInvLd;  // D: the block, then its inverse; W: scratch
-    float *X = W, *Y = W + 32 * kInvLq;
-    load_pivot_block(A, n, k0, b, D);
-    __syncthreads();
-    float *Pq = D, *Bq = D + 32, *Cq = D + 32 * kInvLd, *Eq = Cq + 32;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (w < 4) {  // P^-1 in place
-        float v[8];
+    float *X = ws, *W = ws + kGjBlock * kInvLd;  // X: the inverse; W: D, then I - D X
+    const int r = threadIdx.x >> 2, g = threadIdx.x & 3;
+    const size_t ld = patch_ld(n);
+    float v[16];
+    {
+        const float *Ar = A + (k0 + r) * ld + k0 + 16 * g;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) v[c] = Pq[lane * kInvLd + 8 * w + c];
-        const bool bd = quad_invert32(v, colbuf);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) Pq[lane * kInvLd + 8 * w + c] = v[c];
-        if (threadIdx.x == 0) bad = bd ? 1 : 0;
+        for (int q = 0; q < 16; ++q) {
+            const int c = 16 * g + q;
+            v[q] = (r < b && c < b) ? __ldcg(Ar + q) : (r == c ? 1.0f : 0.0f);
+        }
     }
-    __syncthreads();
-    block_gemm32(Pq, kInvLd, Bq, kInvLd, X, kInvLq, nullptr, 0, 1.0f);  // X = P^-1 B
-    block_gemm32(Cq, kInvLd, Pq, kInvLd, Y, kInvLq, nullptr, 0, 1.0f);  // Y = C P^-1
-    __syncthreads();
-    block_gemm32(Cq, kInvLd, X, kInvLq, Eq, kInvLd, Eq, kInvLd, -1.0f);  // S = E - C X, in place of E
-    __syncthreads();
-    if (w < 4) {  // S^-1 in place
-        float v[8];
+    // Eight panels of eight pivots, panel m held by warp m (rows 8m .. 8m + 7): the warp eliminates the
+    // panel's pivots inside its own rows (pivot rows and column entries by shuffles, no block barrier),
+    // publishes its rows and every other row its entries in the panel's columns, and after one barrier every
+    // other row takes the rank-8 update  x <- [x outside the panel columns] - a_G panel  (block Gauss-Jordan).
+    __shared__ __align__(16) float panel[8][kGjBlock];
+    __shared__ __align__(16) float colg[kGjBlock][8];
+    __shared__ int sbad;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, rl = lane >> 2;
+    if (threadIdx.x == 0) sbad = 0;
+#pragma unroll 1
+    for (int m = 0; m < 8; ++m) {
+        const int cg = m >> 1, half = m & 1;  // the panel's columns 8m + t: chunk cg, element 8 half + t
+        if (w == m) {
+            bool bad = false;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) v[c] = Eq[lane * kInvLd + 8 * w + c];
-        const bool bd = quad_invert32(v, colbuf);
+            for (int t = 0; t < 8; ++t) {
+                float p[16];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) Eq[lane * kInvLd + 8 * w + c] = v[c];
-        if (threadIdx.x == 0 && bd) bad = 1;
+                for (int q = 0; q < 16; ++q) p[q] = __shfl_sync(0xffffffffu, v[q], 4 * t + g);  // pivot row
+                const float mine = half ? v[8 + t] : v[t];
+                const float f = __shfl_sync(0xffffffffu, mine, (lane & ~3) | cg);  // this row's entry, column k
+                const float piv = __shfl_sync(0xffffffffu, mine, 4 * t + cg);
+                bad |= !(fabsf(piv) > 0.0f) || !isfinite(piv);
+                const float ip = __frcp_rn(piv);
+                // v <- a v + b p with (a, b) = (0, 1/piv) in the pivot row, (1, -f/piv) elsewhere; the pivot
+                // column takes b itself
+                const bool own = rl == t;
+                const float a = own ? 0.0f : 1.0f, bq = own ? ip : -f * ip;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) v[q] = fmaf(bq, p[q], a * v[q]);
+                if (g == cg) {
+                    if (half) v[8 + t] = bq;
+                    else v[t] = bq;
+                }
+            }
+            if (bad) sbad = 1;
+#pragma unroll
+            for (int q = 0; q < 16; q += 4)
+                *reinterpret_cast<float4 *>(&panel[rl][16 * g + q]) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+        } else if (g == cg) {
+            const float4 a0 = half ? make_float4(v[8], v[9], v[10], v[11]) : make_float4(v[0], v[1], v[2], v[3]);
+            const float4 a1 = half ? make_float4(v[12], v[13], v[14], v[15]) : make_float4(v[4], v[5], v[6], v[7]);
+            *reinterpret_cast<float4 *>(&colg[r][0]) = a0;
+            *reinterpret_cast<float4 *>(&colg[r][4]) = a1;
+        }
+        __syncthreads();
+        if (w != m) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&colg[r][0]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&colg[r][4]);
+            const float ag[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            if (g == cg) {  // the panel's columns are replaced, not updated
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (half) v[8 + q] = 0.0f;
+                    else v[q] = 0.0f;
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4) {
+                    const float4 pp = *reinterpret_cast<const float4 *>(&panel[t][16 * g + q]);
+                    v[q] = fmaf(-ag[t], pp.x, v[q]);
+                    v[q + 1] = fmaf(-ag[t], pp.y, v[q + 1]);
+                    v[q + 2] = fmaf(-ag[t], pp.z, v[q + 2]);
+                    v[q + 3] = fmaf(-ag[t], pp.w, v[q + 3]);
+                }
+            }
+        }
+        __syncthreads();  // panel and colg are rewritten by the next panel
     }
-    __syncthreads();
-    block_gemm32(X, kInvLq, Eq, kInvLd, Bq, kInvLd, nullptr, 0, -1.0f);  // top right  -X S^-1, in place of B
-    block_gemm32(Eq, kInvLd, Y, kInvLq, Cq, kInvLd, nullptr, 0, -1.0f);  // bottom left -S^-1 Y, in place of C
-    __syncthreads();
-    block_gemm32(Bq, kInvLd, Y, kInvLq, Pq, kInvLd, Pq, kInvLd, -1.0f);  // top left P^-1 - (-X S^-1) Y
-    __syncthreads();
-    // Newton step: W = D again, then W = I - D X, then X + X W straight to dv
+    const bool bad = sbad != 0;
+#pragma unroll
+    for (int q = 0; q < 16; q += 4)
+        *reinterpret_cast<float4 *>(X + r * kInvLd + 16 * g + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+    // Newton step: W = D, then W = I - D X, then X + X W straight to dv
     load_pivot_block(A, n, k0, b, W);
     __syncthreads();
     float acc[4][4];
-    block_gemm64(W, D, acc);
+    block_gemm64(W, X, acc);
     __syncthreads();
     const int r0 = 4 * (threadIdx.x >> 4), c0 = 4 * (threadIdx.x & 15);
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) W[(r0 + u) * kInvLd + c0 + v] = (r0 + u == c0 + v ? 1.0f : 0.0f) - acc[u][v];
+        for (int w = 0; w < 4; ++w) W[(r0 + u) * kInvLd + c0 + w] = (r0 + u == c0 + w ? 1.0f : 0.0f) - acc[u][w];
     __syncthreads();
-    block_gemm64(D, W, acc);
+    block_gemm64(X, W, acc);
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int r = r0 + u, c = c0 + v;
-            dv[r * kGjBlock + c] = (r < b && c < b) ? D[r * kInvLd + c] + acc[u][v] : 0.0f;
+        for (int w = 0; w < 4; ++w) {
+            const int rr = r0 + u, c = c0 + w;
+            dv[rr * kGjBlock + c] = (rr < b && c < b) ? X[rr * kInvLd + c] + acc[u][w] : 0.0f;
         }
     if (threadIdx.x == 0) {
         if (bad) *ok = 0;
@@ -301,12 +295,11 @@ __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int 
 }
 
 __device__ __forceinline__ void pivot_invert_patch(const PatchDev &P, int p, int K, float *ws) {
-    pivot_invert(P.A + P.moff[p], P.nf[p] * P.nbf, P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock, P.ok + p, K,
-                 ws);
+    pivot_invert(P.A + P.moff[p], P.nf[p] * P.nbf, gj_dinv(P, K, p), P.ok + p, K, ws);
 }
 
 // Round 0, part (a): the first pivot block of every patch (later pivot blocks
-// are inverted by the previous round's update, see gj_update_kernel).
+// are inverted inside the rounds, see gj_flow_kernel).
 __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     __shared__ __align__(16) float ws[kInvWs];
     const int p = blockIdx.x;
@@ -315,7 +308,8 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     pivot_invert_patch(P, p, K, ws);
 }
 
-// Round K, part (b), one 64-column tile [j0, j0 + 64) of a patch per block.
+// Round K, part (b), column tile jt [j0, j0 + 64) of patch p, by all 256 threads of a block (sm: kPrepSmem
+// floats of shared memory; the caller checks that K and jt lie inside the patch).
 // The matrix is kept symmetric and only its upper block triangle is
 // maintained, so the pivot rows' entries are
 //   U[s][j] = A[k0 + s][j] for j >= k0,   A[j][k0 + s] for j < k0  (by symmetry);
@@ -328,29 +322,30 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
 // the update pass multiplies them.  Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
 // block's or disjoint from it.  Each thread owns 4 rows x 4 columns of
 // D^-1 U (rows 4ty + u, columns 4tx + v); the loads and stores of the
-// product's operands and results move 16 bytes each.  grid = (tiles, patches).
-__global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
+// product's operands and results move 16 bytes each.  The pivot block's inverse and the rows of A were
+// written by other blocks of the same launch, so they are read past the L1 cache.
+constexpr int kPrepLd = kGjTile + 4;  // 16-byte rows
+constexpr int kPrepSmem = 2 * kGjBlock * kPrepLd;  // floats
+__device__ void gj_prep_tile(const PatchDev &P, int K, int p, int jt, float *sm) {
     static_assert(kGjTile == kGjBlock, "column tiles are pivot-block wide");
-    constexpr int LD = kGjTile + 4;  // 16-byte rows
-    __shared__ __align__(16) float DvT[kGjBlock][LD];  // DvT[s][r] = D^-1[r][s]
-    __shared__ __align__(16) float Us[kGjBlock][LD];
-    const int p = blockIdx.y;
+    constexpr int LD = kPrepLd;
+    float(*DvT)[LD] = reinterpret_cast<float(*)[LD]>(sm);  // DvT[s][r] = D^-1[r][s]
+    float(*Us)[LD] = reinterpret_cast<float(*)[LD]>(sm + kGjBlock * LD);
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
-    const int j0 = blockIdx.x * kGjTile;
-    if (k0 >= n || j0 >= n) return;
+    const int j0 = jt * kGjTile;
     const int b = min(kGjBlock, n - k0);
     const int w = min(kGjTile, n - j0);  // columns in this tile
     const size_t ld = patch_ld(n);
     const float *A = P.A + P.moff[p];
-    float *rs = P.rsplit + (static_cast<size_t>(p) * P.T + blockIdx.x) * 2 * tc::kOperandFloats;
-    float *cs = P.csplit + (static_cast<size_t>(p) * P.T + blockIdx.x) * 2 * tc::kOperandFloats;
-    const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
+    float *rs = P.rsplit + gj_split_off(P, K, p, jt);
+    float *cs = P.csplit + gj_split_off(P, K, p, jt);
+    const float *dv = gj_dinv(P, K, p);
     if (j0 == k0) {  // the pivot columns: -D^-1, and no pivot-row copies
         for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
             const int r = e / kGjTile, c = e - r * kGjTile;
             float h, l;
-            tc::split_tf32(c < w ? -dv[r * kGjBlock + c] : 0.0f, h, l);  // zero-padded rows
+            tc::split_tf32(c < w ? -__ldcg(dv + r * kGjBlock + c) : 0.0f, h, l);  // zero-padded rows
             rs[tc::canon(c, r)] = h;
             rs[tc::kOperandFloats + tc::canon(c, r)] = l;
             cs[tc::canon(c, r)] = 0.0f;
@@ -361,7 +356,7 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     // D^-1, 16-byte loads, stored transposed
     for (int e4 = threadIdx.x; e4 < kGjBlock * kGjBlock / 4; e4 += blockDim.x) {
         const int r = e4 >> 4, c4 = 4 * (e4 & 15);
-        const float4 v = *reinterpret_cast<const float4 *>(dv + r * kGjBlock + c4);
+        const float4 v = __ldcg(reinterpret_cast<const float4 *>(dv + r * kGjBlock + c4));
         DvT[c4][r] = v.x;
         DvT[c4 + 1][r] = v.y;
         DvT[c4 + 2][r] = v.z;
@@ -373,14 +368,14 @@ __global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
         for (int e4 = threadIdx.x; e4 < kGjBlock * kGjTile / 4; e4 += blockDim.x) {
             const int s_ = e4 >> 4, c4 = 4 * (e4 & 15);
             float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (s_ < b && j0 + c4 < static_cast<int>(ld)) v = *reinterpret_cast<const float4 *>(A + (k0 + s_) * ld + j0 + c4);
+            if (s_ < b && j0 + c4 < static_cast<int>(ld)) v = __ldcg(reinterpret_cast<const float4 *>(A + (k0 + s_) * ld + j0 + c4));
             *reinterpret_cast<float4 *>(&Us[s_][c4]) = v;
         }
     } else {  // j0 + 64 <= k0: U[s][c] = A[j0 + c][k0 + s], rows of A read contiguously, stored transposed
         for (int e4 = threadIdx.x; e4 < kGjTile * kGjBlock / 4; e4 += blockDim.x) {
             const int c = e4 >> 4, s4 = 4 * (e4 & 15);
             float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (k0 + s4 < static_cast<int>(ld)) v = *reinterpret_cast<const float4 *>(A + (j0 + c) * ld + k0 + s4);
+            if (k0 + s4 < static_cast<int>(ld)) v = __ldcg(reinterpret_cast<const float4 *>(A + (j0 + c) * ld + k0 + s4));
             Us[s4][c] = v.x;
             Us[s4 + 1][c] = v.y;
             Us[s4 + 2][c] = v.z;
@@ -472,7 +467,7 @@ __device__ __forceinline__ GjTile gj_tile(const PatchDev &P, int K, int T, int i
     return t;
 }
 
-// Stage of the update: the tile's split operands as the prep pass left them
+// Stage of a tile update: the tile's split operands as the prep left them
 // (A = the pivot-row copies of its row tile, B = the scaled pivot rows of its
 // column tile, each a TF32 high part and an FP32 remainder in the canonical
 // layout, 4 x 16 KB).  The old values are read from global memory by the
@@ -481,49 +476,103 @@ __device__ __forceinline__ GjTile gj_tile(const PatchDev &P, int K, int T, int i
 constexpr int kUpStage = 4 * tc::kOperandFloats;
 constexpr size_t kUpdateSmem = kUpStage * sizeof(float);
 
-// Issues the 16-byte copies of a tile's operands into `stage` (contiguous blocks: 8 + 8 chunks per thread;
-// the pivot rows need B only).
-__device__ __forceinline__ void gj_issue_tile(const PatchDev &P, const GjTile &t, float *stage) {
+// Issues the 16-byte copies of a round-K tile's operands into `stage` (contiguous blocks: 8 + 8 chunks per
+// thread; the pivot rows need B only).  cp.async.cg reads through L2, past the L1 cache.
+__device__ __forceinline__ void gj_issue_tile(const PatchDev &P, int K, const GjTile &t, float *stage) {
     float *Ab = stage, *Bb = stage + 2 * tc::kOperandFloats;
-    const float *csrc = P.csplit + (static_cast<size_t>(t.p) * P.T + t.row0 / kGjTile) * 2 * tc::kOperandFloats;
-    const float *rsrc = P.rsplit + (static_cast<size_t>(t.p) * P.T + t.col0 / kGjTile) * 2 * tc::kOperandFloats;
+    const float *csrc = P.csplit + gj_split_off(P, K, t.p, t.row0 / kGjTile);
+    const float *rsrc = P.rsplit + gj_split_off(P, K, t.p, t.col0 / kGjTile);
     for (int c = threadIdx.x; c < 2 * tc::kOperandFloats / 4; c += blockDim.x) {
         cp_async16(Bb + 4 * c, rsrc + 4 * c, true);
         if (!t.prow) cp_async16(Ab + 4 * c, csrc + 4 * c, true);
     }
 }
 
-// Round K, part (c), the 64x64 tiles of the upper block triangle:
+// Dependency flags of the refresh (P.flow, zeroed before each refresh; int each):
+//   [0] the next work item, [1] dead: a wait gave up (later waits give up at once),
+//   tile_round[p][i][j]  rounds of updates finished on tile (i, j), i <= j,
+//   prep_done[p][j][K&1] 1 + the last round K of that parity whose prep of column tile j has finished,
+//   inv_done[p]          1 + the last pivot block inverted (block 0 is inverted before the launch).
+__device__ __forceinline__ int *flow_dead(const PatchDev &P) { return P.flow + 1; }
+__device__ __forceinline__ int *flow_tile(const PatchDev &P, int p, int i, int j) {
+    return P.flow + 2 + (static_cast<size_t>(p) * P.T + i) * P.T + j;
+}
+__device__ __forceinline__ int *flow_prep(const PatchDev &P, int p, int j, int K) {
+    return P.flow + 2 + static_cast<size_t>(P.np) * P.T * P.T + (static_cast<size_t>(p) * P.T + j) * 2 + (K & 1);
+}
+__device__ __forceinline__ int *flow_inv(const PatchDev &P, int p) {
+    return P.flow + 2 + static_cast<size_t>(P.np) * P.T * (P.T + 2) + p;
+}
+__host__ __device__ __forceinline__ size_t flow_ints(int np, int T) {
+    return 2 + static_cast<size_t>(np) * T * (T + 2) + np;
+}
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Polls *flag until it reaches `target` (thread-level); false when it gave up: after kFlowWaitLimit polls
+// (an L2 round trip and a 128 ns sleep each: about a second), or soon after another wait has given up.
+constexpr uint32_t kFlowWaitLimit = 1u << 20;
+__device__ bool flow_poll(const PatchDev &P, const int *flag, int target) {
+    for (uint32_t it = 0; it < kFlowWaitLimit; ++it) {
+        if (ld_acquire(flag) >= target) return true;
+        if ((it & 63) == 63 && ld_acquire(flow_dead(P))) return false;
+        __nanosleep(128);
+    }
+    atomicExch(flow_dead(P), 1);
+    return false;
+}
+
+// Publishes an item: the block's writes (ordered before thread 0's release by the barrier), then the flag,
+// raised to `value` (flags only grow).  All threads.
+__device__ __forceinline__ void flow_release(int *flag, int value) {
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("red.release.gpu.global.max.s32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
+}
+
+// The Gauss-Jordan rounds of every patch in one launch, as a dataflow over work items.  Items are handed out
+// in a fixed order by one counter: round by round, in each round first the prep of every column tile
+// (gj_prep_tile, part (b)), then the update of every tile of the upper block triangle (part (c)):
 //   pivot rows       A[i, j] = rbuf[i - k0][j]      (-D^-1 in the pivot block)
 //   other rows       A[i, j] -= C_i . rbuf[:, j]   (j outside the pivot columns)
 //                    A[i, j]  = -C_i . rbuf[:, j]  (pivot columns: C_i D^-1)
-// with C_i = cbuf[:][i] (the pivot-row copies) and rbuf the scaled pivot rows
-// -- the symmetric sweep, which leaves -A^-1 after the last round.  Tiles and
-// pivot blocks are both 64 wide, so a tile lies in the pivot rows (ti == K, a
-// copy), in the pivot columns (tj == K) or in neither.  Persistent blocks (two
-// per SM) take tiles from a per-round counter.  The tile product C^T rbuf runs
-// on the tensor cores (tc_tf32.cuh: the operands as the prep pass split them,
-// three TF32 products accumulated in FP32 in tensor memory, issued by one
-// thread and committed to an mbarrier).  Read-back: warp w holds tile rows
-// 16 (w % 4) .. + 15 in lanes 0-15 and columns 32 (w / 4) .. + 31; each lane
-// pair (l, l + 16) then splits the 32 columns, so every thread writes 16
-// columns of one row.  The block that takes a patch's diagonal tile
-// (K + 1, K + 1) inverts it for the next round right after its update, while
-// the other blocks go on with the rest.  A wait for the products that gives up
-// (bounded) marks the tile's patch unusable -- it falls back to the
-// block-diagonal preconditioner -- and the block computes no further products.
-// Dynamic shared memory: kUpdateSmem.
-__global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, int T, int *counter) {
+// with C_i = cbuf[:][i] (the pivot-row copies) and rbuf the scaled pivot rows -- the symmetric sweep, which
+// leaves -A^-1 after the last round.  Tiles and pivot blocks are both 64 wide, so a tile lies in the pivot
+// rows (ti == K, a copy), in the pivot columns (tj == K) or in neither.  The block that updates a patch's
+// diagonal tile (K + 1, K + 1) inverts it for the next round (part (a)).  Instead of a launch per round,
+// each item waits for the items it reads from:
+//   prep (K, j):      the inverse of pivot block K; tile (K, j) after round K - 1; and, before it overwrites
+//                     its round-parity buffers, every tile of row and column j after round K - 2;
+//   update (K, i, j): tile (i, j) after round K - 1; the preps (K, i) and (K, j);
+//   inverse K + 1:    before it overwrites its parity's inverse, the preps of round K - 1.
+// Every wait is for items handed out earlier, so the block holding the oldest unfinished item never waits
+// and the launch always drains; the waits are bounded (flow_poll).  An item whose wait gave up is released
+// without its work and its patch falls back to the block-diagonal preconditioner; the wait marks the launch
+// dead, so that every later wait that is not already satisfied gives up at once and the launch ends soon.  Round operands (csplit, rsplit) and inverses are double-buffered by round
+// parity (gj_split_off, gj_dinv); data written by other blocks is read past the L1 cache.  The tile product
+// C^T rbuf runs on the tensor cores (tc_tf32.cuh: the operands as the prep split them, three TF32 products
+// accumulated in FP32 in tensor memory, issued by one thread and committed to an mbarrier).  Read-back: warp
+// w holds tile rows 16 (w % 4) .. + 15 in lanes 0-15 and columns 32 (w / 4) .. + 31; each lane pair
+// (l, l + 16) then splits the 32 columns, so every thread writes 16 columns of one row.  A wait for the
+// products that gives up (bounded) marks the tile's patch unusable and the block computes no further
+// products.  Persistent blocks (two per SM); dynamic shared memory: kUpdateSmem.
+__global__ void __launch_bounds__(256, 2) gj_flow_kernel(PatchDev P) {
     static_assert(kGjTile == 64 && kGjBlock == 64 && tc::kTileMN == 64 && tc::kTileK == 64, "64-wide tiles");
-    static_assert(kUpStage >= kInvWs, "the inversion reuses the stage");
+    static_assert(kUpStage >= kInvWs && kUpStage >= kPrepSmem, "the inversion and the prep reuse the stage");
     extern __shared__ __align__(128) float usm[];
     __shared__ int next_item;
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tbase;
-    __shared__ int tc_ok, dead;
-    const int total = P.np * (T * (T + 1) / 2);
+    __shared__ int tc_ok, tc_dead;
+    chain_wait();
+    const int T = P.T;
+    const int prep_items = P.np * T, per_round = P.np * (T + T * (T + 1) / 2);
+    const int total = per_round * T;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) next_item = atomicAdd(P.flow, 1);
     __syncthreads();
     int item = next_item;
     if (item >= total) return;
@@ -531,7 +580,7 @@ __global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, in
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
         fence_barrier_init();
-        dead = 0;
+        tc_dead = 0;
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -541,109 +590,144 @@ __global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, in
     const float *Ab = usm, *Bb = usm + 2 * tc::kOperandFloats;
     // this thread's output: tile row tr, columns tc0 .. tc0 + 15
     const int tr = 16 * (warp & 3) + (lane & 15), tc0 = 32 * (warp >> 2) + 16 * (lane >> 4);
+    int ahead = 0;  // thread 0: the item after this one, taken while this one runs
     while (item < total) {
-        const GjTile cur = gj_tile(P, K, T, item);
-        if (cur.valid) {
-            gj_issue_tile(P, cur, usm);
-            cp_async_commit();
-            const int n = cur.n, ld = patch_ld(n);
-            const int i = cur.row0 + tr, j = cur.col0 + tc0;
-            float *Arow = P.A + P.moff[cur.p] + static_cast<size_t>(i) * ld + j;
-            // the old values, while the operands land (the pivot columns and rows are overwritten)
-            float res[16];
-#pragma unroll
-            for (int q = 0; q < 16; ++q) res[q] = 0.0f;
-            if (!cur.prow && !cur.pcol && i < n) {
-#pragma unroll
-                for (int q = 0; q < 16; q += 4) {
-                    if (j + q < ld) {
-                        const float4 o4 = *reinterpret_cast<const float4 *>(Arow + q);
-                        res[q] = o4.x;
-                        res[q + 1] = o4.y;
-                        res[q + 2] = o4.z;
-                        res[q + 3] = o4.w;
-                    }
-                }
+        if (threadIdx.x == 0) ahead = atomicAdd(P.flow, 1);
+        const int K = item / per_round, rem = item - K * per_round;
+        if (rem < prep_items) {  // prep of column tile j, the round's next pivot column first
+            const int p = rem % P.np, j = (K + 1 + rem / P.np) % T;
+            const int n = P.nf[p] * P.nbf, Tp = (n + kGjTile - 1) / kGjTile;
+            if (K < Tp && j < Tp) {
+                // the waits run in parallel, one flag per polling thread
+                bool ok = true;
+                const int t = static_cast<int>(threadIdx.x) - 64;
+                if (K > 0 && threadIdx.x == 0) ok = flow_poll(P, flow_inv(P, p), K + 1);
+                if (K > 0 && threadIdx.x == 32) ok = flow_poll(P, flow_tile(P, p, min(K, j), max(K, j)), K);
+                if (K >= 2 && t >= 0 && t < Tp) ok = flow_poll(P, flow_tile(P, p, min(t, j), max(t, j)), K - 1);
+                if (__syncthreads_and(ok)) gj_prep_tile(P, K, p, j, usm);
+                else if (threadIdx.x == 0) P.ok[p] = 0;
+                flow_release(flow_prep(P, p, j, K), K + 1);
             }
-            cp_async_wait<0>();
-            tc::fence_proxy_async();  // the operands are visible to the tensor cores
-            tc::fence_before_sync();
-            __syncthreads();
-            tc::fence_after_sync();
-            bool have = true;
-            if (cur.prow) {  // the pivot rows: the scaled pivot rows themselves (row0 == k0), high + low parts
+        } else {
+            const GjTile cur = gj_tile(P, K, T, rem - prep_items);
+            if (cur.valid) {
+                const int ti = cur.row0 / kGjTile, tj = cur.col0 / kGjTile;
+                bool ok = true;  // the waits run in parallel, one flag per polling thread
+                if (K > 0 && threadIdx.x == 0) ok = flow_poll(P, flow_tile(P, cur.p, ti, tj), K);
+                if (threadIdx.x == 32) ok = flow_poll(P, flow_prep(P, cur.p, tj, K), K + 1);
+                if (!cur.prow && threadIdx.x == 64) ok = flow_poll(P, flow_prep(P, cur.p, ti, K), K + 1);
+                const bool go = __syncthreads_and(ok);
+                if (go) {
+                    gj_issue_tile(P, K, cur, usm);
+                    cp_async_commit();
+                    const int n = cur.n, ld = patch_ld(n);
+                    const int i = cur.row0 + tr, j = cur.col0 + tc0;
+                    float *Arow = P.A + P.moff[cur.p] + static_cast<size_t>(i) * ld + j;
+                    // the old values, while the operands land (the pivot columns and rows are overwritten)
+                    float res[16];
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int e = tc::canon(tc0 + q, tr);
-                    res[q] = Bb[e] + Bb[tc::kOperandFloats + e];
-                }
-            } else if (dead) {
-                have = false;
-            } else {
-                if (threadIdx.x == 0) {
-                    tc::issue_tile_products(tmem, Ab, Ab + tc::kOperandFloats, Bb, Bb + tc::kOperandFloats);
-                    tc::commit(&bar);
-                    bool ok = mbar_wait_bounded(&bar, products & 1u);
-                    if (!ok) ok = mbar_wait_bounded(&bar, products & 1u);  // drain before going on
-                    tc_ok = ok ? 1 : 0;
-                    if (!ok) {
-                        dead = 1;
-                        P.ok[cur.p] = 0;
-                    }
-                }
-                ++products;
-                __syncthreads();
-                tc::fence_after_sync();
-                have = tc_ok != 0;
-                if (have) {
-                    float v[32];
-                    tc::tmem_ld32(tc::tmem_addr(tmem, warp, 32 * (warp >> 2)), v);
-                    // lanes l and l + 16 share row l's 32 columns: l keeps 0..15, l + 16 takes 16..31
+                    for (int q = 0; q < 16; ++q) res[q] = 0.0f;
+                    if (!cur.prow && !cur.pcol && i < n) {
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) {
-                        const float hi16 = __shfl_sync(0xffffffffu, v[16 + q], lane & 15);
-                        res[q] -= (lane < 16) ? v[q] : hi16;
-                    }
-                    tc::fence_before_sync();
-                }
-            }
-            if (have) {
-                // the patch's last round writes its final values: a non-finite one marks the inverse unusable
-                const bool last = (K + 1) * kGjBlock >= n;
-                bool bad = false;
-                if (i < n) {
-#pragma unroll
-                    for (int q = 0; q < 16; q += 4) {
-                        if (j + q + 3 < n) {
-                            *reinterpret_cast<float4 *>(Arow + q) = make_float4(res[q], res[q + 1], res[q + 2], res[q + 3]);
-                        } else {  // the row's last, partial chunk: nothing beyond column n - 1
-#pragma unroll
-                            for (int u = 0; u < 4; ++u)
-                                if (j + q + u < n) Arow[q + u] = res[q + u];
+                        for (int q = 0; q < 16; q += 4) {
+                            if (j + q < ld) {
+                                const float4 o4 = __ldcg(reinterpret_cast<const float4 *>(Arow + q));
+                                res[q] = o4.x;
+                                res[q + 1] = o4.y;
+                                res[q + 2] = o4.z;
+                                res[q + 3] = o4.w;
+                            }
                         }
                     }
-                    if (last)
+                    cp_async_wait<0>();
+                    tc::fence_proxy_async();  // the operands are visible to the tensor cores
+                    tc::fence_before_sync();
+                    __syncthreads();
+                    tc::fence_after_sync();
+                    bool have = true;
+                    if (cur.prow) {  // the pivot rows: the scaled pivot rows themselves (row0 == k0), high + low parts
 #pragma unroll
-                        for (int q = 0; q < 16; ++q) bad |= (j + q < n) && !isfinite(res[q]);
-                }
-                if (bad) P.ok[cur.p] = 0;
-                if (last && cur.row0 < cur.col0 && i < n) {
-                    // final values: also the transposed tile of the lower block triangle (A^-1 is symmetric)
-                    float *At = P.A + P.moff[cur.p] + i;
+                        for (int q = 0; q < 16; ++q) {
+                            const int e = tc::canon(tc0 + q, tr);
+                            res[q] = Bb[e] + Bb[tc::kOperandFloats + e];
+                        }
+                    } else if (tc_dead) {
+                        have = false;
+                    } else {
+                        if (threadIdx.x == 0) {
+                            tc::issue_tile_products(tmem, Ab, Ab + tc::kOperandFloats, Bb, Bb + tc::kOperandFloats);
+                            tc::commit(&bar);
+                            bool done = mbar_wait_bounded(&bar, products & 1u);
+                            if (!done) done = mbar_wait_bounded(&bar, products & 1u);  // drain before going on
+                            tc_ok = done ? 1 : 0;
+                            if (!done) {
+                                tc_dead = 1;
+                                P.ok[cur.p] = 0;
+                            }
+                        }
+                        ++products;
+                        __syncthreads();
+                        tc::fence_after_sync();
+                        have = tc_ok != 0;
+                        if (have) {
+                            float v[32];
+                            tc::tmem_ld32(tc::tmem_addr(tmem, warp, 32 * (warp >> 2)), v);
+                            // lanes l and l + 16 share row l's 32 columns: l keeps 0..15, l + 16 takes 16..31
 #pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        if (j + q < n) At[static_cast<size_t>(j + q) * ld] = res[q];
+                            for (int q = 0; q < 16; ++q) {
+                                const float hi16 = __shfl_sync(0xffffffffu, v[16 + q], lane & 15);
+                                res[q] -= (lane < 16) ? v[q] : hi16;
+                            }
+                            tc::fence_before_sync();
+                        }
+                    }
+                    if (have) {
+                        // the patch's last round writes its final values: a non-finite one marks the inverse unusable
+                        const bool last = (K + 1) * kGjBlock >= n;
+                        bool bad = false;
+                        if (i < n) {
+#pragma unroll
+                            for (int q = 0; q < 16; q += 4) {
+                                if (j + q + 3 < n) {
+                                    *reinterpret_cast<float4 *>(Arow + q) = make_float4(res[q], res[q + 1], res[q + 2], res[q + 3]);
+                                } else {  // the row's last, partial chunk: nothing beyond column n - 1
+#pragma unroll
+                                    for (int u = 0; u < 4; ++u)
+                                        if (j + q + u < n) Arow[q + u] = res[q + u];
+                                }
+                            }
+                            if (last)
+#pragma unroll
+                                for (int q = 0; q < 16; ++q) bad |= (j + q < n) && !isfinite(res[q]);
+                        }
+                        if (bad) P.ok[cur.p] = 0;
+                        if (last && cur.row0 < cur.col0 && i < n) {
+                            // final values: also the transposed tile of the lower block triangle (A^-1 is symmetric)
+                            float *At = P.A + P.moff[cur.p] + i;
+#pragma unroll
+                            for (int q = 0; q < 16; ++q)
+                                if (j + q < n) At[static_cast<size_t>(j + q) * ld] = res[q];
+                        }
+                    } else if (threadIdx.x == 0) {
+                        P.ok[cur.p] = 0;
+                    }
+                } else if (threadIdx.x == 0) {
+                    P.ok[cur.p] = 0;
                 }
-            } else if (threadIdx.x == 0) {
-                P.ok[cur.p] = 0;
-            }
-            if (cur.diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
-                __syncthreads();
-                pivot_invert_patch(P, cur.p, K + 1, usm);
+                flow_release(flow_tile(P, cur.p, ti, tj), K + 1);
+                if (cur.diag) {  // the tile is final for round K + 1: invert it now
+                    const int Tp = (cur.n + kGjTile - 1) / kGjTile;
+                    bool ok2 = go;
+                    if (K >= 1 && static_cast<int>(threadIdx.x) < Tp)
+                        ok2 = flow_poll(P, flow_prep(P, cur.p, threadIdx.x, K - 1), K) && ok2;
+                    if (__syncthreads_and(ok2)) pivot_invert_patch(P, cur.p, K + 1, usm);
+                    else if (threadIdx.x == 0) P.ok[cur.p] = 0;
+                    flow_release(flow_inv(P, cur.p), K + 2);
+                }
             }
         }
         __syncthreads();  // every thread is done with the stage and with next_item
-        if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) next_item = ahead;
         __syncthreads();
         item = next_item;
     }
@@ -735,6 +819,7 @@ __global__ void __launch_bounds__(kArnThreads, 4) patch_arnoldi_kernel(SimDev d,
                                                                        cudaGraphConditionalHandle h) {
     extern __shared__ __align__(16) double xs[];
     __shared__ double sm32[32];
+    chain_wait();
     const int p = blockIdx.y, a = blockIdx.x / kArnParts, part = blockIdx.x % kArnParts;
     if (p == 0 && blockIdx.x == 0 && threadIdx.x == 0) set_loop(h, d.lc, 0);
     if (a >= P.nf[p]) return;

@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_kernel(SymP
 // tile of the pair), so that both these writes and the per-segment reduction
 // that reads them are coalesced.
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_batch_kernel(SymBatchParams p) {
+    chain_wait();
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int src_lane = (lane + 1) & 31;
@@ -666,8 +667,7 @@ namespace cufil {
 
 int rpy_launch_sym_batch(const SymBatchParams &p, int grid, cudaStream_t st) {
     if (p.items <= 0) return CF_OK;
-    rpy_wall_sym_batch_kernel<<<grid, kThreads, 0, st>>>(p);
-    CF_CHECK_LAUNCH("rpy_wall_sym_batch_kernel");
+    CF_CUDA(launch_chained(rpy_wall_sym_batch_kernel, dim3(grid), dim3(kThreads), 0, st, p));
     return CF_OK;
 }
 

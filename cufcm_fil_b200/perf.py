@@ -1,7 +1,8 @@
 """Measurement entry points (the command lines of the committed profiles).
 
-  python -m cufcm_fil_b200.perf step --nx 16 --precond line --steps 2
-      implicit steps of the benchmark lattice (lattice_simulation); with
+  python -m cufcm_fil_b200.perf step --nx 16 --precond line --steps 2 [--warm W]
+      implicit steps of the benchmark lattice (lattice_simulation), each timed
+      with CUDA events, and a fit of step time against GMRES iterations; with
       CUFIL_NO_GRAPH=1 every kernel is an ordinary launch, which is what a
       profiler's launch list needs.
   python -m cufcm_fil_b200.perf fcm --grid 512 --reps 5
@@ -10,6 +11,10 @@
       bandwidth of spreading and interpolation against their algorithmic bytes
       (spread: N ngd^3 x 3 read-modify-writes of 4 bytes each way; gather:
       N ngd^3 x 3 reads of 4 bytes).
+  python -m cufcm_fil_b200.perf refresh --nx 16 --reps 20
+      one rebuild of the line-patch inverses of the benchmark lattice after its
+      first step (assembly + the Gauss-Jordan rounds), CUDA events on the
+      engine's stream, L2 flushed before each rebuild: mean and minimum.
   python -m cufcm_fil_b200.perf mlp --batch 1024 --reps 50
       forward passes of the learned preconditioner's network (182 -> 256 -> 256
       -> 62, BF16 GEMMs) at one filament per row, as one GMRES iteration of the
@@ -26,12 +31,69 @@ import numpy as np
 from . import _lib
 
 
-def run_steps(nx: int, precond: str, steps: int, line_patch: int = 0):
+def run_steps(nx: int, precond: str, steps: int, line_patch: int = 0, warm: int = 0):
+    """`warm` untimed steps, then `steps` implicit steps, each timed with CUDA events on the engine's stream
+    (without warm-up steps the first includes the graph capture).  With three or more timed steps, a
+    least-squares fit step_ms = fixed_ms + ms_per_iteration * iterations splits the step time into the
+    per-step part (kinematics, right-hand side, refresh, finish) and the cost of one GMRES iteration."""
+    import torch
     from .sim import lattice_simulation
     code = {"line": _lib.CF_PRECOND_LINE, "block": _lib.CF_PRECOND_BLOCK_DIAG, "none": _lib.CF_PRECOND_NONE}[precond]
+    its, ms = [], []
     with lattice_simulation(nx, precond=code, line_patch=line_patch) as sim:
-        its = [sim.step(nt).iterations for nt in range(steps)]
-    return {"nx": nx, "precond": precond, "steps": steps, "gmres_iterations": its}
+        stream = torch.cuda.ExternalStream(sim.stream_handle())
+        for nt in range(warm):
+            sim.step(nt)
+        torch.cuda.synchronize()
+        for nt in range(warm, warm + steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            its.append(sim.step(nt).iterations)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+    out = {"nx": nx, "precond": precond, "warm": warm, "steps": steps, "gmres_iterations": its, "step_ms": ms}
+    if steps >= 3 and len(set(its)) > 1:
+        slope, icpt = np.polyfit(np.asarray(its, float), np.asarray(ms, float), 1)
+        out.update(fixed_ms=float(icpt), ms_per_iteration=float(slope), mean_step_ms=float(np.mean(ms)))
+    return out
+
+
+def warm_up(fn, seconds: float = 1.0):
+    """Repeats `fn` for about `seconds` of device time, so that the GPU has left its idle clocks before the
+    timed launches (short runs otherwise start at a fraction of the boost clock)."""
+    import time
+    import torch
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds or n < 3:
+        fn()
+        n += 1
+        if n % 16 == 0:
+            torch.cuda.synchronize()
+    torch.cuda.synchronize()
+
+
+def run_refresh(nx: int, reps: int):
+    import torch
+    from .sim import lattice_simulation
+    with lattice_simulation(nx, precond=_lib.CF_PRECOND_LINE) as sim:
+        sim.step(0)
+        stream = torch.cuda.ExternalStream(sim.stream_handle())
+        flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MiB, twice the L2
+        warm_up(lambda: sim.refresh_preconditioner())
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for a, b in ev:
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a.record(stream)
+            sim.refresh_preconditioner()
+            with torch.cuda.stream(stream):
+                b.record(stream)
+        torch.cuda.synchronize()
+        ms = [a.elapsed_time(b) for a, b in ev]
+    return {"nx": nx, "reps": reps, "refresh_ms_mean": float(np.mean(ms)), "refresh_ms_min": float(np.min(ms))}
 
 
 def run_fcm(grid: int, reps: int, hbm_gbs: float | None = None):
@@ -79,8 +141,7 @@ def run_mlp(batch: int, reps: int):
         y = torch.empty(batch, 62, device="cuda")
         st = torch.cuda.Stream()
         torch.cuda.synchronize()
-        for _ in range(5):
-            net.forward(x, y, stream=st)
+        warm_up(lambda: net.forward(x, y, stream=st), 0.5)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
         for a, b in ev:  # events on the stream the network's kernels run on
             a.record(st)
@@ -101,16 +162,22 @@ def main(argv=None):
     st.add_argument("--precond", choices=["line", "block", "none"], default="line")
     st.add_argument("--steps", type=int, default=2)
     st.add_argument("--line-patch", type=int, default=0)
+    st.add_argument("--warm", type=int, default=0)
     fc = sub.add_parser("fcm")
     fc.add_argument("--grid", type=int, default=512)
     fc.add_argument("--reps", type=int, default=5)
     fc.add_argument("--hbm-gbs", type=float, default=None)
+    rf = sub.add_parser("refresh")
+    rf.add_argument("--nx", type=int, default=16)
+    rf.add_argument("--reps", type=int, default=20)
     ml = sub.add_parser("mlp")
     ml.add_argument("--batch", type=int, default=1024)
     ml.add_argument("--reps", type=int, default=50)
     a = ap.parse_args(argv)
     if a.what == "step":
-        print(json.dumps(run_steps(a.nx, a.precond, a.steps, a.line_patch)))
+        print(json.dumps(run_steps(a.nx, a.precond, a.steps, a.line_patch, a.warm)))
+    elif a.what == "refresh":
+        print(json.dumps(run_refresh(a.nx, a.reps)))
     elif a.what == "mlp":
         print(json.dumps(run_mlp(a.batch, a.reps)))
     else:
