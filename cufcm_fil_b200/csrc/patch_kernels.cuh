@@ -48,24 +48,15 @@ struct PatchDev {
     const long long *roff;   // first entry of each patch in `rows` [np]
     const long long *rows;   // batch-vector row of each local unknown
     float *A;                // patch matrices, then their inverses (row-major n x n, row stride patch_ld(n))
-    // Round operands of the tile update, per round parity, patch and 64-column tile, split for the tensor
-    // cores (tc_tf32.cuh: a TF32 high part and an FP32 remainder, 4096 floats each, canonical K-major
+    // Round operands of the tile update, per patch and 64-column tile, split for the tensor cores
+    // (tc_tf32.cuh: a TF32 high part and an FP32 remainder, 4096 floats each, canonical K-major
     // layout with k the pivot row s and m or n the tile column c):
-    float *csplit;           // the pivot-row copies U[s][c], [2][np][T][2][4096]
+    float *csplit;           // the pivot-row copies U[s][c], [np][T][2][4096]
     float *rsplit;           // the scaled pivot rows (D^-1 U)[s][c] (-D^-1 in the pivot columns), same shape
-    float *dinv;             // inverted pivot blocks, [2][np][kGjBlock][kGjBlock] (round parity)
+    float *dinv;             // inverted pivot blocks, [np][kGjBlock][kGjBlock]
     int *ok;                 // [np] 1 when the inverse is finite
-    int *flow;               // dependency flags of the refresh (gj_flow_kernel), flow_ints(np, T)
+    int *counter;            // per-round tile counters of the update [rounds]
 };
-
-// Round K's operand buffers of column tile t of patch p, and its pivot block's inverse: round parity
-// K & 1, so that one round's prep can run while the previous round's updates still read theirs.
-__device__ __forceinline__ size_t gj_split_off(const PatchDev &P, int K, int p, int t) {
-    return ((static_cast<size_t>(K & 1) * P.np + p) * P.T + t) * 2 * tc::kOperandFloats;
-}
-__device__ __forceinline__ float *gj_dinv(const PatchDev &P, int K, int p) {
-    return P.dinv + (static_cast<size_t>(K & 1) * P.np + p) * 64 * 64;
-}
 
 // Row stride of a patch system of n unknowns: rows start on 16 bytes, so tiles
 // move in 16-byte copies.  The padding columns [n, ld) are never part of a result.
@@ -159,7 +150,7 @@ __device__ __forceinline__ void block_gemm64(const float *L, const float *R, flo
 __device__ __forceinline__ void load_pivot_block(const float *A, int n, int k0, int b, float *M) {
     for (int e = threadIdx.x; e < kGjBlock * kGjBlock; e += blockDim.x) {
         const int r = e >> 6, c = e & 63;
-        M[r * kInvLd + c] = (r < b && c < b) ? __ldcg(A + static_cast<size_t>(k0 + r) * patch_ld(n) + k0 + c) : (r == c ? 1.0f : 0.0f);
+        M[r * kInvLd + c] = (r < b && c < b) ? A[static_cast<size_t>(k0 + r) * patch_ld(n) + k0 + c] : (r == c ? 1.0f : 0.0f);
     }
 }
 
@@ -190,7 +181,7 @@ __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int 
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             const int c = 16 * g + q;
-            v[q] = (r < b && c < b) ? __ldcg(Ar + q) : (r == c ? 1.0f : 0.0f);
+            v[q] = (r < b && c < b) ? Ar[q] : (r == c ? 1.0f : 0.0f);
         }
     }
     // Eight panels of eight pivots, panel m held by warp m (rows 8m .. 8m + 7): the warp eliminates the
@@ -295,11 +286,12 @@ __device__ __noinline__ void pivot_invert(const float *A, int n, float *dv, int 
 }
 
 __device__ __forceinline__ void pivot_invert_patch(const PatchDev &P, int p, int K, float *ws) {
-    pivot_invert(P.A + P.moff[p], P.nf[p] * P.nbf, gj_dinv(P, K, p), P.ok + p, K, ws);
+    pivot_invert(P.A + P.moff[p], P.nf[p] * P.nbf, P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock, P.ok + p, K,
+                 ws);
 }
 
 // Round 0, part (a): the first pivot block of every patch (later pivot blocks
-// are inverted inside the rounds, see gj_flow_kernel).
+// are inverted by the previous round's update, see gj_update_kernel).
 __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     __shared__ __align__(16) float ws[kInvWs];
     const int p = blockIdx.x;
@@ -308,8 +300,7 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
     pivot_invert_patch(P, p, K, ws);
 }
 
-// Round K, part (b), column tile jt [j0, j0 + 64) of patch p, by all 256 threads of a block (sm: kPrepSmem
-// floats of shared memory; the caller checks that K and jt lie inside the patch).
+// Round K, part (b), one 64-column tile [j0, j0 + 64) of a patch per block.
 // The matrix is kept symmetric and only its upper block triangle is
 // maintained, so the pivot rows' entries are
 //   U[s][j] = A[k0 + s][j] for j >= k0,   A[j][k0 + s] for j < k0  (by symmetry);
@@ -322,30 +313,30 @@ __global__ void __launch_bounds__(256) gj_pivot_kernel(PatchDev P, int K) {
 // the update pass multiplies them.  Tiles and pivot blocks are both 64 wide, so a tile is either the pivot
 // block's or disjoint from it.  Each thread owns 4 rows x 4 columns of
 // D^-1 U (rows 4ty + u, columns 4tx + v); the loads and stores of the
-// product's operands and results move 16 bytes each.  The pivot block's inverse and the rows of A were
-// written by other blocks of the same launch, so they are read past the L1 cache.
-constexpr int kPrepLd = kGjTile + 4;  // 16-byte rows
-constexpr int kPrepSmem = 2 * kGjBlock * kPrepLd;  // floats
-__device__ void gj_prep_tile(const PatchDev &P, int K, int p, int jt, float *sm) {
+// product's operands and results move 16 bytes each.  grid = (tiles, patches).
+__global__ void __launch_bounds__(256) gj_prep_kernel(PatchDev P, int K) {
     static_assert(kGjTile == kGjBlock, "column tiles are pivot-block wide");
-    constexpr int LD = kPrepLd;
-    float(*DvT)[LD] = reinterpret_cast<float(*)[LD]>(sm);  // DvT[s][r] = D^-1[r][s]
-    float(*Us)[LD] = reinterpret_cast<float(*)[LD]>(sm + kGjBlock * LD);
+    constexpr int LD = kGjTile + 4;  // 16-byte rows
+    __shared__ __align__(16) float DvT[kGjBlock][LD];  // DvT[s][r] = D^-1[r][s]
+    __shared__ __align__(16) float Us[kGjBlock][LD];
+    chain_wait();
+    const int p = blockIdx.y;
     const int n = P.nf[p] * P.nbf;
     const int k0 = K * kGjBlock;
-    const int j0 = jt * kGjTile;
+    const int j0 = blockIdx.x * kGjTile;
+    if (k0 >= n || j0 >= n) return;
     const int b = min(kGjBlock, n - k0);
     const int w = min(kGjTile, n - j0);  // columns in this tile
     const size_t ld = patch_ld(n);
     const float *A = P.A + P.moff[p];
-    float *rs = P.rsplit + gj_split_off(P, K, p, jt);
-    float *cs = P.csplit + gj_split_off(P, K, p, jt);
-    const float *dv = gj_dinv(P, K, p);
+    float *rs = P.rsplit + (static_cast<size_t>(p) * P.T + blockIdx.x) * 2 * tc::kOperandFloats;
+    float *cs = P.csplit + (static_cast<size_t>(p) * P.T + blockIdx.x) * 2 * tc::kOperandFloats;
+    const float *dv = P.dinv + static_cast<size_t>(p) * kGjBlock * kGjBlock;
     if (j0 == k0) {  // the pivot columns: -D^-1, and no pivot-row copies
         for (int e = threadIdx.x; e < kGjBlock * kGjTile; e += blockDim.x) {
             const int r = e / kGjTile, c = e - r * kGjTile;
             float h, l;
-            tc::split_tf32(c < w ? -__ldcg(dv + r * kGjBlock + c) : 0.0f, h, l);  // zero-padded rows
+            tc::split_tf32(c < w ? -dv[r * kGjBlock + c] : 0.0f, h, l);  // zero-padded rows
             rs[tc::canon(c, r)] = h;
             rs[tc::kOperandFloats + tc::canon(c, r)] = l;
             cs[tc::canon(c, r)] = 0.0f;
@@ -356,7 +347,7 @@ __device__ void gj_prep_tile(const PatchDev &P, int K, int p, int jt, float *sm)
     // D^-1, 16-byte loads, stored transposed
     for (int e4 = threadIdx.x; e4 < kGjBlock * kGjBlock / 4; e4 += blockDim.x) {
         const int r = e4 >> 4, c4 = 4 * (e4 & 15);
-        const float4 v = __ldcg(reinterpret_cast<const float4 *>(dv + r * kGjBlock + c4));
+        const float4 v = *reinterpret_cast<const float4 *>(dv + r * kGjBlock + c4);
         DvT[c4][r] = v.x;
         DvT[c4 + 1][r] = v.y;
         DvT[c4 + 2][r] = v.z;
@@ -368,14 +359,14 @@ __device__ void gj_prep_tile(const PatchDev &P, int K, int p, int jt, float *sm)
         for (int e4 = threadIdx.x; e4 < kGjBlock * kGjTile / 4; e4 += blockDim.x) {
             const int s_ = e4 >> 4, c4 = 4 * (e4 & 15);
             float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (s_ < b && j0 + c4 < static_cast<int>(ld)) v = __ldcg(reinterpret_cast<const float4 *>(A + (k0 + s_) * ld + j0 + c4));
+            if (s_ < b && j0 + c4 < static_cast<int>(ld)) v = *reinterpret_cast<const float4 *>(A + (k0 + s_) * ld + j0 + c4);
             *reinterpret_cast<float4 *>(&Us[s_][c4]) = v;
         }
     } else {  // j0 + 64 <= k0: U[s][c] = A[j0 + c][k0 + s], rows of A read contiguously, stored transposed
         for (int e4 = threadIdx.x; e4 < kGjTile * kGjBlock / 4; e4 += blockDim.x) {
             const int c = e4 >> 4, s4 = 4 * (e4 & 15);
             float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (k0 + s4 < static_cast<int>(ld)) v = __ldcg(reinterpret_cast<const float4 *>(A + (j0 + c) * ld + k0 + s4));
+            if (k0 + s4 < static_cast<int>(ld)) v = *reinterpret_cast<const float4 *>(A + (j0 + c) * ld + k0 + s4);
             Us[s4][c] = v.x;
             Us[s4 + 1][c] = v.y;
             Us[s4 + 2][c] = v.z;
@@ -467,7 +458,7 @@ __device__ __forceinline__ GjTile gj_tile(const PatchDev &P, int K, int T, int i
     return t;
 }
 
-// Stage of a tile update: the tile's split operands as the prep left them
+// Stage of the update: the tile's split operands as the prep pass left them
 // (A = the pivot-row copies of its row tile, B = the scaled pivot rows of its
 // column tile, each a TF32 high part and an FP32 remainder in the canonical
 // layout, 4 x 16 KB).  The old values are read from global memory by the
@@ -476,103 +467,50 @@ __device__ __forceinline__ GjTile gj_tile(const PatchDev &P, int K, int T, int i
 constexpr int kUpStage = 4 * tc::kOperandFloats;
 constexpr size_t kUpdateSmem = kUpStage * sizeof(float);
 
-// Issues the 16-byte copies of a round-K tile's operands into `stage` (contiguous blocks: 8 + 8 chunks per
-// thread; the pivot rows need B only).  cp.async.cg reads through L2, past the L1 cache.
-__device__ __forceinline__ void gj_issue_tile(const PatchDev &P, int K, const GjTile &t, float *stage) {
+// Issues the 16-byte copies of a tile's operands into `stage` (contiguous blocks: 8 + 8 chunks per thread;
+// the pivot rows need B only).
+__device__ __forceinline__ void gj_issue_tile(const PatchDev &P, const GjTile &t, float *stage) {
     float *Ab = stage, *Bb = stage + 2 * tc::kOperandFloats;
-    const float *csrc = P.csplit + gj_split_off(P, K, t.p, t.row0 / kGjTile);
-    const float *rsrc = P.rsplit + gj_split_off(P, K, t.p, t.col0 / kGjTile);
+    const float *csrc = P.csplit + (static_cast<size_t>(t.p) * P.T + t.row0 / kGjTile) * 2 * tc::kOperandFloats;
+    const float *rsrc = P.rsplit + (static_cast<size_t>(t.p) * P.T + t.col0 / kGjTile) * 2 * tc::kOperandFloats;
     for (int c = threadIdx.x; c < 2 * tc::kOperandFloats / 4; c += blockDim.x) {
         cp_async16(Bb + 4 * c, rsrc + 4 * c, true);
         if (!t.prow) cp_async16(Ab + 4 * c, csrc + 4 * c, true);
     }
 }
 
-// Dependency flags of the refresh (P.flow, zeroed before each refresh; int each):
-//   [0] the next work item, [1] dead: a wait gave up (later waits give up at once),
-//   tile_round[p][i][j]  rounds of updates finished on tile (i, j), i <= j,
-//   prep_done[p][j][K&1] 1 + the last round K of that parity whose prep of column tile j has finished,
-//   inv_done[p]          1 + the last pivot block inverted (block 0 is inverted before the launch).
-__device__ __forceinline__ int *flow_dead(const PatchDev &P) { return P.flow + 1; }
-__device__ __forceinline__ int *flow_tile(const PatchDev &P, int p, int i, int j) {
-    return P.flow + 2 + (static_cast<size_t>(p) * P.T + i) * P.T + j;
-}
-__device__ __forceinline__ int *flow_prep(const PatchDev &P, int p, int j, int K) {
-    return P.flow + 2 + static_cast<size_t>(P.np) * P.T * P.T + (static_cast<size_t>(p) * P.T + j) * 2 + (K & 1);
-}
-__device__ __forceinline__ int *flow_inv(const PatchDev &P, int p) {
-    return P.flow + 2 + static_cast<size_t>(P.np) * P.T * (P.T + 2) + p;
-}
-__host__ __device__ __forceinline__ size_t flow_ints(int np, int T) {
-    return 2 + static_cast<size_t>(np) * T * (T + 2) + np;
-}
-
-__device__ __forceinline__ int ld_acquire(const int *p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Polls *flag until it reaches `target` (thread-level); false when it gave up: after kFlowWaitLimit polls
-// (an L2 round trip and a 128 ns sleep each: about a second), or soon after another wait has given up.
-constexpr uint32_t kFlowWaitLimit = 1u << 20;
-__device__ bool flow_poll(const PatchDev &P, const int *flag, int target) {
-    for (uint32_t it = 0; it < kFlowWaitLimit; ++it) {
-        if (ld_acquire(flag) >= target) return true;
-        if ((it & 63) == 63 && ld_acquire(flow_dead(P))) return false;
-        __nanosleep(128);
-    }
-    atomicExch(flow_dead(P), 1);
-    return false;
-}
-
-// Publishes an item: the block's writes (ordered before thread 0's release by the barrier), then the flag,
-// raised to `value` (flags only grow).  All threads.
-__device__ __forceinline__ void flow_release(int *flag, int value) {
-    __syncthreads();
-    if (threadIdx.x == 0) asm volatile("red.release.gpu.global.max.s32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
-}
-
-// The Gauss-Jordan rounds of every patch in one launch, as a dataflow over work items.  Items are handed out
-// in a fixed order by one counter: round by round, in each round first the prep of every column tile
-// (gj_prep_tile, part (b)), then the update of every tile of the upper block triangle (part (c)):
+// Round K, part (c), the 64x64 tiles of the upper block triangle:
 //   pivot rows       A[i, j] = rbuf[i - k0][j]      (-D^-1 in the pivot block)
 //   other rows       A[i, j] -= C_i . rbuf[:, j]   (j outside the pivot columns)
 //                    A[i, j]  = -C_i . rbuf[:, j]  (pivot columns: C_i D^-1)
-// with C_i = cbuf[:][i] (the pivot-row copies) and rbuf the scaled pivot rows -- the symmetric sweep, which
-// leaves -A^-1 after the last round.  Tiles and pivot blocks are both 64 wide, so a tile lies in the pivot
-// rows (ti == K, a copy), in the pivot columns (tj == K) or in neither.  The block that updates a patch's
-// diagonal tile (K + 1, K + 1) inverts it for the next round (part (a)).  Instead of a launch per round,
-// each item waits for the items it reads from:
-//   prep (K, j):      the inverse of pivot block K; tile (K, j) after round K - 1; and, before it overwrites
-//                     its round-parity buffers, every tile of row and column j after round K - 2;
-//   update (K, i, j): tile (i, j) after round K - 1; the preps (K, i) and (K, j);
-//   inverse K + 1:    before it overwrites its parity's inverse, the preps of round K - 1.
-// Every wait is for items handed out earlier, so the block holding the oldest unfinished item never waits
-// and the launch always drains; the waits are bounded (flow_poll).  An item whose wait gave up is released
-// without its work and its patch falls back to the block-diagonal preconditioner; the wait marks the launch
-// dead, so that every later wait that is not already satisfied gives up at once and the launch ends soon.  Round operands (csplit, rsplit) and inverses are double-buffered by round
-// parity (gj_split_off, gj_dinv); data written by other blocks is read past the L1 cache.  The tile product
-// C^T rbuf runs on the tensor cores (tc_tf32.cuh: the operands as the prep split them, three TF32 products
-// accumulated in FP32 in tensor memory, issued by one thread and committed to an mbarrier).  Read-back: warp
-// w holds tile rows 16 (w % 4) .. + 15 in lanes 0-15 and columns 32 (w / 4) .. + 31; each lane pair
-// (l, l + 16) then splits the 32 columns, so every thread writes 16 columns of one row.  A wait for the
-// products that gives up (bounded) marks the tile's patch unusable and the block computes no further
-// products.  Persistent blocks (two per SM); dynamic shared memory: kUpdateSmem.
-__global__ void __launch_bounds__(256, 2) gj_flow_kernel(PatchDev P) {
+// with C_i = cbuf[:][i] (the pivot-row copies) and rbuf the scaled pivot rows
+// -- the symmetric sweep, which leaves -A^-1 after the last round.  Tiles and
+// pivot blocks are both 64 wide, so a tile lies in the pivot rows (ti == K, a
+// copy), in the pivot columns (tj == K) or in neither.  Persistent blocks (two
+// per SM) take tiles from a per-round counter.  The tile product C^T rbuf runs
+// on the tensor cores (tc_tf32.cuh: the operands as the prep pass split them,
+// three TF32 products accumulated in FP32 in tensor memory, issued by one
+// thread and committed to an mbarrier).  Read-back: warp w holds tile rows
+// 16 (w % 4) .. + 15 in lanes 0-15 and columns 32 (w / 4) .. + 31; each lane
+// pair (l, l + 16) then splits the 32 columns, so every thread writes 16
+// columns of one row.  The block that takes a patch's diagonal tile
+// (K + 1, K + 1) inverts it for the next round right after its update, while
+// the other blocks go on with the rest.  A wait for the products that gives up
+// (bounded) marks the tile's patch unusable -- it falls back to the
+// block-diagonal preconditioner -- and the block computes no further products.
+// Dynamic shared memory: kUpdateSmem.
+__global__ void __launch_bounds__(256, 2) gj_update_kernel(PatchDev P, int K, int T, int *counter) {
     static_assert(kGjTile == 64 && kGjBlock == 64 && tc::kTileMN == 64 && tc::kTileK == 64, "64-wide tiles");
-    static_assert(kUpStage >= kInvWs && kUpStage >= kPrepSmem, "the inversion and the prep reuse the stage");
+    static_assert(kUpStage >= kInvWs, "the inversion reuses the stage");
     extern __shared__ __align__(128) float usm[];
     __shared__ int next_item;
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tbase;
-    __shared__ int tc_ok, tc_dead;
+    __shared__ int tc_ok, dead;
     chain_wait();
-    const int T = P.T;
-    const int prep_items = P.np * T, per_round = P.np * (T + T * (T + 1) / 2);
-    const int total = per_round * T;
+    const int total = P.np * (T * (T + 1) / 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) next_item = atomicAdd(P.flow, 1);
+    if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
     __syncthreads();
     int item = next_item;
     if (item >= total) return;
@@ -580,7 +518,7 @@ __global__ void __launch_bounds__(256, 2) gj_flow_kernel(PatchDev P) {
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
         fence_barrier_init();
-        tc_dead = 0;
+        dead = 0;
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -590,144 +528,109 @@ __global__ void __launch_bounds__(256, 2) gj_flow_kernel(PatchDev P) {
     const float *Ab = usm, *Bb = usm + 2 * tc::kOperandFloats;
     // this thread's output: tile row tr, columns tc0 .. tc0 + 15
     const int tr = 16 * (warp & 3) + (lane & 15), tc0 = 32 * (warp >> 2) + 16 * (lane >> 4);
-    int ahead = 0;  // thread 0: the item after this one, taken while this one runs
     while (item < total) {
-        if (threadIdx.x == 0) ahead = atomicAdd(P.flow, 1);
-        const int K = item / per_round, rem = item - K * per_round;
-        if (rem < prep_items) {  // prep of column tile j, the round's next pivot column first
-            const int p = rem % P.np, j = (K + 1 + rem / P.np) % T;
-            const int n = P.nf[p] * P.nbf, Tp = (n + kGjTile - 1) / kGjTile;
-            if (K < Tp && j < Tp) {
-                // the waits run in parallel, one flag per polling thread
-                bool ok = true;
-                const int t = static_cast<int>(threadIdx.x) - 64;
-                if (K > 0 && threadIdx.x == 0) ok = flow_poll(P, flow_inv(P, p), K + 1);
-                if (K > 0 && threadIdx.x == 32) ok = flow_poll(P, flow_tile(P, p, min(K, j), max(K, j)), K);
-                if (K >= 2 && t >= 0 && t < Tp) ok = flow_poll(P, flow_tile(P, p, min(t, j), max(t, j)), K - 1);
-                if (__syncthreads_and(ok)) gj_prep_tile(P, K, p, j, usm);
-                else if (threadIdx.x == 0) P.ok[p] = 0;
-                flow_release(flow_prep(P, p, j, K), K + 1);
+        const GjTile cur = gj_tile(P, K, T, item);
+        if (cur.valid) {
+            gj_issue_tile(P, cur, usm);
+            cp_async_commit();
+            const int n = cur.n, ld = patch_ld(n);
+            const int i = cur.row0 + tr, j = cur.col0 + tc0;
+            float *Arow = P.A + P.moff[cur.p] + static_cast<size_t>(i) * ld + j;
+            // the old values, while the operands land (the pivot columns and rows are overwritten)
+            float res[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) res[q] = 0.0f;
+            if (!cur.prow && !cur.pcol && i < n) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4) {
+                    if (j + q < ld) {
+                        const float4 o4 = *reinterpret_cast<const float4 *>(Arow + q);
+                        res[q] = o4.x;
+                        res[q + 1] = o4.y;
+                        res[q + 2] = o4.z;
+                        res[q + 3] = o4.w;
+                    }
+                }
             }
-        } else {
-            const GjTile cur = gj_tile(P, K, T, rem - prep_items);
-            if (cur.valid) {
-                const int ti = cur.row0 / kGjTile, tj = cur.col0 / kGjTile;
-                bool ok = true;  // the waits run in parallel, one flag per polling thread
-                if (K > 0 && threadIdx.x == 0) ok = flow_poll(P, flow_tile(P, cur.p, ti, tj), K);
-                if (threadIdx.x == 32) ok = flow_poll(P, flow_prep(P, cur.p, tj, K), K + 1);
-                if (!cur.prow && threadIdx.x == 64) ok = flow_poll(P, flow_prep(P, cur.p, ti, K), K + 1);
-                const bool go = __syncthreads_and(ok);
-                if (go) {
-                    gj_issue_tile(P, K, cur, usm);
-                    cp_async_commit();
-                    const int n = cur.n, ld = patch_ld(n);
-                    const int i = cur.row0 + tr, j = cur.col0 + tc0;
-                    float *Arow = P.A + P.moff[cur.p] + static_cast<size_t>(i) * ld + j;
-                    // the old values, while the operands land (the pivot columns and rows are overwritten)
-                    float res[16];
+            cp_async_wait<0>();
+            tc::fence_proxy_async();  // the operands are visible to the tensor cores
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            bool have = true;
+            if (cur.prow) {  // the pivot rows: the scaled pivot rows themselves (row0 == k0), high + low parts
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) res[q] = 0.0f;
-                    if (!cur.prow && !cur.pcol && i < n) {
-#pragma unroll
-                        for (int q = 0; q < 16; q += 4) {
-                            if (j + q < ld) {
-                                const float4 o4 = __ldcg(reinterpret_cast<const float4 *>(Arow + q));
-                                res[q] = o4.x;
-                                res[q + 1] = o4.y;
-                                res[q + 2] = o4.z;
-                                res[q + 3] = o4.w;
-                            }
-                        }
-                    }
-                    cp_async_wait<0>();
-                    tc::fence_proxy_async();  // the operands are visible to the tensor cores
-                    tc::fence_before_sync();
-                    __syncthreads();
-                    tc::fence_after_sync();
-                    bool have = true;
-                    if (cur.prow) {  // the pivot rows: the scaled pivot rows themselves (row0 == k0), high + low parts
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            const int e = tc::canon(tc0 + q, tr);
-                            res[q] = Bb[e] + Bb[tc::kOperandFloats + e];
-                        }
-                    } else if (tc_dead) {
-                        have = false;
-                    } else {
-                        if (threadIdx.x == 0) {
-                            tc::issue_tile_products(tmem, Ab, Ab + tc::kOperandFloats, Bb, Bb + tc::kOperandFloats);
-                            tc::commit(&bar);
-                            bool done = mbar_wait_bounded(&bar, products & 1u);
-                            if (!done) done = mbar_wait_bounded(&bar, products & 1u);  // drain before going on
-                            tc_ok = done ? 1 : 0;
-                            if (!done) {
-                                tc_dead = 1;
-                                P.ok[cur.p] = 0;
-                            }
-                        }
-                        ++products;
-                        __syncthreads();
-                        tc::fence_after_sync();
-                        have = tc_ok != 0;
-                        if (have) {
-                            float v[32];
-                            tc::tmem_ld32(tc::tmem_addr(tmem, warp, 32 * (warp >> 2)), v);
-                            // lanes l and l + 16 share row l's 32 columns: l keeps 0..15, l + 16 takes 16..31
-#pragma unroll
-                            for (int q = 0; q < 16; ++q) {
-                                const float hi16 = __shfl_sync(0xffffffffu, v[16 + q], lane & 15);
-                                res[q] -= (lane < 16) ? v[q] : hi16;
-                            }
-                            tc::fence_before_sync();
-                        }
-                    }
-                    if (have) {
-                        // the patch's last round writes its final values: a non-finite one marks the inverse unusable
-                        const bool last = (K + 1) * kGjBlock >= n;
-                        bool bad = false;
-                        if (i < n) {
-#pragma unroll
-                            for (int q = 0; q < 16; q += 4) {
-                                if (j + q + 3 < n) {
-                                    *reinterpret_cast<float4 *>(Arow + q) = make_float4(res[q], res[q + 1], res[q + 2], res[q + 3]);
-                                } else {  // the row's last, partial chunk: nothing beyond column n - 1
-#pragma unroll
-                                    for (int u = 0; u < 4; ++u)
-                                        if (j + q + u < n) Arow[q + u] = res[q + u];
-                                }
-                            }
-                            if (last)
-#pragma unroll
-                                for (int q = 0; q < 16; ++q) bad |= (j + q < n) && !isfinite(res[q]);
-                        }
-                        if (bad) P.ok[cur.p] = 0;
-                        if (last && cur.row0 < cur.col0 && i < n) {
-                            // final values: also the transposed tile of the lower block triangle (A^-1 is symmetric)
-                            float *At = P.A + P.moff[cur.p] + i;
-#pragma unroll
-                            for (int q = 0; q < 16; ++q)
-                                if (j + q < n) At[static_cast<size_t>(j + q) * ld] = res[q];
-                        }
-                    } else if (threadIdx.x == 0) {
+                for (int q = 0; q < 16; ++q) {
+                    const int e = tc::canon(tc0 + q, tr);
+                    res[q] = Bb[e] + Bb[tc::kOperandFloats + e];
+                }
+            } else if (dead) {
+                have = false;
+            } else {
+                if (threadIdx.x == 0) {
+                    tc::issue_tile_products(tmem, Ab, Ab + tc::kOperandFloats, Bb, Bb + tc::kOperandFloats);
+                    tc::commit(&bar);
+                    bool ok = mbar_wait_bounded(&bar, products & 1u);
+                    if (!ok) ok = mbar_wait_bounded(&bar, products & 1u);  // drain before going on
+                    tc_ok = ok ? 1 : 0;
+                    if (!ok) {
+                        dead = 1;
                         P.ok[cur.p] = 0;
                     }
-                } else if (threadIdx.x == 0) {
-                    P.ok[cur.p] = 0;
                 }
-                flow_release(flow_tile(P, cur.p, ti, tj), K + 1);
-                if (cur.diag) {  // the tile is final for round K + 1: invert it now
-                    const int Tp = (cur.n + kGjTile - 1) / kGjTile;
-                    bool ok2 = go;
-                    if (K >= 1 && static_cast<int>(threadIdx.x) < Tp)
-                        ok2 = flow_poll(P, flow_prep(P, cur.p, threadIdx.x, K - 1), K) && ok2;
-                    if (__syncthreads_and(ok2)) pivot_invert_patch(P, cur.p, K + 1, usm);
-                    else if (threadIdx.x == 0) P.ok[cur.p] = 0;
-                    flow_release(flow_inv(P, cur.p), K + 2);
+                ++products;
+                __syncthreads();
+                tc::fence_after_sync();
+                have = tc_ok != 0;
+                if (have) {
+                    float v[32];
+                    tc::tmem_ld32(tc::tmem_addr(tmem, warp, 32 * (warp >> 2)), v);
+                    // lanes l and l + 16 share row l's 32 columns: l keeps 0..15, l + 16 takes 16..31
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const float hi16 = __shfl_sync(0xffffffffu, v[16 + q], lane & 15);
+                        res[q] -= (lane < 16) ? v[q] : hi16;
+                    }
+                    tc::fence_before_sync();
                 }
+            }
+            if (have) {
+                // the patch's last round writes its final values: a non-finite one marks the inverse unusable
+                const bool last = (K + 1) * kGjBlock >= n;
+                bool bad = false;
+                if (i < n) {
+#pragma unroll
+                    for (int q = 0; q < 16; q += 4) {
+                        if (j + q + 3 < n) {
+                            *reinterpret_cast<float4 *>(Arow + q) = make_float4(res[q], res[q + 1], res[q + 2], res[q + 3]);
+                        } else {  // the row's last, partial chunk: nothing beyond column n - 1
+#pragma unroll
+                            for (int u = 0; u < 4; ++u)
+                                if (j + q + u < n) Arow[q + u] = res[q + u];
+                        }
+                    }
+                    if (last)
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) bad |= (j + q < n) && !isfinite(res[q]);
+                }
+                if (bad) P.ok[cur.p] = 0;
+                if (last && cur.row0 < cur.col0 && i < n) {
+                    // final values: also the transposed tile of the lower block triangle (A^-1 is symmetric)
+                    float *At = P.A + P.moff[cur.p] + i;
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        if (j + q < n) At[static_cast<size_t>(j + q) * ld] = res[q];
+                }
+            } else if (threadIdx.x == 0) {
+                P.ok[cur.p] = 0;
+            }
+            if (cur.diag) {  // the tile is final for round K + 1: invert it now (its writes are the block's own)
+                __syncthreads();
+                pivot_invert_patch(P, cur.p, K + 1, usm);
             }
         }
         __syncthreads();  // every thread is done with the stage and with next_item
-        if (threadIdx.x == 0) next_item = ahead;
+        if (threadIdx.x == 0) next_item = atomicAdd(counter, 1);
         __syncthreads();
         item = next_item;
     }

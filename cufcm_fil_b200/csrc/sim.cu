@@ -211,24 +211,21 @@ int launch_matvec_tail(Engine *e, const double *v, double *out, cudaStream_t st)
     return CF_OK;
 }
 
-// The first CGS2 pass (w -= Q h1) also forms the second pass's coefficients h2 = Q^T w (hnext); the final
-// pass (w -= Q h2) also the norm and the Givens step.
 template <int ROWS>
 int launch_update_t(Engine *e, const double *h, int final_pass, cudaGraphConditionalHandle hc, int grid,
-                    cudaStream_t st, double *hnext) {
-    const size_t smem = final_pass ? e->givens_smem : sizeof(double) * (e->d.mi_max + 1 + ROWS);
-    CF_CUDA(launch_chained(update_kernel<ROWS>, dim3(grid), dim3(256), smem, st, e->d, h, final_pass, hc,
-                           final_pass ? nullptr : hnext));
+                    cudaStream_t st) {
+    CF_CUDA(launch_chained(update_kernel<ROWS>, dim3(grid), dim3(256), final_pass ? e->givens_smem : 0, st, e->d, h,
+                           final_pass, hc));
     return CF_OK;
 }
 
 int launch_update(Engine *e, const double *h, int final_pass, cudaGraphConditionalHandle hc, cudaStream_t st,
-                  int rows, int grid, double *hnext = nullptr) {
+                  int rows, int grid) {
     switch (rows) {
-        case 32: return launch_update_t<32>(e, h, final_pass, hc, grid, st, hnext);
-        case 64: return launch_update_t<64>(e, h, final_pass, hc, grid, st, hnext);
-        case 128: return launch_update_t<128>(e, h, final_pass, hc, grid, st, hnext);
-        case 256: return launch_update_t<256>(e, h, final_pass, hc, grid, st, hnext);
+        case 32: return launch_update_t<32>(e, h, final_pass, hc, grid, st);
+        case 64: return launch_update_t<64>(e, h, final_pass, hc, grid, st);
+        case 128: return launch_update_t<128>(e, h, final_pass, hc, grid, st);
+        case 256: return launch_update_t<256>(e, h, final_pass, hc, grid, st);
         default: return set_error(CF_EINVAL, "update tile of %d rows not built", rows);
     }
 }
@@ -250,19 +247,22 @@ int launch_combine(Engine *e, cudaStream_t st) {
 int launch_refresh(Engine *e, cudaStream_t st) {
     const PatchDev &P = e->P;
     e->refresh_geometry = e->geometry;
-    CF_CUDA(cudaMemsetAsync(P.flow, 0, sizeof(int) * flow_ints(P.np, P.T), st));
+    CF_CUDA(cudaMemsetAsync(P.counter, 0, sizeof(int) * e->gj_rounds, st));
     patch_mobility_kernel<<<dim3(e->mob_grid, P.np), 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_mobility_kernel");
     patch_rates_kernel<<<dim3(e->rates_grid, P.np), 256, 0, st>>>(e->d, P);
     CF_CHECK_LAUNCH("patch_rates_kernel");
-    gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, 0);  // later pivot blocks: inverted inside the rounds
+    gj_pivot_kernel<<<P.np, 256, 0, st>>>(P, 0);  // later pivot blocks: inverted inside the previous update
     CF_CHECK_LAUNCH("gj_pivot_kernel");
-    gj_flow_kernel<<<e->gj_update_grid, 256, kUpdateSmem, st>>>(P);  // every Gauss-Jordan round
-    CF_CHECK_LAUNCH("gj_flow_kernel");
+    for (int K = 0; K < e->gj_rounds; ++K) {
+        CF_CUDA(launch_chained(gj_prep_kernel, dim3(e->gj_cols, P.np), dim3(256), 0, st, P, K));
+        CF_CUDA(launch_chained(gj_update_kernel, dim3(e->gj_update_grid), dim3(256), kUpdateSmem, st, P, K, e->gj_cols,
+                               P.counter + K));
+    }
     return CF_OK;
 }
 
-int refresh_launches(const Engine *e) { return e->line ? 4 : 0; }
+int refresh_launches(const Engine *e) { return e->line ? 3 + 2 * e->gj_rounds : 0; }
 
 int launch_patch_apply(Engine *e, const double *in, double *out, int masked, cudaStream_t st) {
     patch_apply_kernel<<<dim3(e->apply_chunks, e->P.np), kApplyThreads, e->apply_smem, st>>>(e->d, e->P, in, out,
@@ -343,7 +343,8 @@ int launch_body(Engine *e, cudaGraphConditionalHandle h, cudaStream_t st) {
         e->c_pairs += 1;
     }
     CF_CUDA(launch_chained(dots_kernel, dim3(e->dots_grid), dim3(256), 0, st, e->d, e->d.h1));
-    CF_TRY(launch_update(e, e->d.h1, 0, h, st, e->tune.update_rows, e->update_grid, e->d.h2));
+    CF_TRY(launch_update(e, e->d.h1, 0, h, st, e->tune.update_rows, e->update_grid));
+    CF_CUDA(launch_chained(dots_kernel, dim3(e->dots_grid), dim3(256), 0, st, e->d, e->d.h2));
     return launch_update(e, e->d.h2, 1, h, st, e->tune.update_rows, e->update_grid);
 }
 
@@ -616,14 +617,14 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     CF_TRY(eng_alloc(e, &P.A, static_cast<size_t>(mo)));
     CF_CUDA(cudaMemset(P.A, 0, sizeof(float) * static_cast<size_t>(mo)));  // the padding columns stay zero
     P.T = (max_n + kGjTile - 1) / kGjTile;
-    const size_t split_floats = 2 * static_cast<size_t>(P.np) * P.T * 2 * tc::kOperandFloats;  // two round parities
+    const size_t split_floats = static_cast<size_t>(P.np) * P.T * 2 * tc::kOperandFloats;
     CF_TRY(eng_alloc(e, &P.csplit, split_floats));
     CF_TRY(eng_alloc(e, &P.rsplit, split_floats));
     CF_CUDA(cudaMemset(P.csplit, 0, sizeof(float) * split_floats));
     CF_CUDA(cudaMemset(P.rsplit, 0, sizeof(float) * split_floats));
-    CF_TRY(eng_alloc(e, &P.dinv, 2 * static_cast<size_t>(P.np) * kGjBlock * kGjBlock));
+    CF_TRY(eng_alloc(e, &P.dinv, static_cast<size_t>(P.np) * kGjBlock * kGjBlock));
     CF_TRY(eng_alloc(e, &P.ok, P.np));
-    CF_TRY(eng_alloc(e, &P.flow, flow_ints(P.np, P.T)));
+    CF_TRY(eng_alloc(e, &P.counter, std::max(1, (max_n + kGjBlock - 1) / kGjBlock)));
     e->patch_floats = mo;
     const long long ns = static_cast<long long>(max_nf) * d.nseg;
     e->mob_grid = static_cast<int>((ns * ns + 255) / 256);
@@ -632,7 +633,7 @@ int build_patches(Engine *e, const cf_sim_config *cfgs) {
     e->rates_grid = std::max(1, (max_n * max_nf * (nbf - nl) + 255) / 256);
     e->gj_cols = T;
     e->gj_update_grid = static_cast<int>(std::min<long long>(1LL * P.np * (T * (T + 1) / 2), 2LL * e->num_sms));
-    CF_CUDA(cudaFuncSetAttribute(gj_flow_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CF_CUDA(cudaFuncSetAttribute(gj_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kUpdateSmem)));
     e->apply_chunks = (max_n + kApplyRows - 1) / kApplyRows;
     e->apply_smem = sizeof(double) * std::max(patch_ld(max_n), 3 * d.nseg);
@@ -829,7 +830,6 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     d.chunk_arr = e->d_chunk_arr;
     CF_TRY(eng_alloc(e, &d.dots_partial, (mi + 1) * max_chunks));
     CF_TRY(eng_alloc(e, &d.norm_partial, std::max<size_t>(F, nr / kRowUnit)));
-    CF_TRY(eng_alloc(e, &d.dots_partial2, (mi + 1) * (nr / kRowUnit)));
     // pair kernel work list
     int *p_seg0, *p_n, *p_nb;
     long long *p_poff, *p_item0;
@@ -874,9 +874,8 @@ int engine_init(Engine *e, const cf_sim_config *cfgs, int B) {
     e->pre_smem = sizeof(double) * 3 * ns;
     e->givens_smem = sizeof(double) * 3 * (d.mi_max + 2);
     e->epi_grid = (seg + 31) / 32;
-    const size_t update_smem = std::max(e->givens_smem, sizeof(double) * (d.mi_max + 1 + 256));
-    if (update_smem > 48 * 1024) {
-        const int gs = static_cast<int>(update_smem);
+    if (e->givens_smem > 48 * 1024) {
+        const int gs = static_cast<int>(e->givens_smem);
         CF_CUDA(cudaFuncSetAttribute(update_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
         CF_CUDA(cudaFuncSetAttribute(update_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
         CF_CUDA(cudaFuncSetAttribute(update_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
@@ -1038,7 +1037,7 @@ int engine_autotune(Engine *e, int k_hint, int *choice) {
                 const long long ntiles = d.nrows / rows;
                 const int grid = static_cast<int>(std::max(1LL, std::min(ntiles, 1LL * e->num_sms * bps)));
                 CF_TRY(time_launches(
-                    e, [&] { return launch_update(e, e->d.h1, 0, 0, e->stream, rows, grid, e->d.h2); }, reps, &t));
+                    e, [&] { return launch_update(e, e->d.h1, 0, 0, e->stream, rows, grid); }, reps, &t));
                 if (t < bt * 0.98f) {
                     bt = t;
                     best.update_rows = rows;

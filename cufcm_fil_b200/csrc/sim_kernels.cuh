@@ -133,7 +133,6 @@ struct SimDev {
     double *Q, *Z;            // bases [(mi_max + 1) * ldq]
     double *H, *cs, *sn, *beta, *h1, *h2, *y;   // per array, strides hstride / sstride
     double *dots_partial, *norm_partial;
-    double *dots_partial2;    // per-block sums of the fused second-pass dot products [(mi_max + 1) * nrows / 32]
     float4 *f4;               // forces for the pair kernel
     const float4 *partial;    // mobility partials, per array [N][nb]
     GmresCtl *ctl;            // [B]
@@ -940,22 +939,16 @@ __device__ void givens_step(const SimDev &d, int b, int k, double qn, double *gs
 
 // w -= sum_j h_j Q_j over the rows of the running arrays; in the final pass
 // also ||w|| and, by the block arriving last for an array, that array's
-// Givens step; the last array to finish closes the iteration.  In the first
-// pass with `hnext`, also the dot products <Q_j, w> of the updated w, j <= k
-// (the second pass's coefficients), into hnext: per block and array in shared
-// memory (warp j % 8 adds basis vector j's sum over each tile, in tile order),
-// then summed over the blocks in a fixed order by the block arriving last.
+// Givens step; the last array to finish closes the iteration.
 // Tile = ROWS rows x (256/ROWS) basis-vector groups: each thread sums every
 // G-th basis vector for one row with loads unrolled 4 deep, and the groups are
 // combined in shared memory in a fixed order.  Each block takes a contiguous
 // range of tiles (tiles never straddle arrays: arrays start on kRowPad rows).
-// Dynamic shared memory: 3*(mi_max+2) doubles (final pass), mi_max+1+ROWS
-// doubles (first pass with hnext).
 template <int ROWS>
 __global__ void __launch_bounds__(256) update_kernel(SimDev d, const double *h, int final_pass,
-                                                     cudaGraphConditionalHandle hcond, double *hnext) {
+                                                     cudaGraphConditionalHandle hcond) {
     constexpr int G = 256 / ROWS;
-    extern __shared__ double gsm[];  // Givens staging (final pass); dot-product sums and the tile's w (hnext)
+    extern __shared__ double gsm[];  // Givens staging, 3*(mi_max+2) doubles (final pass)
     __shared__ double sm32[32];
     __shared__ double part[G][ROWS];
     __shared__ int last, last_all;
@@ -964,14 +957,9 @@ __global__ void __launch_bounds__(256) update_kernel(SimDev d, const double *h, 
     const int k = d.lc->k;
     if (k >= d.mi_max) return;  // defensive, uniform over the grid
     const int r = threadIdx.x % ROWS, g = threadIdx.x / ROWS;
-    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
     const long long ntiles = d.nrows / ROWS;
     const long long per = (ntiles + gridDim.x - 1) / gridDim.x;
     const long long lo = static_cast<long long>(blockIdx.x) * per, hi = min(ntiles, lo + per);
-    const bool fused = !final_pass && hnext != nullptr;
-    double *dacc = gsm, *wsm = gsm + (d.mi_max + 1);
-    if (fused)
-        for (int j = threadIdx.x; j <= k; j += blockDim.x) dacc[j] = 0.0;
     int cur = -1;
     bool cur_active = false;
     double ss = 0.0;
@@ -979,28 +967,6 @@ __global__ void __launch_bounds__(256) update_kernel(SimDev d, const double *h, 
         const bool done = tile >= hi;
         const int b = done ? -1 : d.rb_arr[tile * (ROWS / kRowUnit)];
         if (done || b != cur) {
-            if (fused && cur >= 0 && cur_active) {  // this block's sums for array cur; the last block adds them up
-                const ArrayInfo &a = d.arr[cur];
-                const long long t0 = a.voff / ROWS, t1 = (a.voff + a.vlen) / ROWS;
-                const long long ntl = d.nrows / kRowUnit;  // slots per basis vector
-                __syncthreads();
-                for (int j = threadIdx.x; j <= k; j += blockDim.x) {
-                    d.dots_partial2[static_cast<size_t>(j) * ntl + max(lo, t0)] = dacc[j];
-                    dacc[j] = 0.0;
-                }
-                if (arrive_last(&d.ctl[cur].counter, ranges_meeting(t0, t1, per), &last)) {
-                    double *hb = hnext + static_cast<size_t>(cur) * d.sstride;
-                    for (int jj = wq; jj <= k; jj += blockDim.x >> 5) {
-                        double acc = 0.0;
-                        for (long long c = t0 / per + lane; c <= (t1 - 1) / per; c += 32)
-                            acc += __ldcg(&d.dots_partial2[static_cast<size_t>(jj) * ntl + max(c * per, t0)]);
-                        acc = warp_sum(acc);
-                        if (lane == 0) hb[jj] = acc;
-                    }
-                    __syncthreads();
-                    if (threadIdx.x == 0) d.ctl[cur].counter = 0;
-                }
-            }
             if (final_pass && cur >= 0 && cur_active) {  // close this block's share of array cur
                 const ArrayInfo &a = d.arr[cur];
                 const long long t0 = a.voff / ROWS, t1 = (a.voff + a.vlen) / ROWS;
@@ -1057,20 +1023,6 @@ __global__ void __launch_bounds__(256) update_kernel(SimDev d, const double *h, 
             const double wn = wi - acc;
             d.w[i] = wn;
             ss += wn * wn;
-            if (fused) wsm[r] = wn;
-        }
-        if (fused) {  // <Q_j, w> over the tile's rows: warp wq takes j = wq, wq + 8, ...
-            __syncthreads();
-            const long long i0 = tile * ROWS;
-            for (int j = wq; j <= k; j += blockDim.x >> 5) {
-                const double *qj = d.Q + static_cast<size_t>(j) * d.ldq + i0;
-                double x = 0.0;
-                for (int rr = lane; rr < ROWS; rr += 32)
-                    if (i0 + rr - a.voff < a.n) x += qj[rr] * wsm[rr];
-                x = warp_sum(x);
-                if (lane == 0) dacc[j] += x;
-            }
-            __syncthreads();
         }
     }
 }

@@ -1,6 +1,6 @@
 """Measurement entry points (the command lines of the committed profiles).
 
-  python -m cufcm_fil_b200.perf step --nx 16 --precond line --steps 2 [--warm W]
+  python -m cufcm_fil_b200.perf step --nx 16 --precond line --steps 2 [--warm W] [--block B]
       implicit steps of the benchmark lattice (lattice_simulation), each timed
       with CUDA events, and a fit of step time against GMRES iterations; with
       CUFIL_NO_GRAPH=1 every kernel is an ordinary launch, which is what a
@@ -31,28 +31,40 @@ import numpy as np
 from . import _lib
 
 
-def run_steps(nx: int, precond: str, steps: int, line_patch: int = 0, warm: int = 0):
+def run_steps(nx: int, precond: str, steps: int, line_patch: int = 0, warm: int = 0, block: int = 0):
     """`warm` untimed steps, then `steps` implicit steps, each timed with CUDA events on the engine's stream
-    (without warm-up steps the first includes the graph capture).  With three or more timed steps, a
-    least-squares fit step_ms = fixed_ms + ms_per_iteration * iterations splits the step time into the
-    per-step part (kinematics, right-hand side, refresh, finish) and the cost of one GMRES iteration."""
+    (without warm-up steps the first includes the graph capture).  With `block`, steps 0 .. block - 1 run
+    again and again, each block restored from the seeded initial state (outside the events; the 20a lattice
+    cannot run long stretches, its colliding cilia reach non-finite states).  With three or more timed
+    steps, a least-squares fit step_ms = fixed_ms + ms_per_iteration * iterations splits the step time into
+    the per-step part (kinematics, right-hand side, refresh, finish) and the cost of one GMRES iteration."""
     import torch
     from .sim import lattice_simulation
     code = {"line": _lib.CF_PRECOND_LINE, "block": _lib.CF_PRECOND_BLOCK_DIAG, "none": _lib.CF_PRECOND_NONE}[precond]
     its, ms = [], []
     with lattice_simulation(nx, precond=code, line_patch=line_patch) as sim:
         stream = torch.cuda.ExternalStream(sim.stream_handle())
-        for nt in range(warm):
-            sim.step(nt)
+        initial = sim.checkpoint() if block else None
+
+        def nt_of(k):
+            if not block:
+                return k
+            if k > 0 and k % block == 0:
+                sim.restore(initial)
+            return k % block
+        for k in range(warm):
+            sim.step(nt_of(k))
         torch.cuda.synchronize()
-        for nt in range(warm, warm + steps):
+        for k in range(warm, warm + steps):
+            nt = nt_of(k)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             its.append(sim.step(nt).iterations)
             b.record(stream)
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
-    out = {"nx": nx, "precond": precond, "warm": warm, "steps": steps, "gmres_iterations": its, "step_ms": ms}
+    out = {"nx": nx, "precond": precond, "warm": warm, "block": block, "steps": steps, "gmres_iterations": its,
+           "step_ms": ms}
     if steps >= 3 and len(set(its)) > 1:
         slope, icpt = np.polyfit(np.asarray(its, float), np.asarray(ms, float), 1)
         out.update(fixed_ms=float(icpt), ms_per_iteration=float(slope), mean_step_ms=float(np.mean(ms)))
@@ -163,6 +175,7 @@ def main(argv=None):
     st.add_argument("--steps", type=int, default=2)
     st.add_argument("--line-patch", type=int, default=0)
     st.add_argument("--warm", type=int, default=0)
+    st.add_argument("--block", type=int, default=0)
     fc = sub.add_parser("fcm")
     fc.add_argument("--grid", type=int, default=512)
     fc.add_argument("--reps", type=int, default=5)
@@ -175,7 +188,7 @@ def main(argv=None):
     ml.add_argument("--reps", type=int, default=50)
     a = ap.parse_args(argv)
     if a.what == "step":
-        print(json.dumps(run_steps(a.nx, a.precond, a.steps, a.line_patch, a.warm)))
+        print(json.dumps(run_steps(a.nx, a.precond, a.steps, a.line_patch, a.warm, a.block)))
     elif a.what == "refresh":
         print(json.dumps(run_refresh(a.nx, a.reps)))
     elif a.what == "mlp":
