@@ -351,6 +351,16 @@ def run_batched_sharded(all_specs, shared, bins, costs, world, rank, W, K):
             "timing": "CUDA events on each rank's batch stream; the job's step time is the slowest rank's"}
 
 
+def _last_solve(sim):
+    """(converged, error text) of the last solve; a non-finite solve (the colliding cilia of the 20a lattices can
+    reach one) is reported, not raised, so that one leg does not end the benchmark."""
+    from cufcm_fil_b200 import _lib
+    try:
+        return bool(sim.last_solve().status == _lib.CF_OK), None
+    except _lib.CufilError as exc:
+        return False, str(exc)
+
+
 def run_large(local, inp, flush, steps=4):
     """1024 cilia (32 x 32 lattice, 20 480 segments): whole-line patches against the block-diagonal preconditioner."""
     import torch
@@ -363,10 +373,12 @@ def run_large(local, inp, flush, steps=4):
         stream = torch.cuda.ExternalStream(sim.stream_handle())
         sim.step(0)
         ms = time_steps(sim, stream, flush, 1, steps)
-        res = sim.last_solve()
+        converged, err = _last_solve(sim)
         its = sim.iteration_log(1 + steps)[1:1 + steps]
         out[name] = {"timesteps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
-                     "gmres_iters_per_step": float(np.mean(its)), "converged": bool(res.status == _lib.CF_OK)}
+                     "gmres_iters_per_step": float(np.mean(its)), "converged": converged}
+        if err:
+            out[name]["error"] = err
         sim.close()
     out["speedup"] = out["line_patches"]["timesteps_per_s"] / out["block_diagonal"]["timesteps_per_s"]
     out["learned"] = run_learned_large(local, inp, flush, steps)
@@ -405,8 +417,11 @@ def run_learned_large(local, inp, flush, steps, seeds=(7, 8, 9), max_pairs=40):
         with make(2024, _lib.CF_PRECOND_LEARNED_LINE) as sim:
             sim.set_network(net)
             sim.set_network_weight(w)
-            r = sim.step(0)
-            by_weight[w] = (r.iterations, r.status)
+            try:
+                r = sim.step(0)
+                by_weight[w] = (r.iterations, r.status)
+            except _lib.CufilError:
+                by_weight[w] = (None, _lib.CF_NONFINITE)
     ok = [w for w in by_weight if by_weight[w][1] == _lib.CF_OK]
     best = min(ok, key=lambda w: (by_weight[w][0], -w)) if ok else 0.0
     out = {"pairs": n_pairs, "collect_s": collect_s, "train_s": train_s, "losses": losses, "weight": best,
@@ -418,10 +433,12 @@ def run_learned_large(local, inp, flush, steps, seeds=(7, 8, 9), max_pairs=40):
         stream = torch.cuda.ExternalStream(sim.stream_handle())
         sim.step(0)
         ms = time_steps(sim, stream, flush, 1, steps)
-        res = sim.last_solve()
+        converged, err = _last_solve(sim)
         its = sim.iteration_log(1 + steps)[1:1 + steps]
         out.update({"timesteps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
-                    "gmres_iters_per_step": float(np.mean(its)), "converged": bool(res.status == _lib.CF_OK)})
+                    "gmres_iters_per_step": float(np.mean(its)), "converged": converged})
+        if err:
+            out["error"] = err
     net.close()
     return out
 
