@@ -424,35 +424,42 @@ __global__ void el_forces_kernel(ElDev d, int nt) {
 // Barrier forces (barrier_forces, cuda_functions.cu:1825-1919, wall and segment-segment terms):
 // a repulsion growing as the fourth power of the overlap within 1.1 (a_i + a_j) of another segment
 // (not the segment itself nor its neighbours in the same filament) and within DL/2 of the wall;
-// added in FP64 to the internal forces and packed as FP32 for the pair kernel.  One thread per
-// segment, sources staged through shared memory.
-constexpr int kBarThreads = 128;
+// added in FP64 to the internal forces and packed as FP32 for the pair kernel.  A block takes 32
+// targets; its eight warps split the sources (warp c takes every eighth of each 1024-source tile
+// staged in shared memory), screen the pairs on the FP32 positions with a margin and evaluate the
+// few within reach in FP64; the eight partial sums are added in a fixed order.
+constexpr int kBarTargets = 32, kBarSplit = 8, kBarThreads = kBarTargets * kBarSplit, kBarTile = 1024;
 __global__ void __launch_bounds__(kBarThreads) el_barrier_kernel(ElDev d) {
-    __shared__ double sx[kBarThreads][3];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float4 sx[kBarTile];
+    __shared__ double part[kBarSplit][kBarTargets][3];
+    const int t = threadIdx.x & 31, c = threadIdx.x >> 5;
+    const int i = blockIdx.x * kBarTargets + t;
     const bool live = i < d.N;
     double xi[3] = {0.0, 0.0, 0.0}, fb[3] = {0.0, 0.0, 0.0};
+    float4 xf = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (live) {
-        for (int c = 0; c < 3; ++c) xi[c] = d.x[3 * i + c];
-        if (xi[2] < 0.5 * d.DL) {
+        for (int q = 0; q < 3; ++q) xi[q] = d.x[3 * i + q];
+        xf = d.x4[i];
+        if (c == 0 && xi[2] < 0.5 * d.DL) {
             const double w = fmin(1.0, 1.0 - (xi[2] - 1.0) / (0.5 * d.DL - 1.0));
             fb[2] = d.frep * w * w * w * w;
         }
     }
     const int fi = live ? i / d.S : -1;
-    for (int j0 = 0; j0 < d.N; j0 += kBarThreads) {
-        const int j = j0 + threadIdx.x;
+    for (int j0 = 0; j0 < d.N; j0 += kBarTile) {
+        const int nj = min(kBarTile, d.N - j0);
         __syncthreads();
-        if (j < d.N)
-            for (int c = 0; c < 3; ++c) sx[threadIdx.x][c] = d.x[3 * j + c];
+        for (int q = threadIdx.x; q < nj; q += kBarThreads) sx[q] = d.x4[j0 + q];
         __syncthreads();
         if (!live) continue;
-        const int nj = min(kBarThreads, d.N - j0);
-        for (int jj = 0; jj < nj; ++jj) {
+        for (int jj = c; jj < nj; jj += kBarSplit) {
+            const float4 sj = sx[jj];
+            const float ex = xf.x - sj.x, ey = xf.y - sj.y, ez = xf.z - sj.z;
+            if (ex * ex + ey * ey + ez * ez >= 4.9f) continue;  // screen: (1.1 * 2a)^2 = 4.84, with margin
             const int js = j0 + jj;
-            const double dx = xi[0] - sx[jj][0], dy = xi[1] - sx[jj][1], dz = xi[2] - sx[jj][2];
+            const double dx = xi[0] - d.x[3 * js], dy = xi[1] - d.x[3 * js + 1], dz = xi[2] - d.x[3 * js + 2];
             const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 >= 4.84) continue;  // (1.1 * 2a)^2
+            if (r2 >= 4.84) continue;
             if (fi == js / d.S && abs(i - js) <= 1) continue;
             const double r = sqrt(r2);
             double w = fmin(1.0, 1.0 - 5.0 * (r - 2.0));
@@ -462,9 +469,15 @@ __global__ void __launch_bounds__(kBarThreads) el_barrier_kernel(ElDev d) {
             fb[2] += w * dz / r;
         }
     }
-    if (live)
-        d.f4[i] = make_float4(static_cast<float>(d.f[6 * i] + fb[0]), static_cast<float>(d.f[6 * i + 1] + fb[1]),
-                              static_cast<float>(d.f[6 * i + 2] + fb[2]), 0.0f);
+    for (int q = 0; q < 3; ++q) part[c][t][q] = fb[q];
+    __syncthreads();
+    if (c == 0 && live) {
+        double tot[3] = {0.0, 0.0, 0.0};
+        for (int cc = 0; cc < kBarSplit; ++cc)
+            for (int q = 0; q < 3; ++q) tot[q] += part[cc][t][q];
+        d.f4[i] = make_float4(static_cast<float>(d.f[6 * i] + tot[0]), static_cast<float>(d.f[6 * i + 1] + tot[1]),
+                              static_cast<float>(d.f[6 * i + 2] + tot[2]), 0.0f);
+    }
 }
 
 // compute_errors (mobility_solver.cpp:2760-2860, wall): backward Euler at step 0, BDF2 afterwards,
@@ -680,55 +693,45 @@ __global__ void el_jacobian_kernel(ElDev d, int nt) {
 }
 
 // In-place Gauss-Jordan inversion with partial pivoting of each filament's 6S x 6S block (FP64,
-// held in shared memory); a zero pivot column sets the non-finite flag.
-constexpr int kInvThreads = 256;
+// held in shared memory); a zero pivot column sets the non-finite flag.  Per pivot: warp 0 finds the
+// pivot row, the rows are interchanged, the pivot column is saved and the pivot row scaled, and the
+// rank-one update runs over a 2-D split of the matrix (warp w takes rows w, w + 16, ..., its lanes
+// consecutive columns).
+constexpr int kInvThreads = 512;
 __global__ void __launch_bounds__(kInvThreads) el_invert_kernel(ElDev d, int *flags) {
     extern __shared__ double A[];
     __shared__ int piv_row[6 * kMaxSeg];
     __shared__ double colk[6 * kMaxSeg];
     __shared__ int sp;
-    __shared__ double sv[kInvThreads / 32];
-    __shared__ int si[kInvThreads / 32];
     const int m = blockIdx.x, n = 6 * d.S;
     double *J = d.jinv + static_cast<size_t>(m) * n * n;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) A[e] = J[e];
     __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     bool singular = false;
     for (int k = 0; k < n; ++k) {
-        // pivot: the largest |A[r][k]|, r >= k (lowest index among ties)
-        double best = -1.0;
-        int bi = k;
-        for (int r = k + threadIdx.x; r < n; r += blockDim.x) {
-            const double a = fabs(A[r * n + k]);
-            if (a > best) {
-                best = a;
-                bi = r;
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_down_sync(0xffffffffu, best, o);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi < bi)) {
-                best = ob;
-                bi = oi;
-            }
-        }
-        if (lane == 0) {
-            sv[w] = best;
-            si[w] = bi;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double b = sv[0];
-            int p = si[0];
-            for (int q = 1; q < kInvThreads / 32; ++q)
-                if (sv[q] > b || (sv[q] == b && si[q] < p)) {
-                    b = sv[q];
-                    p = si[q];
+        if (w == 0) {  // pivot: the largest |A[r][k]|, r >= k (lowest index among ties)
+            double best = -1.0;
+            int bi = k;
+            for (int r = k + lane; r < n; r += 32) {
+                const double a = fabs(A[r * n + k]);
+                if (a > best) {
+                    best = a;
+                    bi = r;
                 }
-            sp = (b > 0.0) ? p : -1;
-            piv_row[k] = sp < 0 ? k : sp;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (lane == 0) {
+                sp = (best > 0.0) ? bi : -1;
+                piv_row[k] = sp < 0 ? k : sp;
+            }
         }
         __syncthreads();
         const int p = sp;
@@ -748,12 +751,12 @@ __global__ void __launch_bounds__(kInvThreads) el_invert_kernel(ElDev d, int *fl
         __syncthreads();
         for (int c = threadIdx.x; c < n; c += blockDim.x) A[k * n + c] = (c == k) ? inv : A[k * n + c] * inv;
         __syncthreads();
-        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-            const int r = e / n, c = e - r * n;
+        const double *prow = A + k * n;
+        for (int r = w; r < n; r += nw) {
             if (r == k) continue;
             const double fr = colk[r];
-            if (c == k) A[e] = -fr * inv;
-            else A[e] -= fr * A[k * n + c];
+            double *Ar = A + r * n;
+            for (int c = lane; c < n; c += 32) Ar[c] = (c == k) ? -fr * inv : fma(-fr, prow[c], Ar[c]);
         }
         __syncthreads();
     }
@@ -888,7 +891,7 @@ int evaluate(cf_elastic *h, int nt, double *e) {
     const ElDev d = dev(h);
     el_forces_kernel<<<h->F, 32, 0, st>>>(d, nt);
     CF_CHECK_LAUNCH("el_forces_kernel");
-    el_barrier_kernel<<<grid_for(h->N, kBarThreads), kBarThreads, 0, st>>>(d);
+    el_barrier_kernel<<<grid_for(h->N, kBarTargets), kBarThreads, 0, st>>>(d);
     CF_CHECK_LAUNCH("el_barrier_kernel");
     RpyBlockDesc bd{};
     bd.wall = 1;

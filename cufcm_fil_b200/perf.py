@@ -15,6 +15,10 @@
       one rebuild of the line-patch inverses of the benchmark lattice after its
       first step (assembly + the Gauss-Jordan rounds), CUDA events on the
       engine's stream, L2 flushed before each rebuild: mean and minimum.
+  python -m cufcm_fil_b200.perf elastic --nx 16 --steps 4
+      elastic instability cilia (cf_elastic): nx x nx filaments of 20
+      segments on a wall lattice at 80a, Broyden's method at the reference's
+      settings; host wall clock per synchronous step after step 0.
   python -m cufcm_fil_b200.perf mlp --batch 1024 --reps 50
       forward passes of the learned preconditioner's network (182 -> 256 -> 256
       -> 62, BF16 GEMMs) at one filament per row, as one GMRES iteration of the
@@ -108,6 +112,20 @@ def run_refresh(nx: int, reps: int):
     return {"nx": nx, "reps": reps, "refresh_ms_mean": float(np.mean(ms)), "refresh_ms_min": float(np.min(ms))}
 
 
+def run_elastic(nx: int, steps: int):
+    import time
+    from . import workloads
+    from .elastic import ElasticCiliaSimulation
+    with ElasticCiliaSimulation(bases=workloads.lattice_bases(nx * nx, nx, 80.0, 1.3)) as sim:
+        sim.step(0)
+        ms, its = [], []
+        for nt in range(1, 1 + steps):
+            t0 = time.perf_counter()
+            its.append(sim.step(nt))
+            ms.append(1e3 * (time.perf_counter() - t0))
+    return {"nx": nx, "steps": steps, "broyden_iterations": its, "step_ms": ms}
+
+
 def run_fcm(grid: int, reps: int, hbm_gbs: float | None = None):
     import torch
     from . import workloads
@@ -183,6 +201,9 @@ def main(argv=None):
     rf = sub.add_parser("refresh")
     rf.add_argument("--nx", type=int, default=16)
     rf.add_argument("--reps", type=int, default=20)
+    el = sub.add_parser("elastic")
+    el.add_argument("--nx", type=int, default=16)
+    el.add_argument("--steps", type=int, default=4)
     ml = sub.add_parser("mlp")
     ml.add_argument("--batch", type=int, default=1024)
     ml.add_argument("--reps", type=int, default=50)
@@ -191,6 +212,8 @@ def main(argv=None):
         print(json.dumps(run_steps(a.nx, a.precond, a.steps, a.line_patch, a.warm, a.block)))
     elif a.what == "refresh":
         print(json.dumps(run_refresh(a.nx, a.reps)))
+    elif a.what == "elastic":
+        print(json.dumps(run_elastic(a.nx, a.steps)))
     elif a.what == "mlp":
         print(json.dumps(run_mlp(a.batch, a.reps)))
     else:
