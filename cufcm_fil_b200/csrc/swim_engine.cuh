@@ -41,6 +41,8 @@ struct cf_swim {
     size_t scratch_cap = 0;
     int *err = nullptr;
     double *rhs = nullptr, *sol = nullptr, *w = nullptr, *z = nullptr, *t = nullptr, *Q = nullptr, *hb = nullptr;
+    double *dpart = nullptr;          // chunk partials of swim_dots_kernel [(max_iter + 1) * kSwimChunks]
+    unsigned int *dcount = nullptr;   // its arrival counter (zero between launches)
     int last_iters = 0, last_status = CF_OK;
     double last_relres = 0.0;
     bool stepped = false;
@@ -383,14 +385,36 @@ __global__ void swim_pc_add_kernel(SwimParams p, double *out) {
 }
 
 // ---- Krylov vector kernels (rows [0, n))
-// h[j] = <Q_j, w> for j < k1, one block per j, fixed-order block sums.
-__global__ void swim_dots_kernel(const double *Q, long long ldq, const double *w, int n, double *h) {
+// h[j] = <Q_j, w> for j < k1 (with `root`, h[0] = sqrt(<w, w>) for Q = w, k1 = 1).  Block (c, j) sums the
+// rows of chunk c with four independent accumulators; the block arriving last sums every j's chunks in a
+// fixed order (part: k1 x kSwimChunks partials, counter: zero on entry, reset by that block).
+constexpr int kSwimChunks = 16;
+__global__ void __launch_bounds__(256) swim_dots_kernel(const double *Q, long long ldq, const double *w, int n,
+                                                        double *part, unsigned int *counter, double *h, int root) {
     __shared__ double sm32[32];
-    const double *q = Q + static_cast<long long>(blockIdx.x) * ldq;
-    double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += q[i] * w[i];
-    s = block_sum(s, sm32);
-    if (threadIdx.x == 0) h[blockIdx.x] = s;
+    __shared__ int last;
+    const int c = blockIdx.x, j = blockIdx.y;
+    const int chunk = (n + kSwimChunks - 1) / kSwimChunks;
+    const int r0 = c * chunk, r1 = min(n, r0 + chunk);
+    const double *q = Q + static_cast<long long>(j) * ldq;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int i = r0 + threadIdx.x;
+    for (; i + 3 * 256 < r1; i += 4 * 256) {
+        a0 += q[i] * w[i];
+        a1 += q[i + 256] * w[i + 256];
+        a2 += q[i + 512] * w[i + 512];
+        a3 += q[i + 768] * w[i + 768];
+    }
+    for (; i < r1; i += 256) a0 += q[i] * w[i];
+    const double sum = block_sum((a0 + a1) + (a2 + a3), sm32);
+    if (threadIdx.x == 0) part[j * kSwimChunks + c] = sum;
+    if (!arrive_last(counter, gridDim.x * gridDim.y, &last)) return;
+    for (int jj = threadIdx.x; jj < static_cast<int>(gridDim.y); jj += blockDim.x) {
+        double t = 0.0;
+        for (int cc = 0; cc < kSwimChunks; ++cc) t += __ldcg(&part[jj * kSwimChunks + cc]);
+        h[jj] = root ? sqrt(t) : t;
+    }
+    if (threadIdx.x == 0) *counter = 0;
 }
 
 // w -= sum_j h[j] Q_j (j < k1)
@@ -400,14 +424,6 @@ __global__ void swim_sub_basis_kernel(double *w, const double *Q, long long ldq,
     double s = 0.0;
     for (int j = 0; j < k1; ++j) s += h[j] * Q[static_cast<long long>(j) * ldq + i];
     w[i] -= s;
-}
-
-__global__ void swim_norm_kernel(const double *w, int n, double *out) {
-    __shared__ double sm32[32];
-    double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += w[i] * w[i];
-    s = block_sum(s, sm32);
-    if (threadIdx.x == 0) *out = sqrt(s);
 }
 
 // dst = a * src + b * dst2 (dst2 may alias dst; b = 0 ignores it)
@@ -650,6 +666,13 @@ int swim_precon_matrix(cf_swim *h) {
     return CF_OK;
 }
 
+// out[j] = <Q_j, w> for j < k1 (Q rows n apart), or with `root` out[0] = |w| for Q = w, k1 = 1.
+int swim_dots(cf_swim *h, const double *Q, const double *w, int k1, double *out, int root) {
+    swim_dots_kernel<<<dim3(kSwimChunks, k1), 256, 0, h->stream>>>(Q, h->n, w, h->n, h->dpart, h->dcount, out, root);
+    CF_CHECK_LAUNCH("swim_dots_kernel");
+    return CF_OK;
+}
+
 // Right-preconditioned GMRES on A sol = rhs with the warm start in sol (mobility_solver.cpp:2187-2669):
 // zero RHS -> zero solution; a good guess is kept; a guess worse than zero is discarded.
 int swim_gmres(cf_swim *h) {
@@ -660,13 +683,11 @@ int swim_gmres(cf_swim *h) {
     // hb layout: [0, M+1) h1, [M+1, 2M+2) h2, [2M+2] norm, [2M+3] |rhs|, [2M+4..) y
     const int M = h->max_iter;
     double *h1 = h->hb, *h2 = h->hb + (M + 1), *nrm = h->hb + 2 * (M + 1), *nrhs = nrm + 1, *yd = nrm + 2;
-    swim_norm_kernel<<<1, 1024, 0, st>>>(h->rhs, n, nrhs);
-    CF_CHECK_LAUNCH("swim_norm_kernel");
+    CF_TRY(swim_dots(h, h->rhs, h->rhs, 1, nrhs, 1));
     CF_TRY(swim_matvec(h, h->sol, h->w));
     swim_axpby_kernel<<<g, 256, 0, st>>>(h->w, 1.0, h->rhs, -1.0, h->w, n);  // r0 = rhs - A x0
     CF_CHECK_LAUNCH("swim_axpby_kernel");
-    swim_norm_kernel<<<1, 1024, 0, st>>>(h->w, n, nrm);
-    CF_CHECK_LAUNCH("swim_norm_kernel");
+    CF_TRY(swim_dots(h, h->w, h->w, 1, nrm, 1));
     double nb[2];
     CF_CUDA(cudaMemcpyAsync(nb, nrm, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CF_TRY(swim_sync(h));
@@ -705,16 +726,13 @@ int swim_gmres(cf_swim *h) {
         const int k1 = it;  // basis vectors Q_0 .. Q_{it-1}
         CF_TRY(swim_precond(h, h->Q + static_cast<long long>(it - 1) * ldq, h->z));
         CF_TRY(swim_matvec(h, h->z, h->w));
-        swim_dots_kernel<<<k1, 512, 0, st>>>(h->Q, ldq, h->w, n, h1);
-        CF_CHECK_LAUNCH("swim_dots_kernel");
+        CF_TRY(swim_dots(h, h->Q, h->w, k1, h1, 0));
         swim_sub_basis_kernel<<<g, 256, 0, st>>>(h->w, h->Q, ldq, h1, k1, n);
         CF_CHECK_LAUNCH("swim_sub_basis_kernel");
-        swim_dots_kernel<<<k1, 512, 0, st>>>(h->Q, ldq, h->w, n, h2);
-        CF_CHECK_LAUNCH("swim_dots_kernel");
+        CF_TRY(swim_dots(h, h->Q, h->w, k1, h2, 0));
         swim_sub_basis_kernel<<<g, 256, 0, st>>>(h->w, h->Q, ldq, h2, k1, n);
         CF_CHECK_LAUNCH("swim_sub_basis_kernel");
-        swim_norm_kernel<<<1, 1024, 0, st>>>(h->w, n, nrm);
-        CF_CHECK_LAUNCH("swim_norm_kernel");
+        CF_TRY(swim_dots(h, h->w, h->w, 1, nrm, 1));
         CF_CUDA(cudaMemcpyAsync(hh.data(), h->hb, hh.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
         CF_TRY(swim_sync(h));
         const double qn = hh[2 * (M + 1)];
@@ -897,8 +915,11 @@ extern "C" int cf_swim_create(const cf_swim_config *cfg, cf_swim **out) {
             (rc = swim_alloc(h, &h->rhs, nv)) || (rc = swim_alloc(h, &h->sol, nv)) || (rc = swim_alloc(h, &h->w, nv)) ||
             (rc = swim_alloc(h, &h->z, nv)) || (rc = swim_alloc(h, &h->t, nv)) ||
             (rc = swim_alloc(h, &h->Q, static_cast<size_t>(h->max_iter + 1) * nv)) ||
-            (rc = swim_alloc(h, &h->hb, 3 * static_cast<size_t>(h->max_iter + 1) + 4)))
+            (rc = swim_alloc(h, &h->hb, 3 * static_cast<size_t>(h->max_iter + 1) + 4)) ||
+            (rc = swim_alloc(h, &h->dpart, static_cast<size_t>(h->max_iter + 1) * kSwimChunks)) ||
+            (rc = swim_alloc(h, &h->dcount, 1)))
             break;
+        if ((rc = cuda_status(cudaMemset(h->dcount, 0, sizeof(unsigned int)), "cudaMemset", __FILE__, __LINE__))) break;
         d.Rfil = h->Rfil;
         RpyBlockDesc bd{};
         bd.wall = 0;

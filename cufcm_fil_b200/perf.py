@@ -19,6 +19,9 @@
       elastic instability cilia (cf_elastic): nx x nx filaments of 20
       segments on a wall lattice at 80a, Broyden's method at the reference's
       settings; host wall clock per synchronous step after step 0.
+  python -m cufcm_fil_b200.perf swimmer --steps 4
+      the free swimmer (cf_swim) of the benchmark: 256 cilia x 20 segments on a
+      sphere of 2562 blobs; host wall clock per synchronous step after step 0.
   python -m cufcm_fil_b200.perf mlp --batch 1024 --reps 50
       forward passes of the learned preconditioner's network (182 -> 256 -> 256
       -> 62, BF16 GEMMs) at one filament per row, as one GMRES iteration of the
@@ -126,6 +129,28 @@ def run_elastic(nx: int, steps: int):
     return {"nx": nx, "steps": steps, "broyden_iterations": its, "step_ms": ms}
 
 
+def run_swimmer(steps: int):
+    import time
+    from pathlib import Path
+    from . import swim
+    golden = Path(__file__).resolve().parents[1] / "tests" / "golden"
+    gold = np.load(golden / "reference_forcing_nseg20_sep2.6.npz")
+    tips = np.load(golden / "ref_tips_16x16_80a.npz")
+    F, B = 256, 2562
+    geo = swim.sphere_geometry(swim.fibonacci_normals(F), swim.fibonacci_normals(B, 0.3), ar=6.0)
+    rng = np.random.default_rng(12)
+    with swim.CiliatedSwimmer(geometry=geo, phase0=rng.uniform(0, 2 * np.pi, F), angle0=rng.normal(0, 0.05, F),
+                              phase_refs=gold["fb_phase"], angle_refs=gold["fb_angle"],
+                              s_table=tips["s_table"]) as sim:
+        sim.step(0)
+        ms, its = [], []
+        for nt in range(1, 1 + steps):
+            t0 = time.perf_counter()
+            its.append(sim.step(nt).iterations)
+            ms.append(1e3 * (time.perf_counter() - t0))
+    return {"steps": steps, "gmres_iterations": its, "step_ms": ms}
+
+
 def run_fcm(grid: int, reps: int, hbm_gbs: float | None = None):
     import torch
     from . import workloads
@@ -204,6 +229,8 @@ def main(argv=None):
     el = sub.add_parser("elastic")
     el.add_argument("--nx", type=int, default=16)
     el.add_argument("--steps", type=int, default=4)
+    sw = sub.add_parser("swimmer")
+    sw.add_argument("--steps", type=int, default=4)
     ml = sub.add_parser("mlp")
     ml.add_argument("--batch", type=int, default=1024)
     ml.add_argument("--reps", type=int, default=50)
@@ -214,6 +241,8 @@ def main(argv=None):
         print(json.dumps(run_refresh(a.nx, a.reps)))
     elif a.what == "elastic":
         print(json.dumps(run_elastic(a.nx, a.steps)))
+    elif a.what == "swimmer":
+        print(json.dumps(run_swimmer(a.steps)))
     elif a.what == "mlp":
         print(json.dumps(run_mlp(a.batch, a.reps)))
     else:
