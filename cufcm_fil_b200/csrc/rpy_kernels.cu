@@ -187,6 +187,7 @@ struct SymParams {
     float4 *partial;
     int n, nb;
     long long items;
+    float a, inv_mu;  // unbounded form: the common radius and 1 / viscosity
 };
 
 __device__ __forceinline__ void sym_item(long long t, int nb, int &I, int &J) {
@@ -212,7 +213,10 @@ __device__ __forceinline__ void sym_load(const SymParams &p, int idx, int lane, 
     }
 }
 
-__global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_kernel(SymParams p) {
+// WALL false: the same scheme for the unbounded product of equal spheres (free_pair_sym_f32); the diagonal
+// tiles then add each target's own self mobility, which the one-sided loop (j != i) leaves out.
+template <bool WALL>
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_sym_kernel(SymParams p) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int src_lane = (lane + 1) & 31;
@@ -238,7 +242,16 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_kernel(SymP
                 fs.y = __shfl_sync(full, fs.y, src_lane);
                 fs.z = __shfl_sync(full, fs.z, src_lane);
                 const float fsv[3] = {fs.x, fs.y, fs.z};
-                wall_pair_f32<3, 3>(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, vi);
+                if constexpr (WALL)
+                    wall_pair_f32<3, 3>(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, vi);
+                else
+                    free_pair_f32<3, 3>(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, p.a, p.a, p.inv_mu, fsv, vi);
+            }
+            if constexpr (!WALL) {  // the self mobility of the target
+                const float self = p.inv_mu / (6.0f * 3.14159265358979f * p.a);
+                vi[0] += self * fi.x;
+                vi[1] += self * fi.y;
+                vi[2] += self * fi.z;
             }
             if (i < p.n) p.partial[static_cast<size_t>(i) * p.nb + I] = make_float4(vi[0], vi[1], vi[2], 0.0f);
         } else {
@@ -246,7 +259,10 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_wall_sym_kernel(SymP
 #pragma unroll 2
             for (int step = 0; step < 32; ++step) {
                 const float fsv[3] = {fs.x, fs.y, fs.z};
-                wall_pair_sym_f32(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, fiv, vi, vs);
+                if constexpr (WALL)
+                    wall_pair_sym_f32(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, xi.z, xs.z, fsv, fiv, vi, vs);
+                else
+                    free_pair_sym_f32(xi.x - xs.x, xi.y - xs.y, xi.z - xs.z, p.a, p.inv_mu, fsv, fiv, vi, vs);
                 xs.x = __shfl_sync(full, xs.x, src_lane);
                 xs.y = __shfl_sync(full, xs.y, src_lane);
                 xs.z = __shfl_sync(full, xs.z, src_lane);
@@ -569,8 +585,11 @@ int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch
         p.n = d.nt;
         p.nb = plan.nb;
         p.items = plan.items;
-        rpy_wall_sym_kernel<<<plan.grid, kThreads, 0, st>>>(p);
-        CF_CHECK_LAUNCH("rpy_wall_sym_kernel");
+        p.a = d.at;
+        p.inv_mu = 1.0f / d.mu;
+        if (d.wall) rpy_sym_kernel<true><<<plan.grid, kThreads, 0, st>>>(p);
+        else rpy_sym_kernel<false><<<plan.grid, kThreads, 0, st>>>(p);
+        CF_CHECK_LAUNCH("rpy_sym_kernel");
         return CF_OK;
     }
     const bool self = d.self_set != 0;
@@ -629,6 +648,8 @@ int pack_ft6_to_float4(const float *aos6, float4 *force, float4 *torque, int n, 
 
 RpyPlan rpy_plan_for(const RpyBlockDesc &d, int num_sms) {
     if (d.wall && d.self_set && d.vd == 3 && d.fd == 3 && d.nt == d.ns && d.xt == d.xs)
+        return rpy_plan_sym(d.nt, num_sms);
+    if (!d.wall && d.vd == 3 && d.fd == 3 && d.nt == d.ns && d.xt == d.xs && d.at == d.as)  // equal spheres
         return rpy_plan_sym(d.nt, num_sms);
     return rpy_plan(d.nt, d.ns, d.vd, d.fd, num_sms);
 }

@@ -316,4 +316,38 @@ __device__ __forceinline__ void wall_pair_sym_f32(float dx, float dy, float dz, 
     }
 }
 
+// Unbounded RPY pair of two equal spheres (radius a) in both directions: the block M = A I + B u u^T is the
+// same for i <- j and j <- i (u changes sign, u u^T does not), so one evaluation serves both.  Branches as in
+// free_pair_f32 with ai = aj = a (far; overlapping, with dmin = 0; coincident: the self mobility).
+__device__ __forceinline__ void free_pair_sym_f32(float dx, float dy, float dz, float a, float inv_mu, const float *fj,
+                                                  const float *fi, float *vi, float *vj) {
+    const float pi = 3.14159265358979f;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float r = sqrtf(r2);
+    const float s = 1.0f / (r + 1e-20f);
+    const float ux = dx * s, uy = dy * s, uz = dz * s;
+    float A, Bc;
+    if (r > 2.0f * a) {
+        const float q = s * s * (2.0f * a * a) * (1.0f / 3.0f);
+        const float c = s * inv_mu * (1.0f / (8.0f * pi));
+        A = (1.0f + q) * c;
+        Bc = (1.0f - 3.0f * q) * c;
+    } else if (r > 0.0f) {
+        const float c = inv_mu / (6.0f * pi * a * a);
+        A = (a - (9.0f / 32.0f) * r) * c;
+        Bc = (3.0f / 32.0f) * r * c;
+    } else {
+        A = inv_mu / (6.0f * pi * a);
+        Bc = 0.0f;
+    }
+    const float tj = Bc * (ux * fj[0] + uy * fj[1] + uz * fj[2]);
+    const float ti = Bc * (ux * fi[0] + uy * fi[1] + uz * fi[2]);
+    vi[0] += A * fj[0] + tj * ux;
+    vi[1] += A * fj[1] + tj * uy;
+    vi[2] += A * fj[2] + tj * uz;
+    vj[0] += A * fi[0] + ti * ux;
+    vj[1] += A * fi[1] + ti * uy;
+    vj[2] += A * fi[2] + ti * uz;
+}
+
 }  // namespace cufil
