@@ -424,15 +424,15 @@ __global__ void el_forces_kernel(ElDev d, int nt) {
 // Barrier forces (barrier_forces, cuda_functions.cu:1825-1919, wall and segment-segment terms):
 // a repulsion growing as the fourth power of the overlap within 1.1 (a_i + a_j) of another segment
 // (not the segment itself nor its neighbours in the same filament) and within DL/2 of the wall;
-// added in FP64 to the internal forces and packed as FP32 for the pair kernel.  A block takes 32
-// targets; its eight warps split the sources (warp c takes every eighth of each 1024-source tile
-// staged in shared memory), screen the pairs on the FP32 positions with a margin and evaluate the
-// few within reach in FP64; the eight partial sums are added in a fixed order.
-constexpr int kBarTargets = 32, kBarSplit = 8, kBarThreads = kBarTargets * kBarSplit, kBarTile = 1024;
+// added in FP64 to the internal forces and packed as FP32 for the pair kernel.  A block takes 16
+// targets; its threads split the sources sixteen ways (split c takes every sixteenth of each
+// 1024-source tile staged in shared memory), screen the pairs on the FP32 positions with a margin and
+// evaluate the few within reach in FP64; the sixteen partial sums are added in a fixed order.
+constexpr int kBarTargets = 16, kBarSplit = 16, kBarThreads = kBarTargets * kBarSplit, kBarTile = 1024;
 __global__ void __launch_bounds__(kBarThreads) el_barrier_kernel(ElDev d) {
     __shared__ float4 sx[kBarTile];
     __shared__ double part[kBarSplit][kBarTargets][3];
-    const int t = threadIdx.x & 31, c = threadIdx.x >> 5;
+    const int t = threadIdx.x % kBarTargets, c = threadIdx.x / kBarTargets;
     const int i = blockIdx.x * kBarTargets + t;
     const bool live = i < d.N;
     double xi[3] = {0.0, 0.0, 0.0}, fb[3] = {0.0, 0.0, 0.0};
@@ -693,15 +693,16 @@ __global__ void el_jacobian_kernel(ElDev d, int nt) {
 }
 
 // In-place Gauss-Jordan inversion with partial pivoting of each filament's 6S x 6S block (FP64,
-// held in shared memory); a zero pivot column sets the non-finite flag.  Per pivot: warp 0 finds the
-// pivot row, the rows are interchanged, the pivot column is saved and the pivot row scaled, and the
-// rank-one update runs over a 2-D split of the matrix (warp w takes rows w, w + 16, ..., its lanes
-// consecutive columns).
+// held in shared memory); a zero pivot column sets the non-finite flag.  Per pivot, three barriers:
+// warp 0 finds the pivot row; the pivot row, row k and the pivot column are saved; then the row
+// interchange, the scaling of the pivot row and the rank-one update are one pass in which every element
+// is written from its own old value and the saved vectors, over a 2-D split of the matrix (warp w takes
+// rows w, w + 16, ..., its lanes consecutive columns).
 constexpr int kInvThreads = 512;
 __global__ void __launch_bounds__(kInvThreads) el_invert_kernel(ElDev d, int *flags) {
     extern __shared__ double A[];
     __shared__ int piv_row[6 * kMaxSeg];
-    __shared__ double colk[6 * kMaxSeg];
+    __shared__ double colk[6 * kMaxSeg], prow_s[6 * kMaxSeg], rowk_s[6 * kMaxSeg];
     __shared__ int sp;
     const int m = blockIdx.x, n = 6 * d.S;
     double *J = d.jinv + static_cast<size_t>(m) * n * n;
@@ -739,24 +740,28 @@ __global__ void __launch_bounds__(kInvThreads) el_invert_kernel(ElDev d, int *fl
             singular = true;
             break;
         }
-        if (p != k)
-            for (int c = threadIdx.x; c < n; c += blockDim.x) {
-                const double t = A[k * n + c];
-                A[k * n + c] = A[p * n + c];
-                A[p * n + c] = t;
-            }
+        // save the scaled pivot row (old row p times 1/pivot, 1/pivot in column k), old row k and the pivot
+        // column with rows k and p interchanged
+        const double inv = 1.0 / A[p * n + k];
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            prow_s[c] = (c == k) ? inv : A[p * n + c] * inv;
+            rowk_s[c] = A[k * n + c];
+        }
+        for (int r = threadIdx.x; r < n; r += blockDim.x) colk[r] = A[(r == k ? p : (r == p ? k : r)) * n + k];
         __syncthreads();
-        const double inv = 1.0 / A[k * n + k];
-        for (int r = threadIdx.x; r < n; r += blockDim.x) colk[r] = A[r * n + k];
-        __syncthreads();
-        for (int c = threadIdx.x; c < n; c += blockDim.x) A[k * n + c] = (c == k) ? inv : A[k * n + c] * inv;
-        __syncthreads();
-        const double *prow = A + k * n;
+        // every element from its own old value and the saved vectors: row k becomes the scaled pivot row, every
+        // other row (row p holding old row k after the interchange) loses its pivot-column entry times it; the
+        // lane that wrote a row's column-k entry then replaces it by -entry / pivot
         for (int r = w; r < n; r += nw) {
-            if (r == k) continue;
-            const double fr = colk[r];
             double *Ar = A + r * n;
-            for (int c = lane; c < n; c += 32) Ar[c] = (c == k) ? -fr * inv : fma(-fr, prow[c], Ar[c]);
+            if (r == k) {
+                for (int c = lane; c < n; c += 32) Ar[c] = prow_s[c];
+                continue;
+            }
+            const double fr = colk[r];
+            const double *src = (r == p) ? rowk_s : Ar;
+            for (int c = lane; c < n; c += 32) Ar[c] = fma(-fr, prow_s[c], src[c]);
+            if (lane == (k & 31)) Ar[k] = -fr * inv;
         }
         __syncthreads();
     }
