@@ -13,6 +13,10 @@ iterations of every step and the segment positions every 10 steps; and, for one
 filament, the inverse approximate Jacobian and the residual of the first
 evaluation of step 0 (the reference's invert_approx_jacobian).
 
+Also writes tests/golden/ref_elastic_2x2_2p1a.npz: the same 2 x 2 lattice at spacing 2.1a for 20 steps, where
+the bases of neighbouring cilia are closer than the barrier range 1.1 (a_i + a_j) = 2.2a, so the segment-segment
+barrier forces act from the first evaluation; positions and Broyden iterations of every step.
+
 Run: python tests/golden/make_elastic_golden.py   (needs the oracle/_ref binaries; a few seconds)
 """
 import sys
@@ -25,7 +29,9 @@ sys.path.insert(0, str(HERE.parents[1]))
 from oracle import ref_step  # noqa: E402
 
 OUT = HERE / "ref_elastic_2x2_80a.npz"
+OUT_CLOSE = HERE / "ref_elastic_2x2_2p1a.npz"
 NX, SPACING, STEPS, PERIOD, EVERY = 2, 80.0, 300, 36.3833, 10
+CLOSE_SPACING, CLOSE_STEPS = 2.1, 20
 
 
 def main():
@@ -35,6 +41,10 @@ def main():
     np.savez_compressed(OUT, nx=NX, spacing=SPACING, steps=STEPS, period=PERIOD, saved_steps=saved,
                         x=r.x[saved], iterations=r.iterations, jinv0=jinv, err0=err0)
     print(OUT, "Broyden iterations per step: mean %.2f max %d" % (r.iterations.mean(), r.iterations.max()))
+    c = ref_step.run_elastic(nfil=NX * NX, fil_x_dim=NX, spacing=CLOSE_SPACING, steps=CLOSE_STEPS, period=PERIOD)
+    np.savez_compressed(OUT_CLOSE, nx=NX, spacing=CLOSE_SPACING, steps=CLOSE_STEPS, period=PERIOD, x=c.x,
+                        iterations=c.iterations)
+    print(OUT_CLOSE, "Broyden iterations per step:", c.iterations.tolist())
 
 
 if __name__ == "__main__":

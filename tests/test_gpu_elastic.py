@@ -1,7 +1,8 @@
 """GPU tests of the elastic-filament step (cf_elastic) through the C ABI.
 
 Oracle: the reference's own host step code for instability-driven cilia on a wall
-(tests/golden/ref_elastic_2x2_80a.npz, make_elastic_golden.py).  The approximate
+(tests/golden/ref_elastic_2x2_80a.npz, and ref_elastic_2x2_2p1a.npz with touching cilia, where the
+segment-segment barrier forces act; make_elastic_golden.py).  The approximate
 Jacobian is FP64 throughout and is compared at 1e-10; the residual of the first
 evaluation carries the FP32 pair mobility (1e-5 of its largest entry).  The trajectory:
 the follower force buckles the filaments, an instability that amplifies any difference,
@@ -19,6 +20,7 @@ from cufcm_fil_b200.elastic import ElasticCiliaSimulation
 pytestmark = pytest.mark.gpu
 
 EL = np.load(Path(__file__).resolve().parent / "golden" / "ref_elastic_2x2_80a.npz")
+ELC = np.load(Path(__file__).resolve().parent / "golden" / "ref_elastic_2x2_2p1a.npz")
 L = 2.6 * 20  # FIL_LENGTH = DL NSEG for elastic filaments
 
 
@@ -83,3 +85,20 @@ def test_broyden_cap_and_non_finite_state_are_reported():
             sim.step(0)
         assert e.value.code == _lib.CF_NONFINITE
         sim.stats()
+
+
+def test_touching_cilia_follow_reference():
+    # 2 x 2 lattice at 2.1a: the bases of neighbouring cilia are inside the barrier range 2.2a, so the
+    # segment-segment barrier forces act from the first evaluation (20 steps of the reference's own step).
+    # The barrier is stiff: Broyden's method takes 40 iterations at step 0 in the reference.
+    iters, worst = [], []
+    with make(int(ELC["nx"]), float(ELC["spacing"])) as sim:
+        for nt in range(int(ELC["steps"])):
+            iters.append(sim.step(nt))
+            x = sim.segments()[0]
+            worst.append(np.abs(x - ELC["x"][nt]).max() / L)
+    it_ref = ELC["iterations"]
+    print(f"touching cilia, 20 steps: position error / L at steps 0, 9, 19: {worst[0]:.2e} {worst[9]:.2e} "
+          f"{worst[19]:.2e}; Broyden iterations {iters} (reference {it_ref.tolist()})")
+    assert max(worst) < 1e-5
+    assert abs(iters[0] - it_ref[0]) <= 2 and abs(np.mean(iters) - it_ref.mean()) < 0.15 * it_ref.mean()
