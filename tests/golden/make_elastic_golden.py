@@ -17,6 +17,10 @@ Also writes tests/golden/ref_elastic_2x2_2p1a.npz: the same 2 x 2 lattice at spa
 the bases of neighbouring cilia are closer than the barrier range 1.1 (a_i + a_j) = 2.2a, so the segment-segment
 barrier forces act from the first evaluation; positions and Broyden iterations of every step.
 
+Also writes tests/golden/ref_elastic_jinv_probes.npz: for one filament of 14, 20 and 24 segments, the reference's
+inverse approximate Jacobian (first evaluation of step 0) times four seeded normal columns
+(numpy default_rng(5)), and its Frobenius norm.  These cover each block size class of the device inversion.
+
 Run: python tests/golden/make_elastic_golden.py   (needs the oracle/_ref binaries; a few seconds)
 """
 import sys
@@ -32,6 +36,19 @@ OUT = HERE / "ref_elastic_2x2_80a.npz"
 OUT_CLOSE = HERE / "ref_elastic_2x2_2p1a.npz"
 NX, SPACING, STEPS, PERIOD, EVERY = 2, 80.0, 300, 36.3833, 10
 CLOSE_SPACING, CLOSE_STEPS = 2.1, 20
+OUT_PROBES = HERE / "ref_elastic_jinv_probes.npz"
+PROBE_NSEG = (14, 20, 24)
+
+
+def write_probes():
+    out = {}
+    for ns in PROBE_NSEG:
+        jinv, _ = ref_step.elastic_jacobian(nseg=ns, period=PERIOD)
+        v = np.random.default_rng(5).standard_normal((6 * ns, 4))
+        out[f"p{ns}"] = jinv @ v
+        out[f"norm{ns}"] = np.linalg.norm(jinv)
+    np.savez_compressed(OUT_PROBES, nseg=np.array(PROBE_NSEG), period=PERIOD, **out)
+    print(OUT_PROBES)
 
 
 def main():
@@ -45,6 +62,7 @@ def main():
     np.savez_compressed(OUT_CLOSE, nx=NX, spacing=CLOSE_SPACING, steps=CLOSE_STEPS, period=PERIOD, x=c.x,
                         iterations=c.iterations)
     print(OUT_CLOSE, "Broyden iterations per step:", c.iterations.tolist())
+    write_probes()
 
 
 if __name__ == "__main__":

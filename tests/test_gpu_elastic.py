@@ -21,6 +21,7 @@ pytestmark = pytest.mark.gpu
 
 EL = np.load(Path(__file__).resolve().parent / "golden" / "ref_elastic_2x2_80a.npz")
 ELC = np.load(Path(__file__).resolve().parent / "golden" / "ref_elastic_2x2_2p1a.npz")
+ELP = np.load(Path(__file__).resolve().parent / "golden" / "ref_elastic_jinv_probes.npz")
 L = 2.6 * 20  # FIL_LENGTH = DL NSEG for elastic filaments
 
 
@@ -36,6 +37,20 @@ def test_first_evaluation_and_jacobian_match_reference():
     ref = EL["jinv0"]
     assert np.linalg.norm(jinv - ref) / np.linalg.norm(ref) < 1e-10
     np.testing.assert_allclose(err, EL["err0"], rtol=0, atol=1e-5 * np.abs(EL["err0"]).max())
+
+
+@pytest.mark.parametrize("nseg", [14, 20, 24])
+def test_jacobian_inverse_every_block_size(nseg):
+    """The device inversion has one form per block size class (84, 120, 144 unknowns here): each matches
+    the reference's invert_approx_jacobian through seeded probes."""
+    bases = workloads.lattice_bases(1, 1, 80.0, 1.3)
+    with ElasticCiliaSimulation(bases=bases, nseg=nseg, seg_sep=2.6, dt=float(ELP["period"]) / 300) as sim:
+        sim.first_evaluation(0)
+        jinv = sim.jacobian_inverse(0)
+    v = np.random.default_rng(5).standard_normal((6 * nseg, 4))
+    ref = ELP[f"p{nseg}"]
+    assert np.linalg.norm(jinv @ v - ref) / np.linalg.norm(ref) < 1e-10
+    assert abs(np.linalg.norm(jinv) / float(ELP[f"norm{nseg}"]) - 1.0) < 1e-10
 
 
 def test_trajectory_follows_reference():
