@@ -360,8 +360,7 @@ extern "C" int cf_apply_mobility_device(cf_mobility *h, const float *d_x_segs, c
     CF_CUDA(cudaSetDevice(h->cfg.device));
     // A null stream is CUDA's legacy default stream, as for any runtime call.
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    CF_TRY(pack_xyz_to_float4(d_x_segs, h->xs4, ns, st));
-    CF_TRY(pack_ft6_to_float4(d_f_segs, h->fs4, h->ts4, ns, st));
+    CF_TRY(pack_set_to_float4(d_x_segs, d_f_segs, h->xs4, h->fs4, h->ts4, ns, st));
     CF_TRY(pack_xyz_to_float4(d_x_blobs, h->xb4, nb, st));
     CF_TRY(pack_xyz_to_float4(d_f_blobs, h->fb4, nb, st));
     return eval_full(h, d_v_segs, d_v_blobs, st);

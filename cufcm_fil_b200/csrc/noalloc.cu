@@ -99,8 +99,7 @@ extern "C" int cf_rpy_wall_segments_noalloc(const float *d_x_segs, const float *
     // unwritten (stale from an earlier call) and sets the flag; the reduction
     // reads the flag and then writes NaN to every output instead of a sum.
     CF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-    CF_TRY(pack_xyz_to_float4(d_x_segs, x4, n_seg, st));
-    CF_TRY(pack_ft6_to_float4(d_f_segs, f4, nullptr, n_seg, st));
+    CF_TRY(pack_set_to_float4(d_x_segs, d_f_segs, x4, f4, nullptr, n_seg, st));
     CF_TRY(rpy_launch_tiles(d, plan, partial, err, st));
     return rpy_launch_reduce_f32(d, plan, partial, d_v_segs, 6, kOutWrite, st, err);
 }

@@ -434,6 +434,17 @@ __global__ void pack_ft6_kernel(const float *__restrict__ a, float4 *__restrict_
     }
 }
 
+// Positions and forces (+ torques) of one particle set in one launch.
+__global__ void pack_set_kernel(const float *__restrict__ x, const float *__restrict__ ft, float4 *__restrict__ xo,
+                                float4 *__restrict__ fo, float4 *__restrict__ to, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        xo[i] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0f);
+        fo[i] = make_float4(ft[6 * i], ft[6 * i + 1], ft[6 * i + 2], 0.0f);
+        if (to) to[i] = make_float4(ft[6 * i + 3], ft[6 * i + 4], ft[6 * i + 5], 0.0f);
+    }
+}
+
 // Raises the dynamic shared-memory cap of one instantiation once per device.
 // Called before any launch (and therefore before any stream capture).
 template <bool WALL, int VD, int FD, int TI, bool SELF>
@@ -636,6 +647,14 @@ int pack_xyz_to_float4(const float *aos3, float4 *out, int n, cudaStream_t st) {
     if (n <= 0) return CF_OK;
     pack_xyz_kernel<<<(n + 255) / 256, 256, 0, st>>>(aos3, out, n);
     CF_CHECK_LAUNCH("pack_xyz_kernel");
+    return CF_OK;
+}
+
+int pack_set_to_float4(const float *aos3, const float *aos6, float4 *x, float4 *force, float4 *torque, int n,
+                       cudaStream_t st) {
+    if (n <= 0) return CF_OK;
+    pack_set_kernel<<<(n + 255) / 256, 256, 0, st>>>(aos3, aos6, x, force, torque, n);
+    CF_CHECK_LAUNCH("pack_set_kernel");
     return CF_OK;
 }
 

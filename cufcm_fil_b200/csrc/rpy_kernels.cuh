@@ -105,6 +105,9 @@ unsigned rpy_wait_limit();
 // Packing helpers between the reference's AoS host layouts and float4 arrays.
 int pack_xyz_to_float4(const float *aos3, float4 *out, int n, cudaStream_t st);
 int pack_ft6_to_float4(const float *aos6, float4 *force, float4 *torque, int n, cudaStream_t st);
+// Both of the above for one particle set (positions [3n], forces + torques [6n]) in one launch.
+int pack_set_to_float4(const float *aos3, const float *aos6, float4 *x, float4 *force, float4 *torque, int n,
+                       cudaStream_t st);
 
 // Full product V_t (=|+=) M F_s with the right staging; convenience wrapper.
 int rpy_block_product(const RpyBlockDesc &d, float4 *scratch, size_t scratch_cap, int *dev_err, float *out_f,
