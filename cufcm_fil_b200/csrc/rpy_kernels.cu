@@ -217,6 +217,7 @@ __device__ __forceinline__ void sym_load(const SymParams &p, int idx, int lane, 
 // tiles then add each target's own self mobility, which the one-sided loop (j != i) leaves out.
 template <bool WALL>
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_sym_kernel(SymParams p) {
+    chain_wait();  // launched as a programmatic dependent of the packing launch
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int src_lane = (lane + 1) & 31;
@@ -367,6 +368,7 @@ struct ReduceParams {
 // block and writes or accumulates the result.
 template <bool WALL_SELF, int VD, int FD>
 __global__ void rpy_reduce_kernel(ReduceParams p) {
+    chain_wait();  // launched as a programmatic dependent of the tile launch
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.nt) return;
@@ -505,7 +507,7 @@ template <bool WS, int VD, int FD>
 int launch_reduce_t(const ReduceParams &p, cudaStream_t st) {
     const int threads = 256;  // 8 targets per block
     const int blocks = (p.nt + 7) / 8;
-    rpy_reduce_kernel<WS, VD, FD><<<blocks, threads, 0, st>>>(p);
+    CF_CUDA(launch_chained(rpy_reduce_kernel<WS, VD, FD>, dim3(blocks), dim3(threads), 0, st, p));
     CF_CHECK_LAUNCH("rpy_reduce_kernel");
     return CF_OK;
 }
@@ -598,8 +600,8 @@ int rpy_launch_tiles(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch
         p.items = plan.items;
         p.a = d.at;
         p.inv_mu = 1.0f / d.mu;
-        if (d.wall) rpy_sym_kernel<true><<<plan.grid, kThreads, 0, st>>>(p);
-        else rpy_sym_kernel<false><<<plan.grid, kThreads, 0, st>>>(p);
+        if (d.wall) CF_CUDA(launch_chained(rpy_sym_kernel<true>, dim3(plan.grid), dim3(kThreads), 0, st, p));
+        else CF_CUDA(launch_chained(rpy_sym_kernel<false>, dim3(plan.grid), dim3(kThreads), 0, st, p));
         CF_CHECK_LAUNCH("rpy_sym_kernel");
         return CF_OK;
     }
