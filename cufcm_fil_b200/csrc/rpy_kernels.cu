@@ -93,6 +93,7 @@ __device__ __forceinline__ void tile_sum(const float4 *__restrict__ xs_s, const 
 // particle set (wall mode skips j == i here; the reduction adds the self block).
 template <bool WALL, int VD, int FD, int TI, bool SELF>
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) rpy_tile_kernel(TileParams p) {
+    chain_wait();  // launched as a programmatic dependent of the packing launch
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
     float4 *xs_s = reinterpret_cast<float4 *>(smem_raw + 16);
@@ -483,7 +484,7 @@ int launch_tiles_t(const RpyBlockDesc &d, const RpyPlan &plan, float4 *scratch, 
     p.err = dev_err;
     p.wait_limit = rpy_wait_limit();
     dim3 grid(plan.tiles, plan.nsplit);
-    kern<<<grid, kThreads, plan.smem, st>>>(p);
+    CF_CUDA(launch_chained(kern, grid, dim3(kThreads), plan.smem, st, p));
     CF_CHECK_LAUNCH("rpy_tile_kernel");
     return CF_OK;
 }
